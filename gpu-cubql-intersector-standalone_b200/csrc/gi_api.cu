@@ -1,0 +1,925 @@
+// gi_api.cu -- C ABI (include/gi/gi.h) over the kernels in gi_kernels.cu.
+//
+// Host flow of gi_intersect (replaces KernelBVHController::runIntersectionPipeline,
+// src/GPUIntersector/KernelBVHController.cu:603-699 in the reference, whose chunk
+// loop syncs and copies to the host several times per chunk and calls CGAL on
+// the CPU for undecided pairs):
+//   counters reset -> frontier init -> k_traverse (cooperative) -> k_exact
+//   -> one counters read-back (capacity check; buffers grow x4 and the call is
+//      re-run on overflow) -> k_segments -> ordering -> copies to the host.
+// No CPU fallback exists: every pair is decided on the device.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/gi/gi.h"
+#include "gi_launch.h"
+
+using namespace gi;
+
+struct gi_mesh {
+    gi_ctx* ctx = nullptr;
+    MeshBuffers b;
+    bool has64 = false;
+};
+
+struct gi_result {
+    std::vector<int32_t> pairs;
+    std::vector<double> segs;
+    std::vector<int32_t> seg_pair;
+    gi_stats stats;
+};
+
+struct gi_ctx {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    LaunchCfg cfg;
+    uint64_t budget = 0;
+    uint32_t flags = 0;
+    std::atomic<uint64_t> mesh_bytes{0};
+    std::string last_error;
+    std::mutex mu;  // serialises device work of this context
+
+    Counters* d_cnt = nullptr;
+    Counters* h_cnt = nullptr;  // pinned
+    JobDev* d_jobs = nullptr;
+    JobDev* h_jobs = nullptr;  // pinned
+    uint32_t cap_jobs = 0;
+    uint4* front[2] = {nullptr, nullptr};
+    uint32_t cap_front = 0, cap_front1 = 0;
+    uint4* cand = nullptr;
+    uint32_t cap_cand = 0;
+    uint4* res = nullptr;
+    uint32_t cap_res = 0;
+    uint32_t* esc = nullptr;
+    uint32_t cap_esc = 0;
+    // outputs
+    double* segs = nullptr;  // 18 per result slot
+    uint32_t* nseg = nullptr;
+    uint32_t* perm = nullptr;
+    int32_t* pairs_out = nullptr;
+    uint32_t* job_out = nullptr;
+    double* segs_out = nullptr;
+    int32_t* segpair_out = nullptr;
+    uint32_t* seg_off = nullptr;
+    uint32_t* seg_scan_tmp = nullptr;
+    uint32_t* d_total = nullptr;
+    uint32_t cap_out = 0;
+    void* order_scratch = nullptr;
+    size_t order_scratch_bytes = 0;
+    // pinned staging for results
+    void* h_stage = nullptr;
+    size_t h_stage_bytes = 0;
+    cudaEvent_t ev[8] = {};
+};
+
+static gi_status set_err(gi_ctx* c, gi_status s, const char* what, cudaError_t e = cudaSuccess)
+{
+    if (c) {
+        char buf[512];
+        if (e != cudaSuccess)
+            snprintf(buf, sizeof buf, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+        else
+            snprintf(buf, sizeof buf, "%s", what);
+        c->last_error = buf;
+    }
+    return s;
+}
+
+#define CK(ctx, x, what)                                                            \
+    do {                                                                            \
+        cudaError_t e_ = (x);                                                       \
+        if (e_ != cudaSuccess) {                                                    \
+            return set_err((ctx), e_ == cudaErrorMemoryAllocation ? GI_ERR_OOM : GI_ERR_CUDA, (what), e_); \
+        }                                                                           \
+    } while (0)
+
+extern "C" const char* gi_status_string(gi_status s)
+{
+    switch (s) {
+        case GI_OK: return "ok";
+        case GI_ERR_INVALID_ARG: return "invalid argument";
+        case GI_ERR_OOM: return "out of memory";
+        case GI_ERR_CAPACITY: return "capacity exceeded";
+        case GI_ERR_TIMEOUT: return "device wait timed out";
+        case GI_ERR_CUDA: return "CUDA error";
+        case GI_ERR_RANGE: return "coordinates outside the supported domain";
+        case GI_ERR_NOT_READY: return "not ready";
+        case GI_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+extern "C" const char* gi_last_error(const gi_ctx* ctx)
+{
+    return ctx ? ctx->last_error.c_str() : "";
+}
+
+extern "C" gi_status gi_device_count(int32_t* n)
+{
+    if (!n) return GI_ERR_INVALID_ARG;
+    int c = 0;
+    cudaError_t e = cudaGetDeviceCount(&c);
+    if (e != cudaSuccess) {
+        *n = 0;
+        return GI_ERR_NO_DEVICE;
+    }
+    *n = c;
+    return GI_OK;
+}
+
+template <class T>
+static cudaError_t grow(T*& p, uint32_t& cap, uint32_t need, cudaStream_t st)
+{
+    if (need <= cap && p) return cudaSuccess;
+    if (p) cudaFreeAsync(p, st);
+    p = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&p, sizeof(T) * (size_t)need, st);
+    if (e == cudaSuccess) cap = need;
+    else cap = 0;
+    return e;
+}
+
+extern "C" gi_status gi_create(const gi_options* opts, gi_ctx** out)
+{
+    if (!out) return GI_ERR_INVALID_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GI_ERR_NO_DEVICE;
+    gi_ctx* c = new (std::nothrow) gi_ctx();
+    if (!c) return GI_ERR_OOM;
+    c->device = opts ? opts->device : 0;
+    c->budget = opts ? opts->hbm_budget_bytes : 0;
+    c->flags = opts ? opts->flags : 0;
+    if (c->device < 0 || c->device >= ndev) {
+        delete c;
+        return GI_ERR_INVALID_ARG;
+    }
+    cudaSetDevice(c->device);
+    cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = query_launch(c->device, &c->cfg);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_cnt, sizeof(Counters));
+    if (e == cudaSuccess) e = cudaMallocHost(&c->h_cnt, sizeof(Counters));
+    for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&c->ev[i]);
+    if (e != cudaSuccess) {
+        gi_destroy(c);
+        return e == cudaErrorMemoryAllocation ? GI_ERR_OOM : GI_ERR_NO_DEVICE;
+    }
+    *out = c;
+    return GI_OK;
+}
+
+extern "C" gi_status gi_destroy(gi_ctx* c)
+{
+    if (!c) return GI_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    if (c->st) cudaStreamSynchronize(c->st);
+    void* dev[] = {c->d_cnt, c->d_jobs, c->front[0], c->front[1], c->cand, c->res, c->esc, c->segs, c->nseg,
+                   c->perm, c->pairs_out, c->job_out, c->segs_out, c->segpair_out, c->seg_off, c->seg_scan_tmp,
+                   c->d_total, c->order_scratch};
+    for (void* p : dev)
+        if (p) cudaFree(p);
+    if (c->h_cnt) cudaFreeHost(c->h_cnt);
+    if (c->h_jobs) cudaFreeHost(c->h_jobs);
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+    return GI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Meshes
+// ---------------------------------------------------------------------------
+static gi_status mesh_finish(gi_ctx* c, gi_mesh* m, gi_mesh** out)
+{
+    unsigned* d_err = nullptr;
+    CK(c, cudaMallocAsync(&d_err, sizeof(unsigned), c->st), "alloc");
+    CK(c, cudaMemsetAsync(d_err, 0, sizeof(unsigned), c->st), "memset");
+    CK(c, launch_validate(m->b.verts, m->b.nv, m->b.tris, m->b.nt, d_err, c->st), "validate");
+    unsigned herr = 0;
+    CK(c, cudaMemcpyAsync(&herr, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st), "copy");
+    CK(c, cudaStreamSynchronize(c->st), "sync");
+    cudaFreeAsync(d_err, c->st);
+    if (herr) {
+        gi_mesh_release(c, m);
+        return set_err(c, (herr & 1u) ? GI_ERR_INVALID_ARG : GI_ERR_RANGE,
+                       (herr & 1u) ? "triangle index out of range" : "vertex coordinate outside the supported domain");
+    }
+    cudaError_t e = build_bvh(m->b, false, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) {
+        gi_mesh_release(c, m);
+        return set_err(c, e == cudaErrorMemoryAllocation ? GI_ERR_OOM : GI_ERR_CUDA, "BVH build", e);
+    }
+    c->mesh_bytes += m->b.bytes;
+    if (c->budget && c->mesh_bytes > c->budget) {
+        gi_mesh_release(c, m);
+        return set_err(c, GI_ERR_OOM, "HBM budget exceeded by mesh upload");
+    }
+    *out = m;
+    return GI_OK;
+}
+
+static gi_status mesh_alloc(gi_ctx* c, uint32_t nv, uint32_t nt, gi_mesh** pm)
+{
+    gi_mesh* m = new (std::nothrow) gi_mesh();
+    if (!m) return GI_ERR_OOM;
+    m->ctx = c;
+    m->b.nv = nv;
+    m->b.nt = nt;
+    size_t vb = sizeof(double) * 3 * (size_t)(nv ? nv : 1), tb = sizeof(uint32_t) * 3 * (size_t)(nt ? nt : 1);
+    if (c->budget && c->mesh_bytes + vb + tb > c->budget) {
+        delete m;
+        return set_err(c, GI_ERR_OOM, "HBM budget exceeded by mesh upload");
+    }
+    cudaError_t e = cudaMallocAsync(&m->b.verts, vb, c->st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&m->b.tris, tb, c->st);
+    if (e != cudaSuccess) {
+        if (m->b.verts) cudaFreeAsync(m->b.verts, c->st);
+        delete m;
+        return set_err(c, GI_ERR_OOM, "mesh allocation", e);
+    }
+    m->b.bytes = vb + tb;
+    *pm = m;
+    return GI_OK;
+}
+
+extern "C" gi_status gi_mesh_upload(gi_ctx* c, const double* verts, uint32_t nv, const uint32_t* tris, uint32_t nt,
+                                    gi_mesh** out)
+{
+    if (!c || !out || (nv && !verts) || (nt && !tris) || nt > 0x7fffffffu) return GI_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    gi_mesh* m = nullptr;
+    gi_status s = mesh_alloc(c, nv, nt, &m);
+    if (s != GI_OK) return s;
+    if (nv) CK(c, cudaMemcpyAsync(m->b.verts, verts, sizeof(double) * 3 * (size_t)nv, cudaMemcpyHostToDevice, c->st),
+               "upload vertices");
+    if (nt) CK(c, cudaMemcpyAsync(m->b.tris, tris, sizeof(uint32_t) * 3 * (size_t)nt, cudaMemcpyHostToDevice, c->st),
+               "upload triangles");
+    return mesh_finish(c, m, out);
+}
+
+extern "C" gi_status gi_mesh_upload_device(gi_ctx* c, const double* d_verts, uint32_t nv, const uint32_t* d_tris,
+                                           uint32_t nt, gi_mesh** out)
+{
+    if (!c || !out || (nv && !d_verts) || (nt && !d_tris) || nt > 0x7fffffffu) return GI_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    gi_mesh* m = nullptr;
+    gi_status s = mesh_alloc(c, nv, nt, &m);
+    if (s != GI_OK) return s;
+    if (nv) CK(c, cudaMemcpyAsync(m->b.verts, d_verts, sizeof(double) * 3 * (size_t)nv, cudaMemcpyDeviceToDevice,
+                                  c->st), "copy vertices");
+    if (nt) CK(c, cudaMemcpyAsync(m->b.tris, d_tris, sizeof(uint32_t) * 3 * (size_t)nt, cudaMemcpyDeviceToDevice,
+                                  c->st), "copy triangles");
+    return mesh_finish(c, m, out);
+}
+
+extern "C" gi_status gi_mesh_release(gi_ctx* c, gi_mesh* m)
+{
+    if (!c || !m || m->ctx != c) return GI_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->st);
+    void* p[] = {m->b.verts, m->b.tris, m->b.leafTri, m->b.leafBox, m->b.nodes, m->b.leafBox64, m->b.nodes64};
+    for (void* q : p)
+        if (q) cudaFree(q);
+    if (m->b.bytes <= c->mesh_bytes) c->mesh_bytes -= m->b.bytes;
+    delete m;
+    return GI_OK;
+}
+
+extern "C" gi_status gi_mesh_info(const gi_mesh* m, uint32_t* nv, uint32_t* nt, uint64_t* nodes, uint64_t* bytes)
+{
+    if (!m) return GI_ERR_INVALID_ARG;
+    if (nv) *nv = m->b.nv;
+    if (nt) *nt = m->b.nt;
+    if (nodes) *nodes = m->b.nnodes;
+    if (bytes) *bytes = m->b.bytes;
+    return GI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Poses (RotationTools.h:28-70)
+// ---------------------------------------------------------------------------
+extern "C" gi_status gi_pose_identity(gi_pose* p)
+{
+    if (!p) return GI_ERR_INVALID_ARG;
+    memset(p, 0, sizeof *p);
+    p->R[0] = p->R[4] = p->R[8] = 1.0;
+    p->identity = 1;
+    return GI_OK;
+}
+
+extern "C" gi_status gi_pose_from_euler_deg(const double rot[3], const double center[3], const double trans[3],
+                                            gi_pose* out)
+{
+    if (!rot || !center || !trans || !out) return GI_ERR_INVALID_ARG;
+    // R = Rz * Ry * Rx (RotationTools.h:28-53), degrees to radians with the same constant
+    volatile double d2r = 3.14159265358979323846 / 180.0;
+    double rx = rot[0] * d2r, ry = rot[1] * d2r, rz = rot[2] * d2r;
+    double cx = cos(rx), sx = sin(rx), cy = cos(ry), sy = sin(ry), cz = cos(rz), sz = sin(rz);
+    memset(out, 0, sizeof *out);
+    out->R[0] = cy * cz;
+    out->R[1] = sx * sy * cz - cx * sz;
+    out->R[2] = cx * sy * cz + sx * sz;
+    out->R[3] = cy * sz;
+    out->R[4] = sx * sy * sz + cx * cz;
+    out->R[5] = cx * sy * sz - sx * cz;
+    out->R[6] = -sy;
+    out->R[7] = sx * cy;
+    out->R[8] = cx * cy;
+    for (int i = 0; i < 3; i++) {
+        out->center[i] = center[i];
+        out->trans[i] = trans[i];
+    }
+    out->identity = (rot[0] == 0.0 && rot[1] == 0.0 && rot[2] == 0.0 && trans[0] == 0.0 && trans[1] == 0.0 &&
+                     trans[2] == 0.0);
+    return GI_OK;
+}
+
+extern "C" gi_status gi_pose_apply(const gi_pose* p, const double* v, uint64_t nv, double* out)
+{
+    if (!p || (nv && (!v || !out))) return GI_ERR_INVALID_ARG;
+    for (uint64_t i = 0; i < nv; i++) {
+        if (p->identity) {
+            out[3 * i] = v[3 * i];
+            out[3 * i + 1] = v[3 * i + 1];
+            out[3 * i + 2] = v[3 * i + 2];
+            continue;
+        }
+        volatile double x = v[3 * i] - p->center[0], y = v[3 * i + 1] - p->center[1], z = v[3 * i + 2] - p->center[2];
+        volatile double t0 = p->R[0] * x, t1 = p->R[1] * y, t2 = p->R[2] * z;
+        volatile double rx = t0 + t1;
+        rx = rx + t2;
+        volatile double u0 = p->R[3] * x, u1 = p->R[4] * y, u2 = p->R[5] * z;
+        volatile double ry = u0 + u1;
+        ry = ry + u2;
+        volatile double w0 = p->R[6] * x, w1 = p->R[7] * y, w2 = p->R[8] * z;
+        volatile double rz = w0 + w1;
+        rz = rz + w2;
+        volatile double ox = rx + p->center[0], oy = ry + p->center[1], oz = rz + p->center[2];
+        out[3 * i] = ox + p->trans[0];
+        out[3 * i + 1] = oy + p->trans[1];
+        out[3 * i + 2] = oz + p->trans[2];
+    }
+    return GI_OK;
+}
+
+static bool pose_ok(const gi_pose& p)
+{
+    if (p.identity) return true;
+    for (double r : p.R)
+        if (!(fabs(r) <= 16.0)) return false;
+    for (int i = 0; i < 3; i++)
+        if (!(fabs(p.center[i]) <= 0x1p90) || !(fabs(p.trans[i]) <= 0x1p90)) return false;
+    return true;
+}
+
+static DevPose make_dev_pose(const gi_pose& p)
+{
+    DevPose d;
+    memset(&d, 0, sizeof d);
+    d.identity = p.identity ? 1 : 0;
+    for (int i = 0; i < 9; i++) d.R[i] = p.identity ? (i % 4 == 0 ? 1.0 : 0.0) : p.R[i];
+    for (int i = 0; i < 3; i++) {
+        d.C[i] = p.identity ? 0.0 : p.center[i];
+        d.T[i] = p.identity ? 0.0 : p.trans[i];
+    }
+    for (int r = 0; r < 3; r++) {
+        double rc = d.R[3 * r] * d.C[0] + d.R[3 * r + 1] * d.C[1] + d.R[3 * r + 2] * d.C[2];
+        d.b64[r] = d.C[r] + d.T[r] - rc;
+        double m = fabs(d.C[r]) + fabs(d.T[r]) + fabs(d.R[3 * r]) * fabs(d.C[0]) +
+                   fabs(d.R[3 * r + 1]) * fabs(d.C[1]) + fabs(d.R[3 * r + 2]) * fabs(d.C[2]);
+        d.padm64[r] = m * (1.0 + 0x1p-40);
+        d.bf[r] = (float)d.b64[r];
+        d.padm[r] = nextafterf((float)d.padm64[r], INFINITY);
+    }
+    for (int i = 0; i < 9; i++) d.Rf[i] = (float)d.R[i];
+    return d;
+}
+
+static MeshDev mesh_dev(const gi_mesh* m)
+{
+    MeshDev d;
+    d.verts = m->b.verts;
+    d.tris = m->b.tris;
+    d.leafTri = m->b.leafTri;
+    d.leafBox = m->b.leafBox;
+    d.leafBox64 = m->b.leafBox64;
+    d.nodes = m->b.nodes;
+    d.nodes64 = m->b.nodes64;
+    d.root = m->b.root;
+    d.nv = m->b.nv;
+    d.nt = m->b.nt;
+    d.nnodes = m->b.nnodes;
+    return d;
+}
+
+extern "C" gi_status gi_intersect_opts_default(gi_intersect_opts* o)
+{
+    if (!o) return GI_ERR_INVALID_ARG;
+    o->want_segments = 1;
+    o->precision_mode = GI_PREC_FP32_CASCADE;
+    o->sort_output = 1;
+    o->reserved = 0;
+    return GI_OK;
+}
+
+static int bits_for(uint64_t n)
+{
+    int b = 1;
+    while ((1ull << b) < n) b++;
+    return b;
+}
+
+static gi_status ensure_fp64(gi_ctx* c, gi_mesh* m)
+{
+    if (m->has64 || m->b.nt == 0) {
+        m->has64 = true;
+        return GI_OK;
+    }
+    cudaError_t e = build_bvh(m->b, true, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) return set_err(c, GI_ERR_CUDA, "FP64 BVH build", e);
+    m->has64 = true;
+    return GI_OK;
+}
+
+static gi_status ensure_pinned(gi_ctx* c, size_t bytes)
+{
+    if (bytes <= c->h_stage_bytes) return GI_OK;
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    c->h_stage = nullptr;
+    size_t want = std::max(bytes, (size_t)1 << 20);
+    if (cudaMallocHost(&c->h_stage, want) != cudaSuccess) {
+        c->h_stage_bytes = 0;
+        return set_err(c, GI_ERR_OOM, "pinned staging");
+    }
+    c->h_stage_bytes = want;
+    return GI_OK;
+}
+
+// Core: runs the job list on the device and fills per-job results.
+static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_intersect_opts& o,
+                          std::vector<gi_result*>& outs)
+{
+    const uint32_t nj = (uint32_t)jobs.size();
+    const int prec = o.precision_mode == GI_PREC_FP64 ? 1 : 0;
+    uint64_t maxA = 1, maxB = 1, sumT = 0;
+    for (const auto& j : jobs) {
+        maxA = std::max<uint64_t>(maxA, j.A.nt);
+        maxB = std::max<uint64_t>(maxB, j.B.nt);
+        sumT += j.A.nt + j.B.nt;
+    }
+    int ba = bits_for(maxA), bb = bits_for(maxB), bj = nj > 1 ? bits_for(nj) : 0;
+    if (ba + bb + bj > 64) return set_err(c, GI_ERR_INVALID_ARG, "batch too large for 64-bit ordering keys");
+    // jobs to the device
+    if (nj > c->cap_jobs) {
+        if (c->d_jobs) cudaFree(c->d_jobs);
+        if (c->h_jobs) cudaFreeHost(c->h_jobs);
+        c->d_jobs = nullptr;
+        c->h_jobs = nullptr;
+        c->cap_jobs = 0;
+        CK(c, cudaMalloc(&c->d_jobs, sizeof(JobDev) * nj), "jobs");
+        CK(c, cudaMallocHost(&c->h_jobs, sizeof(JobDev) * nj), "jobs staging");
+        c->cap_jobs = nj;
+    }
+    memcpy(c->h_jobs, jobs.data(), sizeof(JobDev) * nj);
+    CK(c, cudaMemcpyAsync(c->d_jobs, c->h_jobs, sizeof(JobDev) * nj, cudaMemcpyHostToDevice, c->st), "jobs copy");
+    // initial capacities
+    const bool tiny = (c->flags & GI_FLAG_TINY_BUFFERS) != 0;
+    uint32_t need_front = std::max<uint32_t>(c->cap_front, tiny ? 64u : std::max<uint32_t>(1u << 20, nj * 64u));
+    uint32_t need_cand =
+        std::max<uint32_t>(c->cap_cand, tiny ? 64u : (uint32_t)std::min<uint64_t>(sumT * 2 + 4096, 1u << 22));
+    uint32_t need_res = std::max<uint32_t>(c->cap_res, tiny ? 64u : std::max<uint32_t>(need_cand / 4, 1u << 16));
+    uint32_t need_esc = std::max<uint32_t>(c->cap_esc, tiny ? 64u : std::max<uint32_t>(need_cand / 4, 1u << 16));
+    const unsigned long long launches0 = launch_count();
+    Counters& H = *c->h_cnt;
+    gi_stats st;
+    memset(&st, 0, sizeof st);
+    float ms_trav = 0, ms_exact = 0;
+    int retries = 0;
+    for (;; retries++) {
+        CK(c, grow(c->front[0], c->cap_front, need_front, c->st), "frontier");
+        CK(c, grow(c->front[1], c->cap_front1, need_front, c->st), "frontier");
+        CK(c, grow(c->cand, c->cap_cand, need_cand, c->st), "candidates");
+        CK(c, grow(c->res, c->cap_res, need_res, c->st), "results");
+        CK(c, grow(c->esc, c->cap_esc, need_esc, c->st), "escalations");
+        Bufs b;
+        b.jobs = c->d_jobs;
+        b.njobs = nj;
+        b.front[0] = c->front[0];
+        b.front[1] = c->front[1];
+        b.cap_front = c->cap_front;
+        b.cand = c->cand;
+        b.cap_cand = c->cap_cand;
+        b.res = c->res;
+        b.cap_res = c->cap_res;
+        b.esc = c->esc;
+        b.cap_esc = c->cap_esc;
+        b.cnt = c->d_cnt;
+        b.precision = prec;
+        CK(c, cudaMemsetAsync(c->d_cnt, 0, sizeof(Counters), c->st), "counters");
+        CK(c, launch_init_frontier(b, c->st), "init frontier");
+        CK(c, cudaEventRecord(c->ev[0], c->st), "event");
+        CK(c, launch_traverse(b, c->cfg, prec, c->st), "traverse");
+        CK(c, cudaEventRecord(c->ev[1], c->st), "event");
+        CK(c, launch_exact(b, c->cfg, c->st), "exact stage");
+        CK(c, cudaEventRecord(c->ev[2], c->st), "event");
+        CK(c, cudaMemcpyAsync(c->h_cnt, c->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, c->st), "counters");
+        CK(c, cudaStreamSynchronize(c->st), "sync");
+        if (H.err & kErrBarrier) return set_err(c, GI_ERR_TIMEOUT, "grid barrier wait ran out");
+        if (H.err & kErrExactCapacity) return set_err(c, GI_ERR_RANGE, "exact arithmetic capacity exceeded");
+        if (H.overflow == 0) break;
+        if (retries >= 12) return set_err(c, GI_ERR_CAPACITY, "intersection buffers stayed too small");
+        auto g4 = [](uint32_t cur, uint32_t seen) {
+            uint64_t v = std::max<uint64_t>((uint64_t)cur * 4, (uint64_t)seen + seen / 2 + 1024);
+            return (uint32_t)std::min<uint64_t>(v, 0x7fffffffu);
+        };
+        if (H.overflow & kOvfFrontier) need_front = g4(c->cap_front, c->cap_front);
+        if (H.overflow & kOvfCand) need_cand = g4(c->cap_cand, H.cand);
+        if (H.overflow & (kOvfRes | kOvfCand)) need_res = g4(c->cap_res, H.res);
+        if (H.overflow & (kOvfEsc | kOvfCand)) need_esc = g4(c->cap_esc, H.esc);
+    }
+    cudaEventElapsedTime(&ms_trav, c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&ms_exact, c->ev[1], c->ev[2]);
+    const uint32_t nres = H.res;
+    // output buffers
+    if (nres > c->cap_out) {
+        uint32_t cap = std::max<uint32_t>(nres + nres / 2, 1u << 14);
+        void* old[] = {c->segs, c->nseg, c->perm, c->pairs_out, c->job_out, c->segs_out, c->segpair_out, c->seg_off,
+                       c->seg_scan_tmp, c->d_total};
+        for (void* p : old)
+            if (p) cudaFreeAsync(p, c->st);
+        c->cap_out = 0;
+        CK(c, cudaMallocAsync(&c->segs, sizeof(double) * 18 * (size_t)cap, c->st), "segments");
+        CK(c, cudaMallocAsync(&c->nseg, sizeof(uint32_t) * cap, c->st), "segments");
+        CK(c, cudaMallocAsync(&c->perm, sizeof(uint32_t) * cap, c->st), "order");
+        CK(c, cudaMallocAsync(&c->pairs_out, sizeof(int32_t) * 2 * (size_t)cap, c->st), "pairs");
+        CK(c, cudaMallocAsync(&c->job_out, sizeof(uint32_t) * cap, c->st), "pairs");
+        CK(c, cudaMallocAsync(&c->segs_out, sizeof(double) * 18 * (size_t)cap, c->st), "segments");
+        CK(c, cudaMallocAsync(&c->segpair_out, sizeof(int32_t) * 3 * (size_t)cap, c->st), "segments");
+        CK(c, cudaMallocAsync(&c->seg_off, sizeof(uint32_t) * cap, c->st), "segments");
+        CK(c, cudaMallocAsync(&c->seg_scan_tmp, sizeof(uint32_t) * scan_temp_words_host(cap), c->st), "segments");
+        CK(c, cudaMallocAsync(&c->d_total, sizeof(uint32_t) * 4, c->st), "segments");
+        c->cap_out = cap;
+    }
+    size_t osb = order_scratch_bytes(std::max<uint32_t>(nres, 1));
+    if (osb > c->order_scratch_bytes) {
+        if (c->order_scratch) cudaFreeAsync(c->order_scratch, c->st);
+        c->order_scratch = nullptr;
+        c->order_scratch_bytes = 0;
+        CK(c, cudaMallocAsync(&c->order_scratch, osb * 2, c->st), "order scratch");
+        c->order_scratch_bytes = osb * 2;
+    }
+    Bufs b;
+    b.jobs = c->d_jobs;
+    b.njobs = nj;
+    b.res = c->res;
+    b.cap_res = c->cap_res;
+    b.cnt = c->d_cnt;
+    const bool want_segs = o.want_segments != 0;
+    CK(c, cudaEventRecord(c->ev[3], c->st), "event");
+    if (want_segs && nres) CK(c, launch_segments(b, nres, c->segs, c->nseg, c->cfg, c->st), "segments");
+    CK(c, cudaEventRecord(c->ev[4], c->st), "event");
+    OrderScratch os;
+    os.ptr = c->order_scratch;
+    os.bytes = c->order_scratch_bytes;
+    if (nres) {
+        CK(c, launch_order(c->res, nres, ba, bb, bj, o.sort_output != 0, c->perm, os, c->st), "order");
+        CK(c, launch_gather(c->res, c->perm, nres, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
+                            c->segpair_out, c->seg_off, c->seg_scan_tmp, want_segs, c->d_total, c->st),
+           "gather");
+    }
+    CK(c, cudaEventRecord(c->ev[5], c->st), "event");
+    // copy back: pairs, jobs, total segments
+    size_t pbytes = sizeof(int32_t) * 2 * (size_t)nres, jbytes = sizeof(uint32_t) * (size_t)nres;
+    gi_status s = ensure_pinned(c, pbytes + jbytes + 64);
+    if (s != GI_OK) return s;
+    char* hp = (char*)c->h_stage;
+    uint32_t* htotal = (uint32_t*)(hp + pbytes + jbytes);
+    *htotal = 0;
+    if (nres) {
+        CK(c, cudaMemcpyAsync(hp, c->pairs_out, pbytes, cudaMemcpyDeviceToHost, c->st), "copy pairs");
+        if (nj > 1) CK(c, cudaMemcpyAsync(hp + pbytes, c->job_out, jbytes, cudaMemcpyDeviceToHost, c->st), "copy jobs");
+        if (want_segs)
+            CK(c, cudaMemcpyAsync(htotal, c->d_total, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st), "copy total");
+    }
+    CK(c, cudaStreamSynchronize(c->st), "sync");
+    // counters after the segment stage
+    CK(c, cudaMemcpy(c->h_cnt, c->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost), "counters");
+    if (H.err & kErrExactCapacity) return set_err(c, GI_ERR_RANGE, "exact arithmetic capacity exceeded");
+    float ms_seg = 0, ms_sort = 0, ms_total = 0;
+    cudaEventElapsedTime(&ms_seg, c->ev[3], c->ev[4]);
+    cudaEventElapsedTime(&ms_sort, c->ev[4], c->ev[5]);
+    cudaEventElapsedTime(&ms_total, c->ev[0], c->ev[5]);
+    // split per job
+    std::vector<uint32_t> job_start(nj + 1, 0);
+    if (nj == 1) {
+        job_start[1] = nres;
+    } else {
+        const uint32_t* hj = (const uint32_t*)(hp + pbytes);
+        for (uint32_t k = 0; k < nres; k++) job_start[hj[k] + 1]++;
+        for (uint32_t j = 0; j < nj; j++) job_start[j + 1] += job_start[j];
+    }
+    uint32_t nsegs = want_segs ? *htotal : 0;
+    std::vector<double> hsegs;
+    std::vector<int32_t> hsegpair;
+    if (nsegs) {
+        hsegs.resize(6 * (size_t)nsegs);
+        hsegpair.resize(nsegs);
+        CK(c, cudaMemcpyAsync(hsegs.data(), c->segs_out, sizeof(double) * 6 * nsegs, cudaMemcpyDeviceToHost, c->st),
+           "copy segments");
+        CK(c, cudaMemcpyAsync(hsegpair.data(), c->segpair_out, sizeof(int32_t) * nsegs, cudaMemcpyDeviceToHost, c->st),
+           "copy segments");
+        CK(c, cudaStreamSynchronize(c->st), "sync");
+    }
+    const int32_t* hpairs = (const int32_t*)hp;
+    size_t sp = 0;
+    for (uint32_t j = 0; j < nj; j++) {
+        gi_result* r = new (std::nothrow) gi_result();
+        if (!r) return GI_ERR_OOM;
+        uint32_t a = job_start[j], e = job_start[j + 1];
+        r->pairs.assign(hpairs + 2 * (size_t)a, hpairs + 2 * (size_t)e);
+        while (sp < nsegs && (uint32_t)hsegpair[sp] < e) {
+            r->segs.insert(r->segs.end(), hsegs.begin() + 6 * sp, hsegs.begin() + 6 * sp + 6);
+            r->seg_pair.push_back(hsegpair[sp] - (int32_t)a);
+            sp++;
+        }
+        gi_stats& s2 = r->stats;
+        memset(&s2, 0, sizeof s2);
+        s2.tris_a = jobs[j].A.nt;
+        s2.tris_b = jobs[j].B.nt;
+        s2.nodes_a = jobs[j].A.nnodes;
+        s2.nodes_b = jobs[j].B.nnodes;
+        s2.pairs = e - a;
+        s2.segments = r->seg_pair.size();
+        // launch-wide counters (shared by all jobs of a batch)
+        s2.node_pairs = H.node_pairs;
+        s2.candidates = H.cand;
+        s2.filter_decided = H.filter_decided;
+        s2.escalated = H.esc;
+        s2.exact_signs = H.exact_signs;
+        s2.exact_points = H.exact_points;
+        s2.levels = H.levels;
+        s2.retries = (uint32_t)retries;
+        s2.launches = (uint32_t)(launch_count() - launches0);
+        s2.ms_traverse = ms_trav;
+        s2.ms_exact = ms_exact;
+        s2.ms_segments = ms_seg;
+        s2.ms_sort = ms_sort;
+        s2.ms_total = ms_total;
+        outs[j] = r;
+    }
+    return GI_OK;
+}
+
+extern "C" gi_status gi_intersect(gi_ctx* c, const gi_mesh* A, const gi_pose* pa, const gi_mesh* B, const gi_pose* pb,
+                                  const gi_intersect_opts* opts, gi_result** out)
+{
+    if (!c || !A || !B || !out || A->ctx != c || B->ctx != c) return GI_ERR_INVALID_ARG;
+    gi_pair_job j;
+    j.A = A;
+    j.B = B;
+    if (pa) j.pose_a = *pa;
+    else gi_pose_identity(&j.pose_a);
+    if (pb) j.pose_b = *pb;
+    else gi_pose_identity(&j.pose_b);
+    return gi_intersect_batch(c, &j, 1, opts, out);
+}
+
+extern "C" gi_status gi_intersect_batch(gi_ctx* c, const gi_pair_job* jobs, uint32_t nj, const gi_intersect_opts* opts,
+                                        gi_result** out)
+{
+    if (!c || !jobs || !out || nj == 0) return GI_ERR_INVALID_ARG;
+    gi_intersect_opts o;
+    if (opts) o = *opts;
+    else gi_intersect_opts_default(&o);
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    std::vector<JobDev> jd(nj);
+    for (uint32_t i = 0; i < nj; i++) {
+        const gi_pair_job& j = jobs[i];
+        if (!j.A || !j.B || j.A->ctx != c || j.B->ctx != c) return GI_ERR_INVALID_ARG;
+        if (!pose_ok(j.pose_a) || !pose_ok(j.pose_b)) return set_err(c, GI_ERR_RANGE, "pose outside the supported domain");
+        if (o.precision_mode == GI_PREC_FP64) {
+            gi_status s = ensure_fp64(c, const_cast<gi_mesh*>(j.A));
+            if (s == GI_OK) s = ensure_fp64(c, const_cast<gi_mesh*>(j.B));
+            if (s != GI_OK) return s;
+        }
+        jd[i].A = mesh_dev(j.A);
+        jd[i].B = mesh_dev(j.B);
+        jd[i].pa = make_dev_pose(j.pose_a);
+        jd[i].pb = make_dev_pose(j.pose_b);
+    }
+    std::vector<gi_result*> outs(nj, nullptr);
+    gi_status s = run_jobs(c, jd, o, outs);
+    if (s != GI_OK) {
+        for (auto* r : outs) delete r;
+        return s;
+    }
+    for (uint32_t i = 0; i < nj; i++) out[i] = outs[i];
+    return GI_OK;
+}
+
+extern "C" gi_status gi_intersect_oneshot(gi_ctx* c, const double* vA, uint32_t nvA, const uint32_t* tA, uint32_t ntA,
+                                          const gi_pose* pa, const double* vB, uint32_t nvB, const uint32_t* tB,
+                                          uint32_t ntB, const gi_pose* pb, const gi_intersect_opts* opts,
+                                          gi_result** out)
+{
+    if (!c || !out) return GI_ERR_INVALID_ARG;
+    gi_mesh *A = nullptr, *B = nullptr;
+    gi_status s = gi_mesh_upload(c, vA, nvA, tA, ntA, &A);
+    if (s != GI_OK) return s;
+    s = gi_mesh_upload(c, vB, nvB, tB, ntB, &B);
+    if (s != GI_OK) {
+        gi_mesh_release(c, A);
+        return s;
+    }
+    s = gi_intersect(c, A, pa, B, pb, opts, out);
+    gi_mesh_release(c, A);
+    gi_mesh_release(c, B);
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// Results
+// ---------------------------------------------------------------------------
+extern "C" gi_status gi_result_pairs(const gi_result* r, const int32_t** p, uint64_t* n)
+{
+    if (!r || !p || !n) return GI_ERR_INVALID_ARG;
+    *p = r->pairs.data();
+    *n = r->pairs.size() / 2;
+    return GI_OK;
+}
+extern "C" gi_status gi_result_segments(const gi_result* r, const double** s, const int32_t** sp, uint64_t* n)
+{
+    if (!r || !s || !n) return GI_ERR_INVALID_ARG;
+    *s = r->segs.data();
+    if (sp) *sp = r->seg_pair.data();
+    *n = r->seg_pair.size();
+    return GI_OK;
+}
+extern "C" gi_status gi_result_stats(const gi_result* r, gi_stats* out)
+{
+    if (!r || !out) return GI_ERR_INVALID_ARG;
+    *out = r->stats;
+    return GI_OK;
+}
+extern "C" gi_status gi_result_free(gi_result* r)
+{
+    if (!r) return GI_ERR_INVALID_ARG;
+    delete r;
+    return GI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Serving: a host thread admits pending pose requests into device rounds.
+// ---------------------------------------------------------------------------
+struct gi_server {
+    gi_ctx* ctx = nullptr;
+    gi_server_opts opts;
+    std::mutex mu;
+    std::condition_variable cv, done_cv;
+    struct Req {
+        uint64_t ticket;
+        gi_pair_job job;
+    };
+    std::deque<Req> pending;
+    std::map<uint64_t, gi_result*> done;
+    std::map<uint64_t, gi_status> failed;
+    uint64_t next_ticket = 1;
+    bool stop = false;
+    std::thread worker;
+};
+
+static void server_loop(gi_server* s)
+{
+    for (;;) {
+        std::vector<gi_server::Req> round;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv.wait(lk, [&] { return s->stop || !s->pending.empty(); });
+            if (s->stop && s->pending.empty()) return;
+            uint32_t cap = s->opts.max_inflight ? s->opts.max_inflight : 256;
+            while (!s->pending.empty() && round.size() < cap) {
+                round.push_back(s->pending.front());
+                s->pending.pop_front();
+            }
+        }
+        std::vector<gi_pair_job> jobs(round.size());
+        for (size_t i = 0; i < round.size(); i++) jobs[i] = round[i].job;
+        std::vector<gi_result*> outs(round.size(), nullptr);
+        gi_status st = gi_intersect_batch(s->ctx, jobs.data(), (uint32_t)jobs.size(), &s->opts.opts, outs.data());
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            for (size_t i = 0; i < round.size(); i++) {
+                if (st == GI_OK) s->done[round[i].ticket] = outs[i];
+                else s->failed[round[i].ticket] = st;
+            }
+        }
+        s->done_cv.notify_all();
+    }
+}
+
+extern "C" gi_status gi_server_start(gi_ctx* c, const gi_server_opts* opts, gi_server** out)
+{
+    if (!c || !out) return GI_ERR_INVALID_ARG;
+    gi_server* s = new (std::nothrow) gi_server();
+    if (!s) return GI_ERR_OOM;
+    s->ctx = c;
+    if (opts) s->opts = *opts;
+    else {
+        memset(&s->opts, 0, sizeof s->opts);
+        gi_intersect_opts_default(&s->opts.opts);
+    }
+    s->worker = std::thread(server_loop, s);
+    *out = s;
+    return GI_OK;
+}
+
+extern "C" gi_status gi_server_submit(gi_server* s, const gi_mesh* A, const gi_pose* pa, const gi_mesh* B,
+                                      const gi_pose* pb, uint64_t* ticket)
+{
+    if (!s || !A || !B || !ticket) return GI_ERR_INVALID_ARG;
+    gi_server::Req r;
+    r.job.A = A;
+    r.job.B = B;
+    if (pa) r.job.pose_a = *pa;
+    else gi_pose_identity(&r.job.pose_a);
+    if (pb) r.job.pose_b = *pb;
+    else gi_pose_identity(&r.job.pose_b);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stop) return GI_ERR_INVALID_ARG;
+        r.ticket = s->next_ticket++;
+        s->pending.push_back(r);
+        *ticket = r.ticket;
+    }
+    s->cv.notify_one();
+    return GI_OK;
+}
+
+extern "C" gi_status gi_server_poll(gi_server* s, uint64_t ticket, gi_result** out)
+{
+    if (!s || !out) return GI_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->done.find(ticket);
+    if (it != s->done.end()) {
+        *out = it->second;
+        s->done.erase(it);
+        return GI_OK;
+    }
+    auto f = s->failed.find(ticket);
+    if (f != s->failed.end()) {
+        gi_status st = f->second;
+        s->failed.erase(f);
+        return st;
+    }
+    return GI_ERR_NOT_READY;
+}
+
+extern "C" gi_status gi_server_wait(gi_server* s, uint64_t ticket, uint32_t timeout_ms, gi_result** out)
+{
+    if (!s || !out) return GI_ERR_INVALID_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto ready = [&] { return s->done.count(ticket) || s->failed.count(ticket); };
+    if (!s->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) return GI_ERR_TIMEOUT;
+    auto it = s->done.find(ticket);
+    if (it != s->done.end()) {
+        *out = it->second;
+        s->done.erase(it);
+        return GI_OK;
+    }
+    gi_status st = s->failed[ticket];
+    s->failed.erase(ticket);
+    return st;
+}
+
+extern "C" gi_status gi_server_stop(gi_server* s)
+{
+    if (!s) return GI_ERR_INVALID_ARG;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    for (auto& kv : s->done) delete kv.second;
+    delete s;
+    return GI_OK;
+}

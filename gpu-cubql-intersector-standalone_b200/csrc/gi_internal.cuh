@@ -1,0 +1,102 @@
+// gi_internal.cuh -- device-side data layout shared by the kernels of libgi.
+//
+// HBM layout of one resident mesh (built once by gi_mesh_upload):
+//   verts     double[3*nv]            input vertices (mesh-local frame)
+//   tris      uint32[3*nt]            input triangles (original order)
+//   leafTri   uint4[nt]               per Morton-sorted leaf: v0, v1, v2, original id
+//   leafBox   float[6*nt]             per sorted leaf: FP32 box rounded outward
+//   nodes     WNode[nnodes]           4-wide BVH, 128 B per node (one cache line)
+//   leafBox64 / nodes64               FP64 copies for the plain-FP64 form (built lazily)
+// Traversal runs in the world frame: node boxes are mapped through the pose on
+// the fly (conservatively), so a new pose needs no rebuild or refit.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gi {
+
+constexpr uint32_t kLeaf = 0x80000000u;   // child ref: sorted leaf position
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;  // unused child slot
+
+// 4-wide BVH node: child boxes in SoA so that lane i of a quad reads child i.
+struct __align__(128) WNode {
+    float lox[4], loy[4], loz[4], hix[4], hiy[4], hiz[4];
+    uint32_t child[4];
+    uint32_t pad[4];
+};
+static_assert(sizeof(WNode) == 128, "WNode is one 128-byte line");
+
+struct __align__(256) WNode64 {
+    double lox[4], loy[4], loz[4], hix[4], hiy[4], hiz[4];
+    uint32_t child[4];
+    uint32_t pad[12];
+};
+static_assert(sizeof(WNode64) == 256, "WNode64 is two 128-byte lines");
+
+// Pose on the device.
+//  exact vertex map: world = ((R*(v - C)) + C) + T in FP64, left to right, no FMA
+//  box map (FP32):  world = Rf*v + bf, padded by rho*(|Rf|(|c|+h) + padm)
+struct DevPose {
+    double R[9], C[3], T[3];
+    double b64[3];     // C + T - R*C (FP64), for FP64 node boxes
+    double padm64[3];  // |C| + |T| + |R||C| (FP64), magnitude term of the pad
+    float Rf[9], bf[3], padm[3];
+    int identity;
+    int pad_[3];
+};
+
+struct MeshDev {
+    const double* verts;
+    const uint32_t* tris;
+    const uint4* leafTri;
+    const float* leafBox;
+    const double* leafBox64;
+    const WNode* nodes;
+    const WNode64* nodes64;
+    uint32_t root;  // wide node index, or kLeaf | leaf position when nt == 1
+    uint32_t nv, nt, nnodes;
+};
+
+struct JobDev {
+    MeshDev A, B;
+    DevPose pa, pb;
+};
+
+// Device counters of one intersect launch sequence (zeroed by the host).
+struct Counters {
+    unsigned int front[3];  // rotating frontier counts
+    unsigned int cand;      // candidate leaf pairs
+    unsigned int res;       // intersecting pairs
+    unsigned int esc;       // escalated candidate indices
+    unsigned int overflow;  // kOvf* bits
+    unsigned int err;       // kErr* bits
+    unsigned int levels;
+    unsigned int bar_count;
+    unsigned int bar_gen;
+    unsigned int nseg;      // total segments after ordering
+    unsigned long long node_pairs;
+    unsigned long long filter_decided;
+    unsigned long long exact_signs;
+    unsigned long long exact_points;
+};
+
+constexpr unsigned kOvfFrontier = 1u, kOvfCand = 2u, kOvfRes = 4u, kOvfEsc = 8u;
+constexpr unsigned kErrBarrier = 1u, kErrExactCapacity = 2u;
+
+// Per-call buffers handed to the kernels.
+struct Bufs {
+    const JobDev* jobs;
+    uint32_t njobs;
+    uint4* front[2];
+    uint32_t cap_front;
+    uint4* cand;     // job, leaf posA, leaf posB, 0
+    uint32_t cap_cand;
+    uint4* res;      // job, triA, triB, 0   (original triangle ids)
+    uint32_t cap_res;
+    uint32_t* esc;   // candidate index
+    uint32_t cap_esc;
+    Counters* cnt;
+    int precision;   // 0 FP32 cascade, 1 FP64
+};
+
+}  // namespace gi

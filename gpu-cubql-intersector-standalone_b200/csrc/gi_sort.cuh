@@ -1,0 +1,223 @@
+// gi_sort.cuh -- device scan and LSD radix sort (8-bit digits, stable).
+//
+// Used by the BVH build (30-bit Morton keys, replaces the reference's CUB
+// DeviceRadixSort in include/third-party/cubql/level_cut_builder.h:345-347)
+// and by output ordering (64-bit (job, a, b) keys).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gi {
+
+// counts kernel launches made by this library (for gi_stats.launches)
+void note_launches(unsigned n);
+
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+// block-wide exclusive scan of per-thread sums; returns the block total
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* smem_warp, uint32_t* total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) smem_warp[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t w = lane < nw ? smem_warp[lane] : 0u;
+        uint32_t s = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < nw) smem_warp[lane] = s - w;
+        if (lane == nw - 1) smem_warp[32] = s;
+    }
+    __syncthreads();
+    uint32_t r = smem_warp[wid] + x - v;
+    *total = smem_warp[32];
+    __syncthreads();
+    return r;
+}
+
+__global__ void k_scan_tiles(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tile_sums)
+{
+    __shared__ uint32_t sw[33];
+    uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        v[k] = (base + k < n) ? in[base + k] : 0u;
+        s += v[k];
+    }
+    uint32_t tot;
+    uint32_t ex = block_exclusive_scan(s, sw, &tot);
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        if (base + k < n) out[base + k] = ex;
+        ex += v[k];
+    }
+    if (threadIdx.x == 0 && tile_sums) tile_sums[blockIdx.x] = tot;
+}
+
+__global__ void k_scan_add(uint32_t* out, uint32_t n, const uint32_t* tile_offsets)
+{
+    uint32_t add = tile_offsets[blockIdx.x];
+    uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++)
+        if (base + k < n) out[base + k] += add;
+}
+
+// exclusive scan of n uint32 (in and out may alias); temp needs scan_temp_words(n)
+inline size_t scan_temp_words(size_t n)
+{
+    size_t t = 0;
+    while (n > (size_t)kScanTile) {
+        n = (n + kScanTile - 1) / kScanTile;
+        t += n + 1;
+    }
+    return t + 1;
+}
+inline void scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* temp, cudaStream_t st)
+{
+    if (n == 0) return;
+    uint32_t tiles = (n + kScanTile - 1) / kScanTile;
+    if (tiles == 1) {
+        k_scan_tiles<<<1, kScanThreads, 0, st>>>(in, out, n, nullptr);
+        note_launches(1);
+        return;
+    }
+    uint32_t* sums = temp;
+    k_scan_tiles<<<tiles, kScanThreads, 0, st>>>(in, out, n, sums);
+    scan_exclusive(sums, sums, tiles, temp + tiles + 1, st);
+    k_scan_add<<<tiles, kScanThreads, 0, st>>>(out, n, sums);
+    note_launches(2);
+}
+
+// ---------------------------------------------------------------------------
+// Radix sort
+// ---------------------------------------------------------------------------
+constexpr int kRsThreads = 256;
+constexpr int kRsItems = 16;
+constexpr int kRsTile = kRsThreads * kRsItems;  // 4096
+constexpr int kRsWarps = kRsThreads / 32;
+
+template <class K>
+__global__ void __launch_bounds__(kRsThreads) k_rs_hist(const K* __restrict__ keys, uint32_t n, int shift,
+                                                        uint32_t* __restrict__ counts, uint32_t ntiles)
+{
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    uint32_t base = blockIdx.x * kRsTile;
+#pragma unroll 4
+    for (int k = 0; k < kRsItems; k++) {
+        uint32_t i = base + k * kRsThreads + threadIdx.x;
+        if (i < n) atomicAdd(&h[(uint32_t)(keys[i] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    counts[threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+template <class K>
+__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                           K* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t n,
+                                                           int shift, const uint32_t* __restrict__ offsets,
+                                                           uint32_t ntiles)
+{
+    __shared__ uint32_t wc[kRsWarps][256];
+    __shared__ uint32_t tile_off[256];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int d = lane; d < 256; d += 32) wc[w][d] = 0;
+    tile_off[threadIdx.x] = offsets[threadIdx.x * ntiles + blockIdx.x];
+    __syncwarp();
+    const uint32_t seg = blockIdx.x * kRsTile + w * 32 * kRsItems;
+    K key[kRsItems];
+    uint32_t val[kRsItems];
+    uint32_t rank[kRsItems];
+    uint32_t dig[kRsItems];
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int c = 0; c < kRsItems; c++) {
+        uint32_t i = seg + c * 32 + lane;
+        bool ok = i < n;
+        key[c] = ok ? kin[i] : (K)0;
+        val[c] = ok ? vin[i] : 0u;
+        uint32_t d = ok ? ((uint32_t)(key[c] >> shift) & 255u) : 256u;
+        dig[c] = d;
+        unsigned peers = __match_any_sync(0xffffffffu, d);
+        uint32_t r = 0;
+        if (ok) r = wc[w][d] + __popc(peers & lt);
+        rank[c] = r;
+        __syncwarp();
+        if (ok && (peers & lt) == 0) wc[w][d] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // per digit: exclusive prefix over warps
+    {
+        uint32_t d = threadIdx.x;
+        uint32_t run = 0;
+        for (int q = 0; q < kRsWarps; q++) {
+            uint32_t t = wc[q][d];
+            wc[q][d] = run;
+            run += t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < kRsItems; c++) {
+        uint32_t d = dig[c];
+        if (d < 256u) {
+            uint32_t pos = tile_off[d] + wc[w][d] + rank[c];
+            kout[pos] = key[c];
+            vout[pos] = val[c];
+        }
+    }
+}
+
+// Sorts (keys, vals) by the low `bits` bits of the key; result ends in (k0, v0).
+// Scratch: k1/v1 the same size, counts 256*ntiles words, scan temp.
+template <class K>
+void radix_sort(K* k0, uint32_t* v0, K* k1, uint32_t* v1, uint32_t n, int bits, uint32_t* counts, uint32_t* temp,
+                cudaStream_t st)
+{
+    if (n <= 1) return;
+    uint32_t ntiles = (n + kRsTile - 1) / kRsTile;
+    int passes = (bits + 7) / 8;
+    K* ks = k0;
+    uint32_t* vs = v0;
+    K* kd = k1;
+    uint32_t* vd = v1;
+    for (int p = 0; p < passes; p++) {
+        k_rs_hist<K><<<ntiles, kRsThreads, 0, st>>>(ks, n, 8 * p, counts, ntiles);
+        scan_exclusive(counts, counts, 256u * ntiles, temp, st);
+        k_rs_scatter<K><<<ntiles, kRsThreads, 0, st>>>(ks, vs, kd, vd, n, 8 * p, counts, ntiles);
+        note_launches(2);
+        K* tk = ks;
+        ks = kd;
+        kd = tk;
+        uint32_t* tv = vs;
+        vs = vd;
+        vd = tv;
+    }
+    if (ks != k0) {
+        cudaMemcpyAsync(k0, ks, sizeof(K) * n, cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(v0, vs, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st);
+    }
+}
+
+inline size_t radix_counts_words(uint32_t n)
+{
+    return 256ull * ((n + kRsTile - 1) / kRsTile);
+}
+
+}  // namespace gi

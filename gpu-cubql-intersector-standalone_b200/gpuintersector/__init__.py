@@ -1,0 +1,392 @@
+"""Python host mirror of the reference's GPUIntersector interface over libgi.so.
+
+The compute path is the CUDA library behind the C ABI (include/gi/gi.h); this
+module only marshals arrays and handles.  It mirrors, with the same names and
+argument meaning (reference project paths):
+
+  KernelBVHController          src/GPUIntersector/KernelBVHController.h:36-95
+    construct / setTransformBoth / runIntersectionPipeline / clearGPU /
+    reconstructGPU / getCenterA / getCenterB / isGPUAllocated
+  run_grid_forest_intersection_pipeline
+                               src/GPUIntersector/StandaloneBVHPipeline.h:27-43
+  compute_exact_intersection_curves
+                               src/CPU/MeshIntersectionCurves.h:24-29
+
+If libgi.so is missing or no CUDA device is present the calls raise; nothing
+falls back to a CPU implementation.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _abi
+from ._abi import GI_PREC_FP32_CASCADE, GI_PREC_FP64
+
+__all__ = ["GIError", "Context", "Mesh", "Result", "pose_identity", "pose_from_euler_deg", "pose_raw",
+           "KernelBVHController", "run_grid_forest_intersection_pipeline", "compute_exact_intersection_curves",
+           "GI_PREC_FP32_CASCADE", "GI_PREC_FP64", "lib"]
+
+
+class GIError(RuntimeError):
+    def __init__(self, status, msg=""):
+        self.status = status
+        super().__init__("gi status %d (%s)%s" % (status, _status_name(status), (": " + msg) if msg else ""))
+
+
+def _status_name(s):
+    try:
+        return lib().gi_status_string(s).decode()
+    except Exception:
+        return "?"
+
+
+def lib():
+    return _abi.load()
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _up(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+
+
+# ---------------------------------------------------------------- poses
+def pose_identity():
+    p = _abi.Pose()
+    lib().gi_pose_identity(ctypes.byref(p))
+    return p
+
+
+def pose_from_euler_deg(rot_deg, center=(0.0, 0.0, 0.0), trans=(0.0, 0.0, 0.0)):
+    """R = Rz*Ry*Rx from degrees about `center`, then `trans` (RotationTools.h:28-70)."""
+    p = _abi.Pose()
+    r = np.ascontiguousarray(rot_deg, dtype=np.float64)
+    c = np.ascontiguousarray(center, dtype=np.float64)
+    t = np.ascontiguousarray(trans, dtype=np.float64)
+    rc = lib().gi_pose_from_euler_deg(_dp(r), _dp(c), _dp(t), ctypes.byref(p))
+    if rc:
+        raise GIError(rc)
+    return p
+
+
+def pose_raw(R, center=(0.0, 0.0, 0.0), trans=(0.0, 0.0, 0.0)):
+    """General pose world = R (v - center) + center + trans (R row-major 3x3)."""
+    p = _abi.Pose()
+    R = np.asarray(R, dtype=np.float64).reshape(9)
+    for i in range(9):
+        p.R[i] = float(R[i])
+    for i in range(3):
+        p.center[i] = float(center[i])
+        p.trans[i] = float(trans[i])
+    p.identity = 0
+    return p
+
+
+def pose_apply(pose, verts):
+    v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 3)
+    out = np.empty_like(v)
+    rc = lib().gi_pose_apply(ctypes.byref(pose), _dp(v), v.shape[0], _dp(out))
+    if rc:
+        raise GIError(rc)
+    return out
+
+
+# ---------------------------------------------------------------- handles
+class Context:
+    """Owns one CUDA stream and the scratch buffers of the intersector."""
+
+    def __init__(self, device=0, hbm_budget_bytes=0, flags=0):
+        self._lib = lib()
+        o = _abi.Options(device, flags, hbm_budget_bytes)
+        h = ctypes.c_void_p()
+        rc = self._lib.gi_create(ctypes.byref(o), ctypes.byref(h))
+        if rc:
+            raise GIError(rc, "gi_create")
+        self.handle = h
+
+    def check(self, rc, what=""):
+        if rc:
+            msg = self._lib.gi_last_error(self.handle).decode(errors="replace")
+            raise GIError(rc, "%s %s" % (what, msg))
+
+    def close(self):
+        if self.handle:
+            self._lib.gi_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # meshes
+    def upload(self, verts, tris):
+        return Mesh(self, verts, tris)
+
+    def upload_device(self, d_verts_ptr, nv, d_tris_ptr, nt):
+        """Mesh from device pointers (e.g. torch tensor .data_ptr()) on the context's device."""
+        return Mesh(self, None, None, device_ptrs=(d_verts_ptr, nv, d_tris_ptr, nt))
+
+    # intersection
+    @staticmethod
+    def _opts(want_segments=True, precision=GI_PREC_FP32_CASCADE, sort_output=True):
+        o = _abi.IntersectOpts()
+        lib().gi_intersect_opts_default(ctypes.byref(o))
+        o.want_segments = 1 if want_segments else 0
+        o.precision_mode = int(precision)
+        o.sort_output = 1 if sort_output else 0
+        return o
+
+    def intersect(self, A, B, pose_a=None, pose_b=None, want_segments=True, precision=GI_PREC_FP32_CASCADE,
+                  sort_output=True):
+        o = self._opts(want_segments, precision, sort_output)
+        r = ctypes.c_void_p()
+        rc = self._lib.gi_intersect(self.handle, A.handle, ctypes.byref(pose_a) if pose_a is not None else None,
+                                    B.handle, ctypes.byref(pose_b) if pose_b is not None else None,
+                                    ctypes.byref(o), ctypes.byref(r))
+        self.check(rc, "gi_intersect")
+        return Result(r)
+
+    def intersect_batch(self, jobs, want_segments=True, precision=GI_PREC_FP32_CASCADE, sort_output=True):
+        """jobs: list of (A, pose_a, B, pose_b); returns a list of Result."""
+        n = len(jobs)
+        arr = (_abi.PairJob * n)()
+        for i, (A, pa, B, pb) in enumerate(jobs):
+            arr[i].A = A.handle
+            arr[i].B = B.handle
+            arr[i].pose_a = pa if pa is not None else pose_identity()
+            arr[i].pose_b = pb if pb is not None else pose_identity()
+        outs = (ctypes.c_void_p * n)()
+        o = self._opts(want_segments, precision, sort_output)
+        rc = self._lib.gi_intersect_batch(self.handle, arr, n, ctypes.byref(o), outs)
+        self.check(rc, "gi_intersect_batch")
+        return [Result(ctypes.c_void_p(outs[i])) for i in range(n)]
+
+    def intersect_oneshot(self, vA, tA, vB, tB, pose_a=None, pose_b=None, want_segments=True,
+                          precision=GI_PREC_FP32_CASCADE, sort_output=True):
+        vA = np.ascontiguousarray(vA, dtype=np.float64).reshape(-1, 3)
+        vB = np.ascontiguousarray(vB, dtype=np.float64).reshape(-1, 3)
+        tA = np.ascontiguousarray(tA, dtype=np.uint32).reshape(-1, 3)
+        tB = np.ascontiguousarray(tB, dtype=np.uint32).reshape(-1, 3)
+        o = self._opts(want_segments, precision, sort_output)
+        r = ctypes.c_void_p()
+        rc = self._lib.gi_intersect_oneshot(self.handle, _dp(vA), vA.shape[0], _up(tA), tA.shape[0],
+                                            ctypes.byref(pose_a) if pose_a is not None else None,
+                                            _dp(vB), vB.shape[0], _up(tB), tB.shape[0],
+                                            ctypes.byref(pose_b) if pose_b is not None else None,
+                                            ctypes.byref(o), ctypes.byref(r))
+        self.check(rc, "gi_intersect_oneshot")
+        return Result(r)
+
+    def server(self, max_inflight=256, want_segments=True, precision=GI_PREC_FP32_CASCADE):
+        return Server(self, max_inflight, want_segments, precision)
+
+
+class Mesh:
+    def __init__(self, ctx, verts, tris, device_ptrs=None):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        if device_ptrs is not None:
+            dv, nv, dt, nt = device_ptrs
+            rc = ctx._lib.gi_mesh_upload_device(ctx.handle, ctypes.c_void_p(dv), nv, ctypes.c_void_p(dt), nt,
+                                                ctypes.byref(h))
+        else:
+            v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 3)
+            t = np.ascontiguousarray(tris, dtype=np.uint32).reshape(-1, 3)
+            rc = ctx._lib.gi_mesh_upload(ctx.handle, _dp(v), v.shape[0], _up(t), t.shape[0], ctypes.byref(h))
+        ctx.check(rc, "gi_mesh_upload")
+        self.handle = h
+
+    def info(self):
+        nv, nt = ctypes.c_uint32(), ctypes.c_uint32()
+        nodes, nbytes = ctypes.c_uint64(), ctypes.c_uint64()
+        self.ctx._lib.gi_mesh_info(self.handle, ctypes.byref(nv), ctypes.byref(nt), ctypes.byref(nodes),
+                                   ctypes.byref(nbytes))
+        return dict(nv=nv.value, nt=nt.value, nodes=nodes.value, bytes=nbytes.value)
+
+    def release(self):
+        if self.handle and self.ctx.handle:
+            self.ctx._lib.gi_mesh_release(self.ctx.handle, self.handle)
+        self.handle = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+class Result:
+    """Pairs (n, 2) int32 sorted by (a, b); segments (m, 6) float64; seg_pair (m,)."""
+
+    def __init__(self, handle):
+        L = lib()
+        p = ctypes.POINTER(ctypes.c_int32)()
+        n = ctypes.c_uint64()
+        L.gi_result_pairs(handle, ctypes.byref(p), ctypes.byref(n))
+        self.pairs = (np.ctypeslib.as_array(p, shape=(n.value * 2,)).reshape(-1, 2).copy()
+                      if n.value else np.zeros((0, 2), dtype=np.int32))
+        sp = ctypes.POINTER(ctypes.c_double)()
+        spp = ctypes.POINTER(ctypes.c_int32)()
+        m = ctypes.c_uint64()
+        L.gi_result_segments(handle, ctypes.byref(sp), ctypes.byref(spp), ctypes.byref(m))
+        if m.value:
+            self.segments = np.ctypeslib.as_array(sp, shape=(m.value * 6,)).reshape(-1, 6).copy()
+            self.seg_pair = np.ctypeslib.as_array(spp, shape=(m.value,)).copy()
+        else:
+            self.segments = np.zeros((0, 6))
+            self.seg_pair = np.zeros((0,), dtype=np.int32)
+        st = _abi.Stats()
+        L.gi_result_stats(handle, ctypes.byref(st))
+        self.stats = st.as_dict()
+        L.gi_result_free(handle)
+
+
+class Server:
+    """Pose-update serving loop with continuous batching (gi_server_*)."""
+
+    def __init__(self, ctx, max_inflight, want_segments, precision):
+        self.ctx = ctx
+        o = _abi.ServerOpts()
+        o.max_inflight = max_inflight
+        o.opts = Context._opts(want_segments, precision, True)
+        h = ctypes.c_void_p()
+        ctx.check(ctx._lib.gi_server_start(ctx.handle, ctypes.byref(o), ctypes.byref(h)), "gi_server_start")
+        self.handle = h
+
+    def submit(self, A, pose_a, B, pose_b):
+        t = ctypes.c_uint64()
+        self.ctx.check(self.ctx._lib.gi_server_submit(self.handle, A.handle,
+                                                      ctypes.byref(pose_a) if pose_a is not None else None,
+                                                      B.handle, ctypes.byref(pose_b) if pose_b is not None else None,
+                                                      ctypes.byref(t)), "gi_server_submit")
+        return t.value
+
+    def poll(self, ticket):
+        r = ctypes.c_void_p()
+        rc = self.ctx._lib.gi_server_poll(self.handle, ticket, ctypes.byref(r))
+        if rc == _abi.GI_ERR_NOT_READY:
+            return None
+        self.ctx.check(rc, "gi_server_poll")
+        return Result(r)
+
+    def wait(self, ticket, timeout_ms=60000):
+        r = ctypes.c_void_p()
+        rc = self.ctx._lib.gi_server_wait(self.handle, ticket, timeout_ms, ctypes.byref(r))
+        self.ctx.check(rc, "gi_server_wait")
+        return Result(r)
+
+    def stop(self):
+        if self.handle:
+            self.ctx._lib.gi_server_stop(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- reference-shaped mirrors
+class KernelBVHController:
+    """Mirror of the reference class (KernelBVHController.h:36-95).
+
+    construct(...) uploads both meshes and builds their BVHs once; the level /
+    leafThreshold arguments of the reference's level-cut builder are accepted
+    and not needed (the LBVH has no level cut).  setTransformBoth stores the
+    Euler poses about the stored centres; runIntersectionPipeline intersects
+    under them on the device and returns the (faceA, faceB) pairs as an
+    (n, 2) int32 array (the reference returns a malloc'd int2*)."""
+
+    def __init__(self, device=0):
+        self.ctx = Context(device)
+        self.A = self.B = None
+        self.centerA = np.zeros(3)
+        self.centerB = np.zeros(3)
+        self.rotA = np.zeros(3)
+        self.transA = np.zeros(3)
+        self.rotB = np.zeros(3)
+        self.transB = np.zeros(3)
+        self._host = None
+        self.last_stats = None
+
+    def construct(self, vertsA, trisA, levelA, vertsB, trisB, levelB, leafThreshold=4, centerA=None,
+                  centerB=None):
+        self._host = (np.array(vertsA, dtype=np.float64), np.array(trisA, dtype=np.uint32),
+                      np.array(vertsB, dtype=np.float64), np.array(trisB, dtype=np.uint32))
+        self.clearGPU()
+        self.A = self.ctx.upload(self._host[0], self._host[1])
+        self.B = self.ctx.upload(self._host[2], self._host[3])
+        if centerA is not None:
+            self.centerA = np.asarray(centerA, dtype=np.float64)
+        if centerB is not None:
+            self.centerB = np.asarray(centerB, dtype=np.float64)
+
+    def setTransformBoth(self, rotDegA, transA, rotDegB, transB):
+        self.rotA, self.transA = np.asarray(rotDegA, float), np.asarray(transA, float)
+        self.rotB, self.transB = np.asarray(rotDegB, float), np.asarray(transB, float)
+
+    def poses(self):
+        return (pose_from_euler_deg(self.rotA, self.centerA, self.transA),
+                pose_from_euler_deg(self.rotB, self.centerB, self.transB))
+
+    def runIntersectionPipeline(self, batchMultiplier=1, numberOfDualTreeSteps=0, activateAsyncDownload=0,
+                                gpuDouble=1, want_segments=False):
+        pa, pb = self.poses()
+        r = self.ctx.intersect(self.A, self.B, pa, pb, want_segments=want_segments)
+        self.last_stats = r.stats
+        self.last_result = r
+        return r.pairs
+
+    def clearGPU(self):
+        for m in (self.A, self.B):
+            if m is not None:
+                m.release()
+        self.A = self.B = None
+
+    def reconstructGPU(self):
+        if self._host is not None:
+            self.A = self.ctx.upload(self._host[0], self._host[1])
+            self.B = self.ctx.upload(self._host[2], self._host[3])
+
+    def cleanup(self):
+        self.clearGPU()
+
+    def getCenterA(self):
+        return self.centerA
+
+    def getCenterB(self):
+        return self.centerB
+
+    def isGPUAllocated(self):
+        return self.A is not None and self.B is not None
+
+
+def run_grid_forest_intersection_pipeline(vertsA, trisA, vertsB, trisB, centerA=(0, 0, 0), centerB=(0, 0, 0),
+                                          rotA=(0, 0, 0), transA=(0, 0, 0), rotB=(0, 0, 0), transB=(0, 0, 0),
+                                          ctx=None, want_segments=False):
+    """One-shot path (StandaloneBVHPipeline.h:27-43): upload, build, intersect, release."""
+    own = ctx is None
+    ctx = ctx or Context()
+    try:
+        r = ctx.intersect_oneshot(vertsA, trisA, vertsB, trisB, pose_from_euler_deg(rotA, centerA, transA),
+                                  pose_from_euler_deg(rotB, centerB, transB), want_segments=want_segments)
+    finally:
+        if own:
+            ctx.close()
+    return r
+
+
+def compute_exact_intersection_curves(ctx, A, B, pose_a=None, pose_b=None):
+    """Segments of the intersecting pairs (MeshIntersectionCurves.h:24-29), on the device."""
+    return ctx.intersect(A, B, pose_a, pose_b, want_segments=True).segments

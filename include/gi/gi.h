@@ -1,0 +1,204 @@
+/*
+ * gi.h -- C ABI of the B200 mesh-mesh intersector.
+ *
+ * Plain C: opaque handles, POD structs, pointers and sizes, status codes.
+ * Every entry point returns gi_status; nothing exits the process.
+ *
+ * Each entry point replaces a piece of the reference's GPUIntersector
+ * interface (YuryUoL/gpu-cubql-intersector-standalone, paths in that project):
+ *
+ *   KernelBVHController (src/GPUIntersector/KernelBVHController.h:36-95)
+ *     constructor / cleanup() / ~KernelBVHController   -> gi_create, gi_destroy
+ *     construct(...)            (KernelBVHController.h:46-57, .cu:444-597)
+ *                               -> gi_mesh_upload (once per mesh; the library
+ *                                  copies the arrays and builds the BVH)
+ *     setTransformBoth(...)     (KernelBVHController.h:72-77, .cu:289-412)
+ *                               -> gi_pose_from_euler_deg (+ the poses passed
+ *                                  to gi_intersect; no refit is needed)
+ *     runIntersectionPipeline(...) (KernelBVHController.h:60-63, .cu:603-699)
+ *                               -> gi_intersect + gi_result_pairs / _stats
+ *     clearGPU / reconstructGPU (KernelBVHController.h:66-69)
+ *                               -> gi_mesh_release / gi_mesh_upload
+ *   runGridForestIntersectionPipeline (src/GPUIntersector/StandaloneBVHPipeline.h:27-43)
+ *                               -> gi_intersect_oneshot
+ *   computeExactIntersectionCurves (src/CPU/MeshIntersectionCurves.h:24-29)
+ *                               -> gi_intersect with want_segments = 1,
+ *                                  gi_result_segments
+ *   ExecutionStats / IntersectionTimeTracker (src/common/ExecutionStats.h:12-46,
+ *     src/common/IntersectionTimeTracker.h:6-43)  -> gi_stats
+ *
+ * Semantics: a pair (a, b) is reported iff the closed triangles A[a] and B[b],
+ * after applying their poses in FP64 (world = R*(v - C) + C + T, evaluated left
+ * to right without fused multiply-add, as src/CPU/RotationTools.h:129-145),
+ * share at least one point.  The decision is exact.  Segments follow
+ * src/CPU/MeshIntersectionCurves.cpp:63-78: a crossing segment gives one
+ * segment, a single touching point gives a zero-length segment, a coplanar
+ * overlap that is a triangle gives its three edges, and a coplanar overlap
+ * polygon with four or more corners gives none.  Segment endpoints are the
+ * exact intersection points correctly rounded to FP64.
+ *
+ * Supported coordinate domain (exactness guarantee): finite doubles with
+ * |x| <= 2^100 and x == 0 or |x| >= 2^-100, for input vertices, pose entries and posed
+ * vertices alike.  gi_mesh_upload rejects inputs outside it (GI_ERR_RANGE).
+ *
+ * Threading: one gi_ctx owns one CUDA stream; calls on the same context are
+ * serialised by the caller.  Different contexts may run concurrently.
+ */
+#ifndef GI_GI_H
+#define GI_GI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GI_ABI_VERSION 1
+
+typedef enum {
+    GI_OK = 0,
+    GI_ERR_INVALID_ARG = 1, /* null pointer, bad index, bad size */
+    GI_ERR_OOM = 2,         /* device or host allocation failed, or HBM budget exceeded */
+    GI_ERR_CAPACITY = 3,    /* an internal buffer stayed too small after the retries */
+    GI_ERR_TIMEOUT = 4,     /* a bounded device wait ran out (reported, never hung) */
+    GI_ERR_CUDA = 5,        /* CUDA runtime error (see gi_last_error) */
+    GI_ERR_RANGE = 6,       /* coordinates outside the supported domain */
+    GI_ERR_NOT_READY = 7,   /* serving: the request is still in flight */
+    GI_ERR_NO_DEVICE = 8    /* no CUDA device or the kernels are not loadable */
+} gi_status;
+
+typedef struct gi_ctx gi_ctx;
+typedef struct gi_mesh gi_mesh;
+typedef struct gi_result gi_result;
+typedef struct gi_server gi_server;
+
+/* Context options. */
+/* gi_options.flags */
+#define GI_FLAG_TINY_BUFFERS 1u /* start every intersect buffer at 64 entries: exercises the
+                                   capacity-overflow / retry path (host-side fault injection) */
+
+typedef struct {
+    int32_t device;             /* CUDA device ordinal */
+    uint32_t flags;             /* GI_FLAG_* */
+    uint64_t hbm_budget_bytes;  /* 0 = no budget; else mesh + scratch bytes allowed */
+} gi_options;
+
+/* Rigid (or general affine) pose: world = R * (v - center) + center + trans. */
+typedef struct {
+    double R[9]; /* row-major */
+    double center[3];
+    double trans[3];
+    int32_t identity; /* 1: vertices are used unchanged (R, center, trans ignored) */
+    int32_t reserved;
+} gi_pose;
+
+/* Precision modes. */
+#define GI_PREC_FP32_CASCADE 0 /* FP32 boxes + FP32 filter -> FP64 filter -> exact */
+#define GI_PREC_FP64 1         /* FP64 boxes + FP64 filter -> exact (plain FP64 form) */
+
+typedef struct {
+    int32_t want_segments;  /* 1: emit intersection segments */
+    int32_t precision_mode; /* GI_PREC_* */
+    int32_t sort_output;    /* 1: pairs sorted by (a, b) (default 1) */
+    int32_t reserved;
+} gi_intersect_opts;
+
+/* Result statistics (mirrors ExecutionStats / IntersectionTimeTracker). */
+typedef struct {
+    uint64_t tris_a, tris_b;
+    uint64_t nodes_a, nodes_b;        /* wide BVH nodes */
+    uint64_t node_pairs;              /* BVH node pairs expanded by the traversal */
+    uint64_t candidates;              /* box-overlapping triangle pairs tested */
+    uint64_t filter_decided;          /* pairs decided by the first filter stage */
+    uint64_t escalated;               /* pairs sent to the FP64 / exact stage */
+    uint64_t exact_signs;             /* orientation signs resolved exactly */
+    uint64_t exact_points;            /* constructed points that needed exact division */
+    uint64_t pairs;                   /* intersecting pairs */
+    uint64_t segments;                /* emitted segments */
+    uint32_t levels;                  /* traversal levels */
+    uint32_t retries;                 /* capacity retries */
+    uint32_t launches;                /* kernels launched by this call */
+    uint32_t reserved;
+    double ms_traverse;               /* device time: traversal + first filter */
+    double ms_exact;                  /* device time: FP64 / exact stage */
+    double ms_segments;               /* device time: segment construction */
+    double ms_sort;                   /* device time: output ordering */
+    double ms_total;                  /* device time of the whole call */
+} gi_stats;
+
+/* Batched job: one mesh pair with its poses. */
+typedef struct {
+    const gi_mesh* A;
+    const gi_mesh* B;
+    gi_pose pose_a;
+    gi_pose pose_b;
+} gi_pair_job;
+
+/* Serving options. */
+typedef struct {
+    uint32_t max_inflight;  /* requests admitted per device round (0 = 256) */
+    uint32_t flags;         /* reserved */
+    gi_intersect_opts opts; /* options applied to every request */
+} gi_server_opts;
+
+/* ---- context ------------------------------------------------------------ */
+gi_status gi_create(const gi_options* opts, gi_ctx** out);
+gi_status gi_destroy(gi_ctx* ctx);
+const char* gi_status_string(gi_status s);
+const char* gi_last_error(const gi_ctx* ctx);
+gi_status gi_device_count(int32_t* n);
+
+/* ---- meshes (KernelBVHController::construct) ----------------------------- */
+/* Host arrays: verts_xyz[3*nv] doubles, tris[3*nt] vertex indices. */
+gi_status gi_mesh_upload(gi_ctx* ctx, const double* verts_xyz, uint32_t nv, const uint32_t* tris, uint32_t nt,
+                         gi_mesh** out);
+/* Same, from device pointers already resident on the context's device. */
+gi_status gi_mesh_upload_device(gi_ctx* ctx, const double* d_verts_xyz, uint32_t nv, const uint32_t* d_tris,
+                                uint32_t nt, gi_mesh** out);
+gi_status gi_mesh_release(gi_ctx* ctx, gi_mesh* mesh);
+gi_status gi_mesh_info(const gi_mesh* mesh, uint32_t* nv, uint32_t* nt, uint64_t* nodes, uint64_t* device_bytes);
+
+/* ---- poses (setTransformBoth, RotationTools.h:28-70) ---------------------- */
+gi_status gi_pose_identity(gi_pose* out);
+gi_status gi_pose_from_euler_deg(const double rot_deg[3], const double center[3], const double trans[3],
+                                 gi_pose* out);
+/* world coordinates of vertices under a pose, on the host (same FP64 order) */
+gi_status gi_pose_apply(const gi_pose* pose, const double* verts_xyz, uint64_t nv, double* out_xyz);
+
+/* ---- intersection (runIntersectionPipeline) ------------------------------ */
+gi_status gi_intersect_opts_default(gi_intersect_opts* out);
+gi_status gi_intersect(gi_ctx* ctx, const gi_mesh* A, const gi_pose* pose_a, const gi_mesh* B,
+                       const gi_pose* pose_b, const gi_intersect_opts* opts, gi_result** out);
+/* One-shot from host arrays: upload, build, intersect, release
+ * (runGridForestIntersectionPipeline). */
+gi_status gi_intersect_oneshot(gi_ctx* ctx, const double* vA, uint32_t nvA, const uint32_t* tA, uint32_t ntA,
+                               const gi_pose* pose_a, const double* vB, uint32_t nvB, const uint32_t* tB,
+                               uint32_t ntB, const gi_pose* pose_b, const gi_intersect_opts* opts,
+                               gi_result** out);
+/* Batched: all jobs in one persistent device pass; out[i] receives job i's result. */
+gi_status gi_intersect_batch(gi_ctx* ctx, const gi_pair_job* jobs, uint32_t njobs, const gi_intersect_opts* opts,
+                             gi_result** out);
+
+/* ---- results -------------------------------------------------------------- */
+/* pairs_ab: 2 int32 per pair (faceA, faceB); pointer valid until gi_result_free. */
+gi_status gi_result_pairs(const gi_result* r, const int32_t** pairs_ab, uint64_t* n);
+/* seg6: 6 doubles per segment (p0 xyz, p1 xyz); seg_pair: pair index per segment. */
+gi_status gi_result_segments(const gi_result* r, const double** seg6, const int32_t** seg_pair, uint64_t* n);
+gi_status gi_result_stats(const gi_result* r, gi_stats* out);
+gi_status gi_result_free(gi_result* r);
+
+/* ---- serving: pose-update loop with continuous batching ------------------ */
+gi_status gi_server_start(gi_ctx* ctx, const gi_server_opts* opts, gi_server** out);
+gi_status gi_server_submit(gi_server* s, const gi_mesh* A, const gi_pose* pose_a, const gi_mesh* B,
+                           const gi_pose* pose_b, uint64_t* ticket);
+/* GI_OK with *out set when done; GI_ERR_NOT_READY while in flight. */
+gi_status gi_server_poll(gi_server* s, uint64_t ticket, gi_result** out);
+/* Blocks until the ticket is done (bounded by timeout_ms; GI_ERR_TIMEOUT otherwise). */
+gi_status gi_server_wait(gi_server* s, uint64_t ticket, uint32_t timeout_ms, gi_result** out);
+gi_status gi_server_stop(gi_server* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

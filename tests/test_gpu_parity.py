@@ -1,0 +1,351 @@
+"""GPU parity tests: libgi.so through its C ABI versus the exact CPU oracle and
+the committed golden fixtures.  Bit-exact pair sets (the reference's criterion,
+src/CPU/TestSuite.cpp:285-306: set equality, zero false positives / negatives)
+and bit-exact segment endpoints (both sides round the exact point to nearest)."""
+import json
+import os
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, canonical, gi_pose, oracle_pose
+
+pytestmark = pytest.mark.gpu
+
+
+def assert_same(res, ref, segments=True):
+    got, exp = res.pairs, ref["pairs"]
+    if not np.array_equal(got, exp):
+        gs, es = set(map(tuple, got.tolist())), set(map(tuple, exp.tolist()))
+        raise AssertionError("pair sets differ: %d false positives, %d false negatives (of %d)"
+                             % (len(gs - es), len(es - gs), len(es)))
+    if segments:
+        gp, gs = canonical(res.segments, res.seg_pair)
+        ep, es = canonical(ref["segs"], ref["seg_pair"])
+        assert np.array_equal(gp, ep), "segment grouping differs"
+        if not np.array_equal(gs, es):
+            bad = np.nonzero(np.any(gs != es, axis=1))[0]
+            raise AssertionError("%d of %d segment endpoints differ, first: %s vs %s"
+                                 % (len(bad), len(es), gs[bad[0]], es[bad[0]]))
+
+
+def run_cfg(ctx, gi, oc, cfg, precision=0, want_segments=True, nthreads=0):
+    A = ctx.upload(cfg["vA"], cfg["tA"])
+    B = ctx.upload(cfg["vB"], cfg["tB"])
+    r = ctx.intersect(A, B, gi_pose(gi, cfg["poseA"]), gi_pose(gi, cfg["poseB"]), want_segments=want_segments,
+                      precision=precision)
+    ref = oc.intersect_meshes(cfg["vA"], cfg["tA"], oracle_pose(oc, cfg["poseA"]), cfg["vB"], cfg["tB"],
+                              oracle_pose(oc, cfg["poseB"]), want_segments=want_segments, nthreads=nthreads)
+    A.release()
+    B.release()
+    return r, ref
+
+
+def test_smoke():
+    import __graft_entry__
+
+    __graft_entry__.smoke()
+
+
+def _single_tri_jobs(ctx, cases):
+    meshes, jobs = [], []
+    for t1, t2 in cases:
+        A = ctx.upload(np.array(t1, float), np.array([[0, 1, 2]], np.uint32))
+        B = ctx.upload(np.array(t2, float), np.array([[0, 1, 2]], np.uint32))
+        meshes += [A, B]
+        jobs.append((A, None, B, None))
+    return meshes, jobs
+
+
+NSEG = {0: 0, 1: 1, 2: 1, 3: 3, 4: 0}
+
+
+def test_known_answers_gpu(ctx, gi):
+    cases = json.load(open(os.path.join(GOLDEN, "known_answers.json")))
+    meshes, jobs = _single_tri_jobs(ctx, [(c["t1"], c["t2"]) for c in cases])
+    res = ctx.intersect_batch(jobs, want_segments=True)
+    for c, r in zip(cases, res):
+        assert (r.pairs.shape[0] == 1) == (c["kind"] != 0), c["name"]
+        assert r.segments.shape[0] == NSEG[c["kind"]], c["name"]
+        pts = sorted(tuple(float(Fraction(v)) for v in p) for p in c["pts"])
+        if c["kind"] in (1, 2, 3):
+            got = sorted(set(tuple(s[:3]) for s in r.segments) | set(tuple(s[3:]) for s in r.segments))
+            assert got == pts, c["name"]
+    for m in meshes:
+        m.release()
+
+
+def test_random_pairs_gpu(ctx, gi):
+    cases = json.load(open(os.path.join(GOLDEN, "random_pairs.json")))
+    tr = lambda t: [[float.fromhex(x) for x in p] for p in t]
+    meshes, jobs = _single_tri_jobs(ctx, [(tr(c["t1"]), tr(c["t2"])) for c in cases])
+    res = ctx.intersect_batch(jobs, want_segments=True)
+    for c, r in zip(cases, res):
+        assert (r.pairs.shape[0] == 1) == (c["kind"] != 0)
+        assert r.segments.shape[0] == NSEG[c["kind"]]
+        if c["kind"] in (1, 2, 3):
+            exp = sorted(tuple(float.fromhex(x) for x in p) for p in c["pts"])
+            got = sorted(set(tuple(s[:3]) for s in r.segments) | set(tuple(s[3:]) for s in r.segments))
+            assert got == exp
+    for m in meshes:
+        m.release()
+
+
+def test_config1_golden_gpu(ctx, gi):
+    g = np.load(os.path.join(GOLDEN, "config1.npz"))
+    A, B = ctx.upload(g["vA"], g["tA"]), ctx.upload(g["vB"], g["tB"])
+    for prec in (0, 1):
+        r = ctx.intersect(A, B, None, gi.pose_raw(g["poseB_R"], g["poseB_C"], g["poseB_T"]), precision=prec)
+        assert_same(r, dict(pairs=g["pairs"], segs=g["segs"], seg_pair=g["seg_pair"]))
+    A.release()
+    B.release()
+
+
+def test_grid64_golden_gpu(ctx, gi):
+    g = np.load(os.path.join(GOLDEN, "grid64.npz"))
+    A, B = ctx.upload(g["vA"], g["tA"]), ctx.upload(g["vB"], g["tB"])
+    for prec in (0, 1):
+        r = ctx.intersect(A, B, None, None, precision=prec)
+        assert_same(r, dict(pairs=g["pairs"], segs=g["segs"], seg_pair=g["seg_pair"]))
+    A.release()
+    B.release()
+
+
+def test_config2_full_vs_oracle(ctx, gi, oc):
+    from gpuintersector import meshgen as mg
+
+    cfg = mg.config2()
+    r, ref = run_cfg(ctx, gi, oc, cfg)
+    assert_same(r, ref)
+    st = r.stats
+    assert st["pairs"] == len(ref["pairs"]) and st["candidates"] >= ref["stats"].candidates
+    assert st["filter_decided"] >= 0.99 * st["candidates"]
+
+
+def test_config3_full_vs_oracle(ctx, gi, oc):
+    from gpuintersector import meshgen as mg
+
+    cfg = mg.config3()
+    r, ref = run_cfg(ctx, gi, oc, cfg)
+    assert len(ref["pairs"]) > 1_000_000
+    assert_same(r, ref)
+
+
+def test_fp64_form_identical(ctx, gi, oc):
+    from gpuintersector import meshgen as mg
+
+    cfg = mg.config2(level=6)
+    r32, ref = run_cfg(ctx, gi, oc, cfg, precision=0)
+    r64, _ = run_cfg(ctx, gi, oc, cfg, precision=1)
+    assert_same(r32, ref)
+    assert_same(r64, ref)
+
+
+def test_unsorted_output_same_set(ctx, gi, oc):
+    from gpuintersector import meshgen as mg
+
+    cfg = mg.config1(seed=9)
+    A, B = ctx.upload(cfg["vA"], cfg["tA"]), ctx.upload(cfg["vB"], cfg["tB"])
+    r1 = ctx.intersect(A, B, None, gi_pose(gi, cfg["poseB"]), sort_output=True)
+    r2 = ctx.intersect(A, B, None, gi_pose(gi, cfg["poseB"]), sort_output=False)
+    assert set(map(tuple, r1.pairs.tolist())) == set(map(tuple, r2.pairs.tolist()))
+    A.release()
+    B.release()
+
+
+def test_pose_sweep_like_runsuite(ctx, gi, oc):
+    """Seeded random rotations (+-15 deg) and translations (+-0.5) of B about a
+    centre, as TestSuite::runSuite (src/CPU/TestSuite.cpp:455-505); FP = FN = 0."""
+    from gpuintersector import meshgen as mg
+
+    v, t = mg.uv_sphere(64, 40)
+    rng = np.random.default_rng(1337)
+    A, B = ctx.upload(v, t), ctx.upload(v, t)
+    for step in range(8):
+        rot = rng.uniform(-15, 15, 3)
+        tr = rng.uniform(-0.5, 0.5, 3)
+        cen = [0.01, -0.02, 0.03]
+        r = ctx.intersect(A, B, None, gi.pose_from_euler_deg(rot, cen, tr))
+        ref = oc.intersect_meshes(v, t, oc.pose_identity(), v, t, oc.pose_from_euler_deg(rot, cen, tr))
+        assert_same(r, ref)
+    A.release()
+    B.release()
+
+
+def test_both_meshes_posed(ctx, gi, oc):
+    from gpuintersector import meshgen as mg
+
+    v, t = mg.icosphere(4)
+    rng = np.random.default_rng(5)
+    v = mg.displace(v, mg.displacement_params(rng))
+    pa = (mg.random_rotation(rng), np.array([0.1, 0.0, -0.2]), np.array([1.0, -2.0, 0.5]))
+    pb = (mg.random_rotation(rng), np.array([0.0, 0.3, 0.0]), np.array([1.3, -1.9, 0.4]))
+    r, ref = run_cfg(ctx, gi, oc, dict(vA=v, tA=t, vB=v, tB=t, poseA=pa, poseB=pb))
+    assert len(ref["pairs"]) > 0
+    assert_same(r, ref)
+
+
+def test_identical_meshes_coplanar_everywhere(ctx, gi, oc):
+    """A == B under the identity pose: every pair of neighbours touches or overlaps
+    coplanarly -- the exact stage decides almost every candidate."""
+    from gpuintersector import meshgen as mg
+
+    v, t = mg.uv_sphere(16, 10)
+    r, ref = run_cfg(ctx, gi, oc, dict(vA=v, tA=t, vB=v, tB=t, poseA=None, poseB=None))
+    assert len(ref["pairs"]) > t.shape[0]
+    assert_same(r, ref)
+    assert r.stats["escalated"] > 0
+
+
+def test_batch_equals_individual(ctx, gi, oc):
+    from gpuintersector import meshgen as mg
+
+    jobs = mg.config4(seed=8, pairs=6, t_min=200, t_max=4000)
+    meshes, bjobs, refs = [], [], []
+    for j in jobs:
+        A, B = ctx.upload(j["vA"], j["tA"]), ctx.upload(j["vB"], j["tB"])
+        meshes += [A, B]
+        bjobs.append((A, None, B, gi_pose(gi, j["poseB"])))
+        refs.append(oc.intersect_meshes(j["vA"], j["tA"], oc.pose_identity(), j["vB"], j["tB"],
+                                        oracle_pose(oc, j["poseB"])))
+    res = ctx.intersect_batch(bjobs)
+    assert sum(len(r["pairs"]) for r in refs) > 0
+    for r, ref, (A, pa, B, pb) in zip(res, refs, bjobs):
+        assert_same(r, ref)
+        single = ctx.intersect(A, B, pa, pb)
+        assert_same(single, ref)
+    for m in meshes:
+        m.release()
+
+
+def test_oneshot_and_controller_mirror(ctx, gi, oc):
+    from gpuintersector import meshgen as mg
+
+    v, t = mg.uv_sphere(48, 30)
+    rot, cen, tr = [5.0, 10.0, -12.0], [0.0, 0.0, 0.0], [0.6, 0.05, 0.0]
+    ref = oc.intersect_meshes(v, t, oc.pose_identity(), v, t, oc.pose_from_euler_deg(rot, cen, tr))
+    r = ctx.intersect_oneshot(v, t, v, t, None, gi.pose_from_euler_deg(rot, cen, tr))
+    assert_same(r, ref)
+    r2 = gi.run_grid_forest_intersection_pipeline(v, t, v, t, rotB=rot, transB=tr, ctx=ctx, want_segments=True)
+    assert_same(r2, ref)
+    kc = gi.KernelBVHController()
+    kc.construct(v, t, 12, v, t, 12, 4)
+    kc.setTransformBoth([0, 0, 0], [0, 0, 0], rot, tr)
+    pairs = kc.runIntersectionPipeline(1, 0, 0, 1)
+    assert np.array_equal(pairs, ref["pairs"])
+    kc.clearGPU()
+    assert not kc.isGPUAllocated()
+    kc.reconstructGPU()
+    assert np.array_equal(kc.runIntersectionPipeline(), ref["pairs"])
+    kc.cleanup()
+
+
+def test_degenerate_triangles_in_meshes(ctx, gi, oc):
+    from gpuintersector import meshgen as mg
+
+    v, t = mg.uv_sphere(20, 12)
+    rng = np.random.default_rng(2)
+    t = t.copy()
+    # collapse some triangles to segments and points
+    for k in rng.choice(t.shape[0], 30, replace=False):
+        t[k, 2] = t[k, 1] if k % 2 else t[k, 0]
+    v2 = np.concatenate([v, [[0.1, 0.2, 0.3], [0.3, 0.6, 0.9], [0.2, 0.4, 0.6]]])
+    t2 = np.concatenate([t, [[v.shape[0], v.shape[0] + 1, v.shape[0] + 2]]]).astype(np.uint32)  # collinear
+    R = mg.random_rotation(rng)
+    r, ref = run_cfg(ctx, gi, oc, dict(vA=v2, tA=t2, vB=v2, tB=t2, poseA=None, poseB=(R, np.zeros(3),
+                                                                                      np.array([0.3, 0, 0]))))
+    assert_same(r, ref)
+    r, ref = run_cfg(ctx, gi, oc, dict(vA=v2, tA=t2, vB=v2, tB=t2, poseA=None, poseB=None))
+    assert_same(r, ref)
+
+
+def test_empty_and_tiny_meshes(ctx, gi, oc):
+    one = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], float)
+    tri = np.array([[0, 1, 2]], np.uint32)
+    A = ctx.upload(one, tri)
+    E = ctx.upload(one, np.zeros((0, 3), np.uint32))
+    r = ctx.intersect(A, E)
+    assert r.pairs.shape == (0, 2)
+    r = ctx.intersect(A, A)
+    assert r.pairs.tolist() == [[0, 0]] and r.segments.shape[0] == 3
+    for m in (A, E):
+        m.release()
+
+
+def test_far_from_origin_and_scaled(ctx, gi, oc):
+    from gpuintersector import meshgen as mg
+
+    v, t = mg.icosphere(3)
+    v = v * 1e-3 + np.array([1e5, -3e4, 7.0])
+    R = mg.random_rotation(np.random.default_rng(4))
+    cen = np.array([1e5, -3e4, 7.0])
+    r, ref = run_cfg(ctx, gi, oc, dict(vA=v, tA=t, vB=v, tB=t, poseA=None,
+                                       poseB=(R, cen, np.array([6e-4, 0.0, 0.0]))))
+    assert len(ref["pairs"]) > 0
+    assert_same(r, ref)
+
+
+def test_invalid_inputs_are_reported(ctx, gi):
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], float)
+    with pytest.raises(gi.GIError) as e:
+        ctx.upload(v, np.array([[0, 1, 7]], np.uint32))
+    assert e.value.status == 1
+    with pytest.raises(gi.GIError) as e:
+        ctx.upload(np.array([[0, 0, np.nan], [1, 0, 0], [0, 1, 0]]), np.array([[0, 1, 2]], np.uint32))
+    assert e.value.status == 6
+    with pytest.raises(gi.GIError) as e:
+        ctx.upload(np.array([[0, 0, 1e40], [1, 0, 0], [0, 1, 0]]), np.array([[0, 1, 2]], np.uint32))
+    assert e.value.status == 6
+    A = ctx.upload(v, np.array([[0, 1, 2]], np.uint32))
+    bad = gi.pose_raw(np.eye(3), (0, 0, 0), (1e300, 0, 0))
+    with pytest.raises(gi.GIError) as e:
+        ctx.intersect(A, A, None, bad)
+    assert e.value.status == 6
+    A.release()
+
+
+def test_capacity_retry_path(gi, oc):
+    """Host-side fault injection: every buffer starts at 64 entries, so the
+    overflow flags fire and the call grows its buffers and re-runs."""
+    from gpuintersector import meshgen as mg
+
+    cfg = mg.config1(seed=4)
+    with gi.Context(0, flags=gi._abi.GI_FLAG_TINY_BUFFERS) as c:
+        r, ref = run_cfg(c, gi, oc, cfg)
+    assert r.stats["retries"] > 0
+    assert_same(r, ref)
+
+
+def test_hbm_budget_admission(gi):
+    from gpuintersector import meshgen as mg
+
+    v, t = mg.icosphere(5)
+    with gi.Context(0, hbm_budget_bytes=1 << 20) as c:
+        with pytest.raises(gi.GIError) as e:
+            c.upload(v, t)
+        assert e.value.status == 2
+
+
+def test_server_results_alone_and_in_mix(ctx, gi):
+    """Continuous batching: requests that arrive while others run are admitted
+    into later device rounds; every result equals the one computed alone."""
+    from gpuintersector import meshgen as mg
+
+    v, t = mg.icosphere(4)
+    v = mg.displace(v, mg.displacement_params(np.random.default_rng(6)))
+    A, B = ctx.upload(v, t), ctx.upload(v, t)
+    rng = np.random.default_rng(7)
+    poses = []
+    for R, tr in mg.pose_stream(rng, 24, 5.0, 0.05):
+        poses.append(gi.pose_raw(R, (0, 0, 0), tr + np.array([0.35, 0.0, 0.0])))
+    alone = [ctx.intersect(A, B, None, p) for p in poses]
+    srv = ctx.server(max_inflight=5)
+    tickets = [srv.submit(A, None, B, p) for p in poses]
+    mixed = [srv.wait(tk) for tk in tickets]
+    srv.stop()
+    for a, m in zip(alone, mixed):
+        assert np.array_equal(a.pairs, m.pairs)
+        assert np.array_equal(a.segments, m.segments)
+    A.release()
+    B.release()
