@@ -283,6 +283,7 @@ def main():
         "tri_pair_tests_per_s": tests_per_s,
         "filter_decided_frac": float(st["filter_decided"] / max(1, st["candidates"])),
         "escalated": int(st["escalated"]), "exact_signs": int(st["exact_signs"]),
+        "levels": int(st["levels"]), "node_pairs": int(st["node_pairs"]),
         "stage_ms": {"traverse_filter": trav, "exact": float(np.mean([s["ms_exact"] for s in stats])),
                      "segments": float(np.mean([s["ms_segments"] for s in stats])),
                      "ordering": float(np.mean([s["ms_sort"] for s in stats]))},

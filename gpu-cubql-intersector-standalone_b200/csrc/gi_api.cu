@@ -67,15 +67,12 @@ struct gi_ctx {
     // outputs
     double* segs = nullptr;  // 18 per result slot
     uint32_t* nseg = nullptr;
-    uint32_t* perm = nullptr;
     int32_t* pairs_out = nullptr;
     uint32_t* job_out = nullptr;
     double* segs_out = nullptr;
     int32_t* segpair_out = nullptr;
-    uint32_t* seg_off = nullptr;
-    uint32_t* seg_scan_tmp = nullptr;
-    uint32_t* d_total = nullptr;
     uint32_t cap_out = 0;
+    uint64_t pred_pairs = 0, pred_segs = 0;  // result sizes of the previous call
     void* order_scratch = nullptr;
     size_t order_scratch_bytes = 0;
     // pinned staging for results
@@ -186,8 +183,7 @@ extern "C" gi_status gi_destroy(gi_ctx* c)
     cudaSetDevice(c->device);
     if (c->st) cudaStreamSynchronize(c->st);
     void* dev[] = {c->d_cnt, c->d_jobs, c->front[0], c->front[1], c->cand, c->res, c->esc, c->segs, c->nseg,
-                   c->perm, c->pairs_out, c->job_out, c->segs_out, c->segpair_out, c->seg_off, c->seg_scan_tmp,
-                   c->d_total, c->order_scratch};
+                   c->pairs_out, c->job_out, c->segs_out, c->segpair_out, c->order_scratch};
     for (void* p : dev)
         if (p) cudaFree(p);
     if (c->h_cnt) cudaFreeHost(c->h_cnt);
@@ -294,7 +290,8 @@ extern "C" gi_status gi_mesh_release(gi_ctx* c, gi_mesh* m)
     if (!c || !m || m->ctx != c) return GI_ERR_INVALID_ARG;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->st);
-    void* p[] = {m->b.verts, m->b.tris, m->b.leafTri, m->b.leafBox, m->b.nodes, m->b.leafBox64, m->b.nodes64};
+    void* p[] = {m->b.verts,     m->b.tris,    m->b.leafTri, m->b.leafBox, m->b.nodes,
+                 m->b.leafBox64, m->b.nodes64, m->b.cutRef,  m->b.cutBox,  m->b.cutBox64};
     for (void* q : p)
         if (q) cudaFree(q);
     if (m->b.bytes <= c->mesh_bytes) c->mesh_bytes -= m->b.bytes;
@@ -422,6 +419,10 @@ static MeshDev mesh_dev(const gi_mesh* m)
     d.leafBox64 = m->b.leafBox64;
     d.nodes = m->b.nodes;
     d.nodes64 = m->b.nodes64;
+    d.cutRef = m->b.cutRef;
+    d.cutBox = m->b.cutBox;
+    d.cutBox64 = m->b.cutBox64;
+    d.ncut = m->b.ncut;
     d.root = m->b.root;
     d.nv = m->b.nv;
     d.nt = m->b.nt;
@@ -474,11 +475,16 @@ static gi_status ensure_pinned(gi_ctx* c, size_t bytes)
 }
 
 // Core: runs the job list on the device and fills per-job results.
+// One host synchronisation per call: every kernel takes its sizes from the
+// device counters, and the results are copied back speculatively at the size
+// of the previous call (a second copy follows only when the result grew).
 static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_intersect_opts& o,
                           std::vector<gi_result*>& outs)
 {
     const uint32_t nj = (uint32_t)jobs.size();
     const int prec = o.precision_mode == GI_PREC_FP64 ? 1 : 0;
+    const bool want_segs = o.want_segments != 0;
+    const bool sort = o.sort_output != 0;
     uint64_t maxA = 1, maxB = 1, sumT = 0;
     for (const auto& j : jobs) {
         maxA = std::max<uint64_t>(maxA, j.A.nt);
@@ -487,7 +493,6 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
     }
     int ba = bits_for(maxA), bb = bits_for(maxB), bj = nj > 1 ? bits_for(nj) : 0;
     if (ba + bb + bj > 64) return set_err(c, GI_ERR_INVALID_ARG, "batch too large for 64-bit ordering keys");
-    // jobs to the device
     if (nj > c->cap_jobs) {
         if (c->d_jobs) cudaFree(c->d_jobs);
         if (c->h_jobs) cudaFreeHost(c->h_jobs);
@@ -500,7 +505,6 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
     }
     memcpy(c->h_jobs, jobs.data(), sizeof(JobDev) * nj);
     CK(c, cudaMemcpyAsync(c->d_jobs, c->h_jobs, sizeof(JobDev) * nj, cudaMemcpyHostToDevice, c->st), "jobs copy");
-    // initial capacities
     const bool tiny = (c->flags & GI_FLAG_TINY_BUFFERS) != 0;
     uint32_t need_front = std::max<uint32_t>(c->cap_front, tiny ? 64u : std::max<uint32_t>(1u << 20, nj * 64u));
     uint32_t need_cand =
@@ -509,22 +513,46 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
     uint32_t need_esc = std::max<uint32_t>(c->cap_esc, tiny ? 64u : std::max<uint32_t>(need_cand / 4, 1u << 16));
     const unsigned long long launches0 = launch_count();
     Counters& H = *c->h_cnt;
-    gi_stats st;
-    memset(&st, 0, sizeof st);
-    float ms_trav = 0, ms_exact = 0;
     int retries = 0;
+    uint32_t nres = 0, nsegs = 0;
+    char* hp = nullptr;
+    size_t off_jobs = 0, off_segs = 0, off_segpair = 0;
     for (;; retries++) {
         CK(c, grow(c->front[0], c->cap_front, need_front, c->st), "frontier");
         CK(c, grow(c->front[1], c->cap_front1, need_front, c->st), "frontier");
         CK(c, grow(c->cand, c->cap_cand, need_cand, c->st), "candidates");
         CK(c, grow(c->res, c->cap_res, need_res, c->st), "results");
         CK(c, grow(c->esc, c->cap_esc, need_esc, c->st), "escalations");
+        const uint32_t cap = c->cap_res;
+        if (cap > c->cap_out) {
+            void* old[] = {c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out, c->segpair_out};
+            for (void* p : old)
+                if (p) cudaFreeAsync(p, c->st);
+            c->cap_out = 0;
+            CK(c, cudaMallocAsync(&c->segs, sizeof(double) * 18 * (size_t)cap, c->st), "segments");
+            CK(c, cudaMallocAsync(&c->nseg, sizeof(uint32_t) * cap, c->st), "segments");
+            CK(c, cudaMallocAsync(&c->pairs_out, sizeof(int32_t) * 2 * (size_t)cap, c->st), "pairs");
+            CK(c, cudaMallocAsync(&c->job_out, sizeof(uint32_t) * cap, c->st), "pairs");
+            CK(c, cudaMallocAsync(&c->segs_out, sizeof(double) * 18 * (size_t)cap, c->st), "segments");
+            CK(c, cudaMallocAsync(&c->segpair_out, sizeof(int32_t) * 3 * (size_t)cap, c->st), "segments");
+            c->cap_out = cap;
+        }
+        size_t osb = order_scratch_bytes(cap, kOsMaxPasses);
+        if (osb > c->order_scratch_bytes) {
+            if (c->order_scratch) cudaFreeAsync(c->order_scratch, c->st);
+            c->order_scratch = nullptr;
+            c->order_scratch_bytes = 0;
+            CK(c, cudaMallocAsync(&c->order_scratch, osb, c->st), "order scratch");
+            CK(c, cudaMemsetAsync(c->order_scratch, 0, osb, c->st), "order scratch");
+            c->order_scratch_bytes = osb;
+        }
+        OrderBufs O = make_order_bufs(c->order_scratch, cap, ba, bb, bj);
         Bufs b;
         b.jobs = c->d_jobs;
         b.njobs = nj;
         b.front[0] = c->front[0];
         b.front[1] = c->front[1];
-        b.cap_front = c->cap_front;
+        b.cap_front = std::min(c->cap_front, c->cap_front1);
         b.cand = c->cand;
         b.cap_cand = c->cap_cand;
         b.res = c->res;
@@ -534,131 +562,117 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         b.cnt = c->d_cnt;
         b.precision = prec;
         CK(c, cudaMemsetAsync(c->d_cnt, 0, sizeof(Counters), c->st), "counters");
-        CK(c, launch_init_frontier(b, c->st), "init frontier");
+        CK(c, launch_init_frontier(b, prec, c->st), "init frontier");
         CK(c, cudaEventRecord(c->ev[0], c->st), "event");
         CK(c, launch_traverse(b, c->cfg, prec, c->st), "traverse");
+        CK(c, launch_filter(b, c->cfg, prec, c->st), "filter");
         CK(c, cudaEventRecord(c->ev[1], c->st), "event");
         CK(c, launch_exact(b, c->cfg, c->st), "exact stage");
         CK(c, cudaEventRecord(c->ev[2], c->st), "event");
+        if (want_segs) CK(c, launch_segments(b, c->segs, c->nseg, c->cfg, c->st), "segments");
+        CK(c, cudaEventRecord(c->ev[3], c->st), "event");
+        CK(c, launch_order_gather(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
+                                  c->segpair_out, want_segs, c->cfg, c->st),
+           "ordering");
+        CK(c, cudaEventRecord(c->ev[4], c->st), "event");
+        // speculative copy at the previous call's size
+        uint32_t pp = std::min<uint32_t>(cap, (uint32_t)std::min<uint64_t>(c->pred_pairs + c->pred_pairs / 4 + 1024,
+                                                                          0xffffffffu));
+        uint32_t ps = want_segs ? std::min<uint32_t>(3 * cap, c->pred_segs + c->pred_segs / 4 + 1024) : 0u;
+        off_jobs = sizeof(int32_t) * 2 * (size_t)pp;
+        off_segs = off_jobs + (nj > 1 ? sizeof(uint32_t) * (size_t)pp : 0);
+        off_segs = (off_segs + 15) & ~(size_t)15;
+        off_segpair = off_segs + sizeof(double) * 6 * (size_t)ps;
+        gi_status s = ensure_pinned(c, off_segpair + sizeof(int32_t) * (size_t)ps + 64);
+        if (s != GI_OK) return s;
+        hp = (char*)c->h_stage;
         CK(c, cudaMemcpyAsync(c->h_cnt, c->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, c->st), "counters");
+        CK(c, cudaMemcpyAsync(hp, c->pairs_out, off_jobs, cudaMemcpyDeviceToHost, c->st), "copy pairs");
+        if (nj > 1)
+            CK(c, cudaMemcpyAsync(hp + off_jobs, c->job_out, sizeof(uint32_t) * pp, cudaMemcpyDeviceToHost, c->st),
+               "copy jobs");
+        if (ps) {
+            CK(c, cudaMemcpyAsync(hp + off_segs, c->segs_out, sizeof(double) * 6 * ps, cudaMemcpyDeviceToHost, c->st),
+               "copy segments");
+            CK(c, cudaMemcpyAsync(hp + off_segpair, c->segpair_out, sizeof(int32_t) * ps, cudaMemcpyDeviceToHost,
+                                  c->st),
+               "copy segments");
+        }
         CK(c, cudaStreamSynchronize(c->st), "sync");
-        if (H.err & kErrBarrier) return set_err(c, GI_ERR_TIMEOUT, "grid barrier wait ran out");
+        if (H.err & kErrBarrier) return set_err(c, GI_ERR_TIMEOUT, "a bounded device wait ran out");
         if (H.err & kErrExactCapacity) return set_err(c, GI_ERR_RANGE, "exact arithmetic capacity exceeded");
-        if (H.overflow == 0) break;
-        if (retries >= 12) return set_err(c, GI_ERR_CAPACITY, "intersection buffers stayed too small");
-        auto g4 = [](uint32_t cur, uint32_t seen) {
-            uint64_t v = std::max<uint64_t>((uint64_t)cur * 4, (uint64_t)seen + seen / 2 + 1024);
-            return (uint32_t)std::min<uint64_t>(v, 0x7fffffffu);
-        };
-        if (H.overflow & kOvfFrontier) need_front = g4(c->cap_front, c->cap_front);
-        if (H.overflow & kOvfCand) need_cand = g4(c->cap_cand, H.cand);
-        if (H.overflow & (kOvfRes | kOvfCand)) need_res = g4(c->cap_res, H.res);
-        if (H.overflow & (kOvfEsc | kOvfCand)) need_esc = g4(c->cap_esc, H.esc);
+        if (H.overflow) {
+            if (retries >= 12) return set_err(c, GI_ERR_CAPACITY, "intersection buffers stayed too small");
+            auto g4 = [](uint32_t cur, uint32_t seen) {
+                uint64_t v = std::max<uint64_t>((uint64_t)cur * 4, (uint64_t)seen + seen / 2 + 1024);
+                return (uint32_t)std::min<uint64_t>(v, 0x7fffffffu);
+            };
+            if (H.overflow & kOvfFrontier) need_front = g4(std::min(c->cap_front, c->cap_front1), 0);
+            if (H.overflow & kOvfCand) need_cand = g4(c->cap_cand, H.cand);
+            if (H.overflow & (kOvfRes | kOvfCand)) need_res = g4(c->cap_res, H.res);
+            if (H.overflow & (kOvfEsc | kOvfCand)) need_esc = g4(c->cap_esc, H.esc);
+            continue;
+        }
+        nres = H.res;
+        nsegs = want_segs ? H.nseg : 0;
+        if (nres > pp || nsegs > ps) {
+            // the result outgrew the speculative copy: copy it again at its real size
+            off_jobs = sizeof(int32_t) * 2 * (size_t)nres;
+            off_segs = (off_jobs + (nj > 1 ? sizeof(uint32_t) * (size_t)nres : 0) + 15) & ~(size_t)15;
+            off_segpair = off_segs + sizeof(double) * 6 * (size_t)nsegs;
+            s = ensure_pinned(c, off_segpair + sizeof(int32_t) * (size_t)nsegs + 64);
+            if (s != GI_OK) return s;
+            hp = (char*)c->h_stage;
+            if (nres) CK(c, cudaMemcpyAsync(hp, c->pairs_out, off_jobs, cudaMemcpyDeviceToHost, c->st), "copy pairs");
+            if (nres && nj > 1)
+                CK(c, cudaMemcpyAsync(hp + off_jobs, c->job_out, sizeof(uint32_t) * nres, cudaMemcpyDeviceToHost,
+                                      c->st),
+                   "copy jobs");
+            if (nsegs) {
+                CK(c, cudaMemcpyAsync(hp + off_segs, c->segs_out, sizeof(double) * 6 * nsegs, cudaMemcpyDeviceToHost,
+                                      c->st),
+                   "copy segments");
+                CK(c, cudaMemcpyAsync(hp + off_segpair, c->segpair_out, sizeof(int32_t) * nsegs,
+                                      cudaMemcpyDeviceToHost, c->st),
+                   "copy segments");
+            }
+            CK(c, cudaStreamSynchronize(c->st), "sync");
+        }
+        break;
     }
+    c->pred_pairs = nres;
+    c->pred_segs = nsegs;
+    float ms_trav = 0, ms_exact = 0, ms_seg = 0, ms_sort = 0, ms_total = 0;
     cudaEventElapsedTime(&ms_trav, c->ev[0], c->ev[1]);
     cudaEventElapsedTime(&ms_exact, c->ev[1], c->ev[2]);
-    const uint32_t nres = H.res;
-    // output buffers
-    if (nres > c->cap_out) {
-        uint32_t cap = std::max<uint32_t>(nres + nres / 2, 1u << 14);
-        void* old[] = {c->segs, c->nseg, c->perm, c->pairs_out, c->job_out, c->segs_out, c->segpair_out, c->seg_off,
-                       c->seg_scan_tmp, c->d_total};
-        for (void* p : old)
-            if (p) cudaFreeAsync(p, c->st);
-        c->cap_out = 0;
-        CK(c, cudaMallocAsync(&c->segs, sizeof(double) * 18 * (size_t)cap, c->st), "segments");
-        CK(c, cudaMallocAsync(&c->nseg, sizeof(uint32_t) * cap, c->st), "segments");
-        CK(c, cudaMallocAsync(&c->perm, sizeof(uint32_t) * cap, c->st), "order");
-        CK(c, cudaMallocAsync(&c->pairs_out, sizeof(int32_t) * 2 * (size_t)cap, c->st), "pairs");
-        CK(c, cudaMallocAsync(&c->job_out, sizeof(uint32_t) * cap, c->st), "pairs");
-        CK(c, cudaMallocAsync(&c->segs_out, sizeof(double) * 18 * (size_t)cap, c->st), "segments");
-        CK(c, cudaMallocAsync(&c->segpair_out, sizeof(int32_t) * 3 * (size_t)cap, c->st), "segments");
-        CK(c, cudaMallocAsync(&c->seg_off, sizeof(uint32_t) * cap, c->st), "segments");
-        CK(c, cudaMallocAsync(&c->seg_scan_tmp, sizeof(uint32_t) * scan_temp_words_host(cap), c->st), "segments");
-        CK(c, cudaMallocAsync(&c->d_total, sizeof(uint32_t) * 4, c->st), "segments");
-        c->cap_out = cap;
-    }
-    size_t osb = order_scratch_bytes(std::max<uint32_t>(nres, 1));
-    if (osb > c->order_scratch_bytes) {
-        if (c->order_scratch) cudaFreeAsync(c->order_scratch, c->st);
-        c->order_scratch = nullptr;
-        c->order_scratch_bytes = 0;
-        CK(c, cudaMallocAsync(&c->order_scratch, osb * 2, c->st), "order scratch");
-        c->order_scratch_bytes = osb * 2;
-    }
-    Bufs b;
-    b.jobs = c->d_jobs;
-    b.njobs = nj;
-    b.res = c->res;
-    b.cap_res = c->cap_res;
-    b.cnt = c->d_cnt;
-    const bool want_segs = o.want_segments != 0;
-    CK(c, cudaEventRecord(c->ev[3], c->st), "event");
-    if (want_segs && nres) CK(c, launch_segments(b, nres, c->segs, c->nseg, c->cfg, c->st), "segments");
-    CK(c, cudaEventRecord(c->ev[4], c->st), "event");
-    OrderScratch os;
-    os.ptr = c->order_scratch;
-    os.bytes = c->order_scratch_bytes;
-    if (nres) {
-        CK(c, launch_order(c->res, nres, ba, bb, bj, o.sort_output != 0, c->perm, os, c->st), "order");
-        CK(c, launch_gather(c->res, c->perm, nres, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
-                            c->segpair_out, c->seg_off, c->seg_scan_tmp, want_segs, c->d_total, c->st),
-           "gather");
-    }
-    CK(c, cudaEventRecord(c->ev[5], c->st), "event");
-    // copy back: pairs, jobs, total segments
-    size_t pbytes = sizeof(int32_t) * 2 * (size_t)nres, jbytes = sizeof(uint32_t) * (size_t)nres;
-    gi_status s = ensure_pinned(c, pbytes + jbytes + 64);
-    if (s != GI_OK) return s;
-    char* hp = (char*)c->h_stage;
-    uint32_t* htotal = (uint32_t*)(hp + pbytes + jbytes);
-    *htotal = 0;
-    if (nres) {
-        CK(c, cudaMemcpyAsync(hp, c->pairs_out, pbytes, cudaMemcpyDeviceToHost, c->st), "copy pairs");
-        if (nj > 1) CK(c, cudaMemcpyAsync(hp + pbytes, c->job_out, jbytes, cudaMemcpyDeviceToHost, c->st), "copy jobs");
-        if (want_segs)
-            CK(c, cudaMemcpyAsync(htotal, c->d_total, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st), "copy total");
-    }
-    CK(c, cudaStreamSynchronize(c->st), "sync");
-    // counters after the segment stage
-    CK(c, cudaMemcpy(c->h_cnt, c->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost), "counters");
-    if (H.err & kErrExactCapacity) return set_err(c, GI_ERR_RANGE, "exact arithmetic capacity exceeded");
-    float ms_seg = 0, ms_sort = 0, ms_total = 0;
-    cudaEventElapsedTime(&ms_seg, c->ev[3], c->ev[4]);
-    cudaEventElapsedTime(&ms_sort, c->ev[4], c->ev[5]);
-    cudaEventElapsedTime(&ms_total, c->ev[0], c->ev[5]);
-    // split per job
+    cudaEventElapsedTime(&ms_seg, c->ev[2], c->ev[3]);
+    cudaEventElapsedTime(&ms_sort, c->ev[3], c->ev[4]);
+    cudaEventElapsedTime(&ms_total, c->ev[0], c->ev[4]);
+    // split per job (sorted by job first)
     std::vector<uint32_t> job_start(nj + 1, 0);
     if (nj == 1) {
         job_start[1] = nres;
     } else {
-        const uint32_t* hj = (const uint32_t*)(hp + pbytes);
+        const uint32_t* hj = (const uint32_t*)(hp + off_jobs);
         for (uint32_t k = 0; k < nres; k++) job_start[hj[k] + 1]++;
         for (uint32_t j = 0; j < nj; j++) job_start[j + 1] += job_start[j];
     }
-    uint32_t nsegs = want_segs ? *htotal : 0;
-    std::vector<double> hsegs;
-    std::vector<int32_t> hsegpair;
-    if (nsegs) {
-        hsegs.resize(6 * (size_t)nsegs);
-        hsegpair.resize(nsegs);
-        CK(c, cudaMemcpyAsync(hsegs.data(), c->segs_out, sizeof(double) * 6 * nsegs, cudaMemcpyDeviceToHost, c->st),
-           "copy segments");
-        CK(c, cudaMemcpyAsync(hsegpair.data(), c->segpair_out, sizeof(int32_t) * nsegs, cudaMemcpyDeviceToHost, c->st),
-           "copy segments");
-        CK(c, cudaStreamSynchronize(c->st), "sync");
-    }
     const int32_t* hpairs = (const int32_t*)hp;
+    const double* hsegs = (const double*)(hp + off_segs);
+    const int32_t* hsegpair = (const int32_t*)(hp + off_segpair);
     size_t sp = 0;
     for (uint32_t j = 0; j < nj; j++) {
         gi_result* r = new (std::nothrow) gi_result();
         if (!r) return GI_ERR_OOM;
         uint32_t a = job_start[j], e = job_start[j + 1];
         r->pairs.assign(hpairs + 2 * (size_t)a, hpairs + 2 * (size_t)e);
-        while (sp < nsegs && (uint32_t)hsegpair[sp] < e) {
-            r->segs.insert(r->segs.end(), hsegs.begin() + 6 * sp, hsegs.begin() + 6 * sp + 6);
-            r->seg_pair.push_back(hsegpair[sp] - (int32_t)a);
-            sp++;
+        size_t s0 = sp;
+        while (sp < nsegs && (uint32_t)hsegpair[sp] < e) sp++;
+        if (sp > s0) {
+            r->segs.assign(hsegs + 6 * s0, hsegs + 6 * sp);
+            r->seg_pair.assign(hsegpair + s0, hsegpair + sp);
+            if (a)
+                for (auto& q : r->seg_pair) q -= (int32_t)a;
         }
         gi_stats& s2 = r->stats;
         memset(&s2, 0, sizeof s2);

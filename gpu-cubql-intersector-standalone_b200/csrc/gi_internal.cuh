@@ -53,9 +53,16 @@ struct MeshDev {
     const double* leafBox64;
     const WNode* nodes;
     const WNode64* nodes64;
+    const uint32_t* cutRef;  // depth-3 cut: node / leaf refs whose subtrees cover all leaves
+    const float* cutBox;     // their boxes (6 floats each)
+    const double* cutBox64;  // FP64 boxes of the same cut (FP64 form)
     uint32_t root;  // wide node index, or kLeaf | leaf position when nt == 1
     uint32_t nv, nt, nnodes;
+    uint32_t ncut;
+    uint32_t pad_;
 };
+
+constexpr int kCutMax = 64;  // 4^3
 
 struct JobDev {
     MeshDev A, B;
@@ -73,6 +80,8 @@ struct Counters {
     unsigned int levels;
     unsigned int bar_count;
     unsigned int bar_gen;
+    unsigned int bar_stop;  // stop snapshot taken inside the grid barrier
+    unsigned int pool_next[2];  // depth-first phase: next pool entry to hand out (per round parity)
     unsigned int nseg;      // total segments after ordering
     unsigned long long node_pairs;
     unsigned long long filter_decided;

@@ -271,6 +271,60 @@ __global__ void k_collapse(int n, const uint2* __restrict__ child, const uint32_
     nodes[widx[i]] = out;
 }
 
+// Depth-3 cut of the wide BVH: the root expanded three times (leaves met on the
+// way are kept), with each entry's box from its parent's child slot.  At most
+// 4^3 = 64 entries; the traversal starts from all pairs of the two cuts.
+template <class S, class NodeT>
+__global__ void k_cut(const NodeT* __restrict__ nodes, const S* __restrict__ leafBox, uint32_t root,
+                      uint32_t* __restrict__ cutRef, S* __restrict__ cutBox, uint32_t* __restrict__ ncut)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    uint32_t r[kCutMax], r2[kCutMax];
+    S b[kCutMax][6], b2[kCutMax][6];
+    int n = 0;
+    if (root & kLeaf) {
+        r[0] = root;
+        for (int k = 0; k < 6; k++) b[0][k] = leafBox[6 * (size_t)(root & ~kLeaf) + k];
+        n = 1;
+    } else {
+        r[0] = root;
+        n = 1;
+        for (int depth = 0; depth < 3; depth++) {
+            int m = 0;
+            for (int e = 0; e < n; e++) {
+                if (r[e] & kLeaf) {
+                    r2[m] = r[e];
+                    for (int k = 0; k < 6; k++) b2[m][k] = b[e][k];
+                    m++;
+                    continue;
+                }
+                const NodeT& nd = nodes[r[e]];
+                for (int c = 0; c < 4; c++) {
+                    if (nd.child[c] == kEmpty) continue;
+                    r2[m] = nd.child[c];
+                    b2[m][0] = nd.lox[c];
+                    b2[m][1] = nd.loy[c];
+                    b2[m][2] = nd.loz[c];
+                    b2[m][3] = nd.hix[c];
+                    b2[m][4] = nd.hiy[c];
+                    b2[m][5] = nd.hiz[c];
+                    m++;
+                }
+            }
+            n = m;
+            for (int e = 0; e < n; e++) {
+                r[e] = r2[e];
+                for (int k = 0; k < 6; k++) b[e][k] = b2[e][k];
+            }
+        }
+    }
+    for (int e = 0; e < n; e++) {
+        cutRef[e] = r[e];
+        for (int k = 0; k < 6; k++) cutBox[6 * e + k] = b[e][k];
+    }
+    *ncut = (uint32_t)n;
+}
+
 cudaError_t launch_validate(const double* verts, uint32_t nv, const uint32_t* tris, uint32_t nt, unsigned* d_err,
                             cudaStream_t st)
 {
@@ -367,6 +421,24 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaStream_t st)
         m.nnodes = nw;
         m.root = 0;
     }
+    // depth-3 cut (refs shared by both precisions; boxes per precision)
+    {
+        uint32_t* d_n = nullptr;
+        GI_TRY(cudaMallocAsync(&d_n, sizeof(uint32_t), st));
+        if (!m.cutRef) GI_TRY(cudaMallocAsync(&m.cutRef, sizeof(uint32_t) * kCutMax, st));
+        if (!fp64) {
+            GI_TRY(cudaMallocAsync(&m.cutBox, sizeof(float) * 6 * kCutMax, st));
+            k_cut<float, WNode><<<1, 32, 0, st>>>(m.nodes, m.leafBox, m.root, m.cutRef, m.cutBox, d_n);
+        } else {
+            GI_TRY(cudaMallocAsync(&m.cutBox64, sizeof(double) * 6 * kCutMax, st));
+            k_cut<double, WNode64><<<1, 32, 0, st>>>(m.nodes64, m.leafBox64, m.root, m.cutRef, m.cutBox64, d_n);
+        }
+        uint32_t hn = 0;
+        GI_TRY(cudaMemcpyAsync(&hn, d_n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        GI_TRY(cudaStreamSynchronize(st));
+        cudaFreeAsync(d_n, st);
+        m.ncut = hn;
+    }
     GI_TRY(cudaGetLastError());
     cudaFreeAsync(box, st);
     if (box64) cudaFreeAsync(box64, st);
@@ -460,32 +532,85 @@ struct Prec<true> {
     static __device__ __forceinline__ const S* leafBox(const MeshDev& M) { return M.leafBox64; }
 };
 
-template <bool F64>
-__device__ __forceinline__ bool load_child(const MeshDev& M, uint32_t ref, int i, Box<typename Prec<F64>::S>& b,
-                                           uint32_t& cref)
+// Children of a node reference in the mesh-local frame: a wide node gives up
+// to four (one 128-byte line, loaded as seven 16-byte vectors); a leaf
+// reference stands for itself.
+__device__ __forceinline__ void load_kids(const MeshDev& M, uint32_t ref, Box<float> b[4], uint32_t c[4])
 {
-    using S = typename Prec<F64>::S;
-    if (ref == kEmpty) return false;
     if (ref & kLeaf) {
-        if (i != 0) return false;
-        const S* lb = Prec<F64>::leafBox(M) + 6 * (size_t)(ref & ~kLeaf);
-        for (int k = 0; k < 3; k++) {
-            b.lo[k] = __ldg(lb + k);
-            b.hi[k] = __ldg(lb + 3 + k);
-        }
-        cref = ref;
-        return true;
+        const float2* lb = reinterpret_cast<const float2*>(M.leafBox + 6 * (size_t)(ref & ~kLeaf));
+        float2 a = __ldg(lb), bb = __ldg(lb + 1), cc = __ldg(lb + 2);
+        b[0].lo[0] = a.x;
+        b[0].lo[1] = a.y;
+        b[0].lo[2] = bb.x;
+        b[0].hi[0] = bb.y;
+        b[0].hi[1] = cc.x;
+        b[0].hi[2] = cc.y;
+        c[0] = ref;
+        c[1] = c[2] = c[3] = kEmpty;
+        return;
     }
-    const typename Prec<F64>::Node* nd = Prec<F64>::nodes(M) + ref;
-    cref = __ldg(&nd->child[i]);
-    if (cref == kEmpty) return false;
-    b.lo[0] = __ldg(&nd->lox[i]);
-    b.lo[1] = __ldg(&nd->loy[i]);
-    b.lo[2] = __ldg(&nd->loz[i]);
-    b.hi[0] = __ldg(&nd->hix[i]);
-    b.hi[1] = __ldg(&nd->hiy[i]);
-    b.hi[2] = __ldg(&nd->hiz[i]);
-    return true;
+    const float4* p = reinterpret_cast<const float4*>(M.nodes + ref);
+    float4 lx = __ldg(p), ly = __ldg(p + 1), lz = __ldg(p + 2), hx = __ldg(p + 3), hy = __ldg(p + 4),
+           hz = __ldg(p + 5);
+    uint4 ch = __ldg(reinterpret_cast<const uint4*>(p + 6));
+    const float* LX = &lx.x;
+    const float* LY = &ly.x;
+    const float* LZ = &lz.x;
+    const float* HX = &hx.x;
+    const float* HY = &hy.x;
+    const float* HZ = &hz.x;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        b[i].lo[0] = LX[i];
+        b[i].lo[1] = LY[i];
+        b[i].lo[2] = LZ[i];
+        b[i].hi[0] = HX[i];
+        b[i].hi[1] = HY[i];
+        b[i].hi[2] = HZ[i];
+    }
+    c[0] = ch.x;
+    c[1] = ch.y;
+    c[2] = ch.z;
+    c[3] = ch.w;
+}
+__device__ __forceinline__ void load_kids(const MeshDev& M, uint32_t ref, Box<double> b[4], uint32_t c[4])
+{
+    if (ref & kLeaf) {
+        const double2* lb = reinterpret_cast<const double2*>(M.leafBox64 + 6 * (size_t)(ref & ~kLeaf));
+        double2 a = __ldg(lb), bb = __ldg(lb + 1), cc = __ldg(lb + 2);
+        b[0].lo[0] = a.x;
+        b[0].lo[1] = a.y;
+        b[0].lo[2] = bb.x;
+        b[0].hi[0] = bb.y;
+        b[0].hi[1] = cc.x;
+        b[0].hi[2] = cc.y;
+        c[0] = ref;
+        c[1] = c[2] = c[3] = kEmpty;
+        return;
+    }
+    const double2* p = reinterpret_cast<const double2*>(M.nodes64 + ref);
+    double v[24];
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+        double2 q = __ldg(p + k);
+        v[2 * k] = q.x;
+        v[2 * k + 1] = q.y;
+    }
+    uint4 ch = __ldg(reinterpret_cast<const uint4*>(p + 12));
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        b[i].lo[0] = v[i];
+        b[i].lo[1] = v[4 + i];
+        b[i].lo[2] = v[8 + i];
+        b[i].hi[0] = v[12 + i];
+        b[i].hi[1] = v[16 + i];
+        b[i].hi[2] = v[20 + i];
+    }
+    c[0] = ch.x;
+    c[1] = ch.y;
+    c[2] = ch.z;
+    c[3] = ch.w;
 }
 
 template <class S>
@@ -507,6 +632,49 @@ __device__ __forceinline__ unsigned warp_append(bool pred, unsigned* counter)
     return base + __popc(m & ((1u << lane) - 1u));
 }
 
+// Reserves `cnt` consecutive slots per lane with one atomic per warp.
+__device__ __forceinline__ unsigned warp_reserve(unsigned cnt, unsigned* counter)
+{
+    const unsigned lane = threadIdx.x & 31;
+    unsigned incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (unsigned)o) incl += y;
+    }
+    unsigned total = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned base = 0;
+    if (lane == 31 && total) base = atomicAdd(counter, total);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    return base + incl - cnt;
+}
+
+// Two reservations with their atomics issued back to back (one round trip).
+__device__ __forceinline__ void warp_reserve2(unsigned c1, unsigned* ctr1, unsigned c2, unsigned* ctr2,
+                                              unsigned* p1, unsigned* p2)
+{
+    const unsigned lane = threadIdx.x & 31;
+    unsigned i1 = c1, i2 = c2;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned y1 = __shfl_up_sync(0xffffffffu, i1, o);
+        unsigned y2 = __shfl_up_sync(0xffffffffu, i2, o);
+        if (lane >= (unsigned)o) {
+            i1 += y1;
+            i2 += y2;
+        }
+    }
+    unsigned b1 = 0, b2 = 0;
+    if (lane == 31) {
+        if (i1) b1 = atomicAdd(ctr1, i1);
+        if (i2) b2 = atomicAdd(ctr2, i2);
+    }
+    b1 = __shfl_sync(0xffffffffu, b1, 31);
+    b2 = __shfl_sync(0xffffffffu, b2, 31);
+    *p1 = b1 + i1 - c1;
+    *p2 = b2 + i2 - c2;
+}
+
 __device__ __forceinline__ unsigned ld_cg_u32(const unsigned* p)
 {
     return __ldcg(p);
@@ -515,18 +683,24 @@ __device__ __forceinline__ unsigned ld_cg_u32(const unsigned* p)
 constexpr unsigned long long kBarrierSpins = 1ull << 22;
 
 // Software grid barrier for a cooperative launch (all blocks co-resident).
+// The last block to arrive takes a snapshot of the overflow / error flags
+// before it releases the others, so every block leaves with the same stop
+// decision (flags set during the next level cannot split the grid).
 // Every wait is bounded: after kBarrierSpins polls the block records
-// kErrBarrier and continues; the kernel then drains and the host reports
-// GI_ERR_TIMEOUT.
-__device__ void grid_sync(Counters* C)
+// kErrBarrier and stops; the host then reports GI_ERR_TIMEOUT.
+__device__ bool grid_sync(Counters* C)
 {
+    __shared__ unsigned s_stop;
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile unsigned* genp = &C->bar_gen;
         unsigned g = *genp;
         __threadfence();
         unsigned arrived = atomicAdd(&C->bar_count, 1u);
+        unsigned timed_out = 0;
         if (arrived == gridDim.x - 1) {
+            unsigned stop = (ld_cg_u32(&C->overflow) | ld_cg_u32(&C->err)) ? 1u : 0u;
+            atomicExch(&C->bar_stop, stop);
             atomicExch(&C->bar_count, 0u);
             __threadfence();
             atomicAdd(&C->bar_gen, 1u);
@@ -535,14 +709,17 @@ __device__ void grid_sync(Counters* C)
             while (*genp == g) {
                 if (++spins > kBarrierSpins) {
                     atomicOr(&C->err, kErrBarrier);
+                    timed_out = 1;
                     break;
                 }
-                __nanosleep(100);
+                __nanosleep(32);
             }
         }
         __threadfence();
+        s_stop = ld_cg_u32(&C->bar_stop) | timed_out;
     }
     __syncthreads();
+    return s_stop != 0;
 }
 
 template <bool F64>
@@ -556,62 +733,110 @@ __device__ __forceinline__ void load_tri(const MeshDev& M, const DevPose& P, uin
     *tri_id = t.w;
 }
 
+// One node pair per lane: load both nodes (2 x 128 B), map the child boxes to
+// the world frame, test the 4 x 4 child pairs.  fm / cm: bit 4i+j set when
+// child pair (i, j) overlaps and leads to a node pair / a leaf pair.
 template <bool F64>
-__global__ void __launch_bounds__(256) k_traverse(Bufs B)
+__device__ __forceinline__ void expand_pair(const Bufs& B, const uint4& ent, unsigned& fm, unsigned& cm,
+                                            uint32_t ca[4], uint32_t cb[4])
 {
     using S = typename Prec<F64>::S;
+    Box<S> ba[4], bb[4];
+    const JobDev& J = B.jobs[ent.x];
+    load_kids(J.A, ent.y, ba, ca);
+    load_kids(J.B, ent.z, bb, cb);
+    const bool ia = J.pa.identity, ib = J.pb.identity;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        if (!ia && ca[i] != kEmpty) world_box(J.pa, ba[i]);
+        if (!ib && cb[i] != kEmpty) world_box(J.pb, bb[i]);
+    }
+    fm = cm = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (ca[i] == kEmpty || cb[j] == kEmpty || !overlap(ba[i], bb[j])) continue;
+            const unsigned bit = 1u << (4 * i + j);
+            if ((ca[i] & kLeaf) && (cb[j] & kLeaf)) cm |= bit;
+            else fm |= bit;
+        }
+}
+
+constexpr int kTravWarps = 8;  // warps per block
+
+// BVH4 x BVH4 traversal in one cooperative launch, breadth first: every level
+// is spread over all lanes (one node pair per lane) and levels are separated
+// by the bounded grid barrier.  It starts from the all-pairs test of the two
+// meshes' depth-3 cuts (k_cut_pairs), so the top levels -- too narrow to fill
+// the GPU -- cost one step instead of three.  Leaf pairs go to the candidate
+// list for k_filter.
+template <bool F64>
+__global__ void __launch_bounds__(kTravWarps * 32) k_traverse(Bufs B)
+{
     Counters* C = B.cnt;
     const unsigned lane = threadIdx.x & 31;
     const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
-    const unsigned hl = lane & 15, ci = hl & 3, cj = hl >> 2, half = lane >> 4;
     unsigned long long visited = 0;
-    unsigned level = 0;
+    unsigned level = 0, n = 0;
+    bool stop = false;
+    // ---- phase 1 ----
     for (; level < 4096; level++) {
         const unsigned cur = level % 3, nxt = (level + 1) % 3, clr = (level + 2) % 3;
-        unsigned n = ld_cg_u32(&C->front[cur]);
-        if (n == 0 || ld_cg_u32(&C->overflow) || ld_cg_u32(&C->err)) break;
-        if (n > B.cap_front) n = B.cap_front;
+        n = ld_cg_u32(&C->front[cur]);
+        if (n == 0 || stop) break;
+        if (n > B.cap_front) n = B.cap_front;  // an overflowed count: read only what was stored
         if (blockIdx.x == 0 && threadIdx.x == 0) C->front[clr] = 0;
         const uint4* in = B.front[level & 1];
         uint4* out = B.front[(level + 1) & 1];
-        for (unsigned base = warp * 2; base < n; base += nwarps * 2) {
-            const unsigned e = base + half;
-            const bool have = e < n;
-            uint4 ent = have ? __ldcg(in + e) : make_uint4(0u, kEmpty, kEmpty, 0u);
-            visited += (have && hl == 0);
-            const JobDev& J = B.jobs[ent.x];
-            Box<S> ba, bb;
-            uint32_t ca = kEmpty, cb = kEmpty;
-            bool va = have && load_child<F64>(J.A, ent.y, ci, ba, ca);
-            bool vb = have && load_child<F64>(J.B, ent.z, cj, bb, cb);
-            bool valid = va && vb;
-            if (valid) {
-                if (!J.pa.identity) world_box(J.pa, ba);
-                if (!J.pb.identity) world_box(J.pb, bb);
-                valid = overlap(ba, bb);
+        for (unsigned base = warp * 32; base < n; base += nwarps * 32) {
+            const unsigned e = base + lane;
+            unsigned fm = 0, cm = 0;
+            uint32_t ca[4], cb[4];
+            uint4 ent = make_uint4(0u, kEmpty, kEmpty, 0u);
+            if (e < n) {
+                ent = __ldcg(in + e);
+                visited++;
+                expand_pair<F64>(B, ent, fm, cm, ca, cb);
             }
-            const bool isCand = valid && (ca & kLeaf) && (cb & kLeaf);
-            const bool isFront = valid && !isCand;
-            unsigned pf = warp_append(isFront, &C->front[nxt]);
-            if (isFront) {
-                if (pf < B.cap_front) out[pf] = make_uint4(ent.x, ca, cb, 0u);
-                else atomicOr(&C->overflow, kOvfFrontier);
-            }
-            unsigned pc = warp_append(isCand, &C->cand);
-            if (isCand) {
-                if (pc < B.cap_cand) B.cand[pc] = make_uint4(ent.x, ca & ~kLeaf, cb & ~kLeaf, 0u);
-                else atomicOr(&C->overflow, kOvfCand);
+            unsigned pf, pc;
+            warp_reserve2(__popc(fm), &C->front[nxt], __popc(cm), &C->cand, &pf, &pc);
+            if (fm | cm) {
+#pragma unroll
+                for (int k = 0; k < 16; k++) {
+                    const unsigned bit = 1u << k;
+                    if (fm & bit) {
+                        if (pf < B.cap_front) out[pf] = make_uint4(ent.x, ca[k >> 2], cb[k & 3], 0u);
+                        else atomicOr(&C->overflow, kOvfFrontier);
+                        pf++;
+                    }
+                    if (cm & bit) {
+                        if (pc < B.cap_cand)
+                            B.cand[pc] = make_uint4(ent.x, ca[k >> 2] & ~kLeaf, cb[k & 3] & ~kLeaf, 0u);
+                        else atomicOr(&C->overflow, kOvfCand);
+                        pc++;
+                    }
+                }
             }
         }
-        grid_sync(C);
+        stop = grid_sync(C);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) C->levels = level;
     for (int o = 16; o > 0; o >>= 1) visited += __shfl_xor_sync(0xffffffffu, visited, o);
     if (lane == 0 && visited) atomicAdd(&C->node_pairs, visited);
-    if (ld_cg_u32(&C->overflow) || ld_cg_u32(&C->err)) return;
+}
 
-    // ---- first filter stage over all leaf pairs ----
+// First filter stage over all leaf pairs: FP32 (or FP64) semi-static filter of
+// the general-position case; decided pairs are final, the rest escalate.
+template <bool F64>
+__global__ void __launch_bounds__(256) k_filter(Bufs B)
+{
+    Counters* C = B.cnt;
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
+    if (ld_cg_u32(&C->overflow) || ld_cg_u32(&C->err)) return;
     unsigned nc = ld_cg_u32(&C->cand);
     if (nc > B.cap_cand) nc = B.cap_cand;
     unsigned long long decided = 0;
@@ -696,12 +921,14 @@ __device__ __forceinline__ void load_tri_orig(const MeshDev& M, const DevPose& P
     out[2] = world_vertex(M.verts, __ldg(t + 2), P);
 }
 
-__global__ void __launch_bounds__(128) k_segments(Bufs B, uint32_t nres, double* __restrict__ segs,
-                                                  uint32_t* __restrict__ nseg)
+__global__ void __launch_bounds__(128) k_segments(Bufs B, double* __restrict__ segs, uint32_t* __restrict__ nseg)
 {
     Counters* C = B.cnt;
     const unsigned gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const unsigned nth = gridDim.x * blockDim.x;
+    if (ld_cg_u32(&C->overflow)) return;
+    unsigned nres = ld_cg_u32(&C->res);
+    if (nres > B.cap_res) nres = B.cap_res;
     for (unsigned i = gtid; i < nres; i += nth) {
         uint4 rr = __ldcg(B.res + i);
         const JobDev& J = B.jobs[rr.x];
@@ -740,123 +967,340 @@ __global__ void __launch_bounds__(128) k_segments(Bufs B, uint32_t nres, double*
 }
 
 // ===========================================================================
-// Ordering
+// Ordering: results sorted by (job, a, b) with an LSD radix sort whose sizes
+// come from the device counters (no host round trip).  One kernel builds the
+// keys and the digit histograms of every pass, one scans them, and each pass
+// is one scatter kernel: tiles of 4096 items take their global offset per
+// digit by decoupled look-back over the preceding tiles (bounded waits).
+// The gather kernel applies the permutation and places the segments, finding
+// its segment offset by the same look-back.
 // ===========================================================================
-__global__ void k_order_keys(const uint4* __restrict__ res, uint32_t n, int bits_a, int bits_b,
-                             unsigned long long* __restrict__ keys, uint32_t* __restrict__ vals)
+constexpr int kOsThreads = 256;
+constexpr int kOsItems = 16;
+constexpr int kOsTile = kOsThreads * kOsItems;
+constexpr int kOsWarps = kOsThreads / 32;
+constexpr int kOsGatherTile = 1024;
+constexpr unsigned kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kCountMask = (1u << 30) - 1u;
+constexpr unsigned long long kLookbackSpins = 1ull << 22;
+
+__device__ __forceinline__ unsigned res_count(const Bufs& B)
 {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    uint4 r = res[i];
-    keys[i] = ((unsigned long long)r.x << (bits_a + bits_b)) | ((unsigned long long)r.y << bits_b) | r.z;
-    vals[i] = i;
-}
-__global__ void k_iota(uint32_t* v, uint32_t n)
-{
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) v[i] = i;
+    if (ld_cg_u32(&B.cnt->overflow)) return 0u;
+    unsigned n = ld_cg_u32(&B.cnt->res);
+    return n > B.cap_res ? B.cap_res : n;
 }
 
-size_t scan_temp_words_host(size_t n)
+__device__ __forceinline__ unsigned long long order_key(const uint4& r, const OrderBufs& O)
 {
-    return scan_temp_words(n);
+    return ((unsigned long long)r.x << (O.bits_a + O.bits_b)) | ((unsigned long long)r.y << O.bits_b) | r.z;
 }
 
-size_t order_scratch_bytes(uint32_t n)
+// Keys, identity values and the histograms of every digit pass; the last
+// block to finish scans the histograms into digit bases (and clears them for
+// the next call), so no separate scan launch is needed.
+__global__ void __launch_bounds__(kOsThreads) k_os_hist(Bufs B, OrderBufs O)
 {
-    size_t cw = radix_counts_words(n);
-    size_t sw = scan_temp_words(cw > n ? cw : n);
-    return 2 * sizeof(unsigned long long) * (size_t)n + sizeof(uint32_t) * ((size_t)n + cw + sw) + 1024;
-}
-
-cudaError_t launch_order(const uint4* res, uint32_t n, int bits_a, int bits_b, int bits_job, bool sort,
-                         uint32_t* perm_out, OrderScratch scratch, cudaStream_t st)
-{
-    if (n == 0) return cudaSuccess;
-    int tb = 256, gb = (int)((n + tb - 1) / tb);
-    if (!sort) {
-        k_iota<<<gb, tb, 0, st>>>(perm_out, n);
-        note_launches(1);
-        return cudaGetLastError();
+    __shared__ unsigned h[kOsMaxPasses][256];
+    __shared__ uint32_t sw[33];
+    __shared__ unsigned s_last;
+    const unsigned n = res_count(B);
+    for (int p = 0; p < O.passes; p++) h[p][threadIdx.x] = 0;
+    // look-back status of every pass and of the gather starts unset
+    const unsigned ntiles = (n + kOsTile - 1) / kOsTile;
+    const size_t nstat = (size_t)(O.passes + 1) * O.ntiles_cap * 256;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nstat; k += (size_t)gridDim.x * blockDim.x) {
+        const size_t t = (k / 256) % O.ntiles_cap;
+        if (t < ntiles) O.status[k] = 0u;
     }
-    char* p = (char*)scratch.ptr;
-    unsigned long long* k0 = (unsigned long long*)p;
-    p += sizeof(unsigned long long) * (size_t)n;
-    unsigned long long* k1 = (unsigned long long*)p;
-    p += sizeof(unsigned long long) * (size_t)n;
-    uint32_t* v1 = (uint32_t*)p;
-    p += sizeof(uint32_t) * (size_t)n;
-    size_t cw = radix_counts_words(n);
-    uint32_t* counts = (uint32_t*)p;
-    p += sizeof(uint32_t) * cw;
-    uint32_t* stemp = (uint32_t*)p;
-    k_order_keys<<<gb, tb, 0, st>>>(res, n, bits_a, bits_b, k0, perm_out);
-    note_launches(1);
-    radix_sort<unsigned long long>(k0, perm_out, k1, v1, n, bits_a + bits_b + bits_job, counts, stemp, st);
-    return cudaGetLastError();
+    const unsigned ngather = (n + kOsGatherTile - 1) / kOsGatherTile;
+    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < ngather; k += gridDim.x * blockDim.x)
+        O.gstatus[k] = 0u;
+    if (blockIdx.x == 0 && threadIdx.x <= (unsigned)O.passes) O.tile_ctr[threadIdx.x] = 0u;
+    __syncthreads();
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned long long key = order_key(__ldcg(B.res + i), O);
+        O.keys[0][i] = key;
+        O.vals[0][i] = i;
+        for (int p = 0; p < O.passes; p++) atomicAdd(&h[p][(unsigned)(key >> (8 * p)) & 255u], 1u);
+    }
+    __syncthreads();
+    for (int p = 0; p < O.passes; p++)
+        if (h[p][threadIdx.x]) atomicAdd(&O.hist[p * 256 + threadIdx.x], h[p][threadIdx.x]);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = (atomicAdd(&O.tile_ctr[kOsMaxPasses + 1], 1u) == gridDim.x - 1) ? 1u : 0u;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int p = 0; p < O.passes; p++) {
+        const unsigned v = __ldcg(&O.hist[p * 256 + threadIdx.x]);
+        unsigned tot;
+        const unsigned ex = block_exclusive_scan(v, sw, &tot);
+        O.base[p * 256 + threadIdx.x] = ex;
+        O.hist[p * 256 + threadIdx.x] = 0u;
+    }
+    if (threadIdx.x == 0) O.tile_ctr[kOsMaxPasses + 1] = 0u;
 }
 
-__global__ void k_gather_pairs(const uint4* __restrict__ res, const uint32_t* __restrict__ perm, uint32_t n,
-                               const uint32_t* __restrict__ nseg, int32_t* __restrict__ pairs_out,
-                               uint32_t* __restrict__ job_out, uint32_t* __restrict__ cnt_sorted)
+// Exclusive prefix of this tile over the preceding tiles, per status slot.
+// Returns false if a wait ran out (the error bit is set; results are invalid).
+__device__ __forceinline__ bool lookback(unsigned* status, unsigned tile, unsigned stride, unsigned own,
+                                         unsigned* excl_out, unsigned* err)
 {
-    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    uint32_t s = perm[k];
-    uint4 r = res[s];
+    unsigned excl = 0;
+    if (tile > 0) {
+        // publish the local aggregate first so successors need not wait for our prefix
+        atomicExch(status + (size_t)tile * stride, kFlagAgg | (own & kCountMask));
+        unsigned t = tile - 1;
+        for (;;) {
+            volatile unsigned* q = status + (size_t)t * stride;
+            unsigned v = *q;
+            unsigned long long spins = 0;
+            while ((v & ~kCountMask) == 0u) {
+                if (++spins > kLookbackSpins) {
+                    atomicOr(err, kErrBarrier);
+                    *excl_out = 0;
+                    return false;
+                }
+                __nanosleep(32);
+                v = *q;
+            }
+            excl += v & kCountMask;
+            if ((v & ~kCountMask) == kFlagInc || t == 0) break;
+            t--;
+        }
+    }
+    __threadfence();
+    atomicExch(status + (size_t)tile * stride, kFlagInc | ((excl + own) & kCountMask));
+    *excl_out = excl;
+    return true;
+}
+
+__global__ void __launch_bounds__(kOsThreads) k_os_scatter(Bufs B, OrderBufs O, int pass)
+{
+    __shared__ unsigned wc[kOsWarps][256];
+    __shared__ unsigned tile_base[256];
+    __shared__ unsigned s_tile;
+    const unsigned n = res_count(B);
+    const unsigned ntiles = (n + kOsTile - 1) / kOsTile;
+    if (threadIdx.x == 0) s_tile = atomicAdd(&O.tile_ctr[pass], 1u);
+    __syncthreads();
+    const unsigned tile = s_tile;
+    if (tile >= ntiles) return;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int shift = 8 * pass;
+    const unsigned long long* kin = O.keys[pass & 1];
+    const uint32_t* vin = O.vals[pass & 1];
+    unsigned long long* kout = O.keys[(pass + 1) & 1];
+    uint32_t* vout = O.vals[(pass + 1) & 1];
+    for (int d = lane; d < 256; d += 32) wc[w][d] = 0;
+    __syncwarp();
+    const unsigned seg = tile * kOsTile + w * 32 * kOsItems;
+    unsigned long long key[kOsItems];
+    uint32_t val[kOsItems], rank[kOsItems], dig[kOsItems];
+    const unsigned lt = (1u << lane) - 1u;
+    // all loads first (independent, in flight together), then the ranking
+#pragma unroll
+    for (int c = 0; c < kOsItems; c++) {
+        const unsigned i = seg + c * 32 + lane;
+        key[c] = i < n ? __ldcg(kin + i) : 0ull;
+        val[c] = i < n ? __ldcg(vin + i) : 0u;
+    }
+#pragma unroll
+    for (int c = 0; c < kOsItems; c++) {
+        const unsigned i = seg + c * 32 + lane;
+        const bool ok = i < n;
+        const unsigned d = ok ? ((unsigned)(key[c] >> shift) & 255u) : 256u;
+        dig[c] = d;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        rank[c] = ok ? wc[w][d] + __popc(peers & lt) : 0u;
+        __syncwarp();
+        if (ok && (peers & lt) == 0) wc[w][d] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    {
+        const unsigned d = threadIdx.x;
+        unsigned run = 0;
+        for (int q = 0; q < kOsWarps; q++) {
+            const unsigned t = wc[q][d];
+            wc[q][d] = run;
+            run += t;
+        }
+        unsigned excl;
+        lookback(O.status + (size_t)pass * O.ntiles_cap * 256 + d, tile, 256, run, &excl, &B.cnt->err);
+        tile_base[d] = O.base[pass * 256 + d] + excl;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < kOsItems; c++) {
+        const unsigned d = dig[c];
+        if (d < 256u) {
+            const unsigned pos = tile_base[d] + wc[w][d] + rank[c];
+            kout[pos] = key[c];
+            vout[pos] = val[c];
+        }
+    }
+}
+
+// sorted position k -> pairs_out[k], job_out[k]; the segments of the pair go
+// to the prefix sum of the segment counts (tile look-back).  One item per
+// thread, so every load of a thread is issued at once.
+__global__ void __launch_bounds__(kOsGatherTile) k_os_gather(Bufs B, OrderBufs O, const double* __restrict__ segs,
+                                                             const uint32_t* __restrict__ nseg, int32_t* pairs_out,
+                                                             uint32_t* job_out, double* segs_out,
+                                                             int32_t* segpair_out, int want_segments, int sorted)
+{
+    __shared__ uint32_t sw[33];
+    __shared__ unsigned s_tile, s_base;
+    const unsigned n = res_count(B);
+    const unsigned ntiles = (n + kOsGatherTile - 1) / kOsGatherTile;
+    if (threadIdx.x == 0) s_tile = atomicAdd(&O.tile_ctr[O.passes], 1u);
+    __syncthreads();
+    const unsigned tile = s_tile;
+    if (tile >= ntiles) return;
+    const unsigned k = tile * kOsGatherTile + threadIdx.x;
+    const bool ok = k < n;
+    const unsigned src = ok ? (sorted ? __ldcg(O.vals[O.passes & 1] + k) : k) : 0u;
+    const unsigned c = (ok && want_segments) ? __ldcg(nseg + src) : 0u;
+    const uint4 r = ok ? __ldcg(B.res + src) : make_uint4(0u, 0u, 0u, 0u);
+    unsigned tot;
+    const unsigned ex = block_exclusive_scan(c, sw, &tot);
+    if (threadIdx.x == 0) {
+        unsigned excl;
+        lookback(O.gstatus, tile, 1, tot, &excl, &B.cnt->err);
+        s_base = excl;
+        if (tile == ntiles - 1) B.cnt->nseg = excl + tot;
+    }
+    __syncthreads();
+    if (!ok) return;
     pairs_out[2 * (size_t)k] = (int32_t)r.y;
     pairs_out[2 * (size_t)k + 1] = (int32_t)r.z;
-    if (job_out) job_out[k] = r.x;
-    if (cnt_sorted) cnt_sorted[k] = nseg[s];
-}
-__global__ void k_gather_segs(const uint32_t* __restrict__ perm, uint32_t n, const double* __restrict__ segs,
-                              const uint32_t* __restrict__ nseg, const uint32_t* __restrict__ off,
-                              double* __restrict__ segs_out, int32_t* __restrict__ segpair_out, uint32_t* total)
-{
-    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    uint32_t s = perm[k];
-    uint32_t c = nseg[s], o = off[k];
-    for (uint32_t q = 0; q < c; q++) {
-        for (int j = 0; j < 6; j++) segs_out[6 * (size_t)(o + q) + j] = segs[18 * (size_t)s + 6 * q + j];
-        segpair_out[o + q] = (int32_t)k;
+    job_out[k] = r.x;
+    const unsigned off = s_base + ex;
+    for (unsigned q = 0; q < c; q++) {
+        const double2* sp = reinterpret_cast<const double2*>(segs + 18 * (size_t)src + 6 * q);
+        double2* dp = reinterpret_cast<double2*>(segs_out + 6 * (size_t)(off + q));
+        dp[0] = __ldcg(sp);
+        dp[1] = __ldcg(sp + 1);
+        dp[2] = __ldcg(sp + 2);
+        segpair_out[off + q] = (int32_t)k;
     }
-    if (k == n - 1) *total = o + c;
 }
 
-cudaError_t launch_gather(const uint4* res, const uint32_t* perm, uint32_t n, const double* segs,
-                          const uint32_t* nseg, int32_t* pairs_out, uint32_t* job_out, double* segs_out,
-                          int32_t* segpair_out, uint32_t* seg_offsets, uint32_t* seg_scan_temp, bool want_segments,
-                          uint32_t* d_total_segs, cudaStream_t st)
+size_t order_scratch_bytes(uint32_t cap, int passes)
 {
-    if (n == 0) return cudaSuccess;
-    int tb = 256, gb = (int)((n + tb - 1) / tb);
-    k_gather_pairs<<<gb, tb, 0, st>>>(res, perm, n, nseg, pairs_out, job_out, want_segments ? seg_offsets : nullptr);
+    size_t ntiles = (cap + kOsTile - 1) / kOsTile;
+    return 2 * sizeof(unsigned long long) * (size_t)cap + 2 * sizeof(uint32_t) * (size_t)cap +
+           sizeof(uint32_t) * ((size_t)(passes + 1) * ntiles * 256 + 2 * kOsMaxPasses * 256 + kOsMaxPasses + 2 +
+                               (size_t)cap / kOsGatherTile + 1) +
+           8192;
+}
+
+OrderBufs make_order_bufs(void* scratch, uint32_t cap, int bits_a, int bits_b, int bits_job)
+{
+    OrderBufs O;
+    O.bits_a = bits_a;
+    O.bits_b = bits_b;
+    O.passes = (bits_a + bits_b + bits_job + 7) / 8;
+    O.ntiles_cap = (cap + kOsTile - 1) / kOsTile;
+    char* p = (char*)scratch;
+    auto take = [&](size_t bytes) {
+        char* q = p;
+        p += (bytes + 255) & ~(size_t)255;
+        return (void*)q;
+    };
+    O.keys[0] = (unsigned long long*)take(sizeof(unsigned long long) * cap);
+    O.keys[1] = (unsigned long long*)take(sizeof(unsigned long long) * cap);
+    O.vals[0] = (uint32_t*)take(sizeof(uint32_t) * cap);
+    O.vals[1] = (uint32_t*)take(sizeof(uint32_t) * cap);
+    // fixed layout (independent of the pass count of the call): the histogram
+    // must stay at the same, zeroed, address from one call to the next
+    O.status = (uint32_t*)take(sizeof(uint32_t) * (size_t)(kOsMaxPasses + 1) * O.ntiles_cap * 256);
+    O.gstatus = (uint32_t*)take(sizeof(uint32_t) * ((size_t)cap / kOsGatherTile + 1));
+    O.hist = (uint32_t*)take(sizeof(uint32_t) * kOsMaxPasses * 256);
+    O.base = (uint32_t*)take(sizeof(uint32_t) * kOsMaxPasses * 256);
+    O.tile_ctr = (uint32_t*)take(sizeof(uint32_t) * (kOsMaxPasses + 2));
+    return O;
+}
+
+cudaError_t launch_order_gather(const Bufs& b, const OrderBufs& O, bool sort, const double* segs,
+                                const uint32_t* nseg, int32_t* pairs_out, uint32_t* job_out, double* segs_out,
+                                int32_t* segpair_out, bool want_segments, const LaunchCfg& cfg, cudaStream_t st)
+{
+    const unsigned tiles = O.ntiles_cap ? O.ntiles_cap : 1u;
+    OrderBufs o = O;
+    if (!sort) o.passes = 0;
+    k_os_hist<<<cfg.sms * 2, kOsThreads, 0, st>>>(b, o);
     note_launches(1);
-    if (want_segments) {
-        scan_exclusive(seg_offsets, seg_offsets, n, seg_scan_temp, st);
-        k_gather_segs<<<gb, tb, 0, st>>>(perm, n, segs, nseg, seg_offsets, segs_out, segpair_out, d_total_segs);
-        note_launches(1);
+    if (sort) {
+        for (int p = 0; p < o.passes; p++) {
+            k_os_scatter<<<tiles, kOsThreads, 0, st>>>(b, o, p);
+            note_launches(1);
+        }
     }
+    const unsigned gtiles = O.ntiles_cap * (kOsTile / kOsGatherTile);
+    k_os_gather<<<gtiles, kOsGatherTile, 0, st>>>(b, o, segs, nseg, pairs_out, job_out, segs_out, segpair_out,
+                                                  want_segments ? 1 : 0, sort ? 1 : 0);
+    note_launches(1);
     return cudaGetLastError();
 }
 
 // ===========================================================================
 // Launchers
 // ===========================================================================
-__global__ void k_init_frontier(Bufs B)
+// Initial frontier: every pair of cut entries (one thread each) whose world
+// boxes overlap becomes a node pair (or, if both are leaves, a candidate).
+template <bool F64>
+__global__ void __launch_bounds__(256) k_cut_pairs(Bufs B)
 {
-    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= B.njobs) return;
-    const JobDev& J = B.jobs[j];
-    if (J.A.nt == 0 || J.B.nt == 0) return;
-    unsigned p = atomicAdd(&B.cnt->front[0], 1u);
-    B.front[0][p] = make_uint4(j, J.A.root, J.B.root, 0u);
+    using S = typename Prec<F64>::S;
+    Counters* C = B.cnt;
+    for (unsigned job = blockIdx.y; job < B.njobs; job += gridDim.y) {
+        const JobDev& J = B.jobs[job];
+        const unsigned nA = (J.A.nt && J.B.nt) ? J.A.ncut : 0u, nB = J.B.ncut;
+        const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+        const bool have = t < nA * nB;
+        bool front = false, cand = false;
+        uint32_t ra = 0, rb = 0;
+        if (have) {
+            const unsigned i = t / nB, j = t % nB;
+            const S* ba_ = F64 ? (const S*)J.A.cutBox64 : (const S*)J.A.cutBox;
+            const S* bb_ = F64 ? (const S*)J.B.cutBox64 : (const S*)J.B.cutBox;
+            Box<S> ba, bb;
+            for (int k = 0; k < 3; k++) {
+                ba.lo[k] = ba_[6 * i + k];
+                ba.hi[k] = ba_[6 * i + 3 + k];
+                bb.lo[k] = bb_[6 * j + k];
+                bb.hi[k] = bb_[6 * j + 3 + k];
+            }
+            if (!J.pa.identity) world_box(J.pa, ba);
+            if (!J.pb.identity) world_box(J.pb, bb);
+            if (overlap(ba, bb)) {
+                ra = J.A.cutRef[i];
+                rb = J.B.cutRef[j];
+                cand = (ra & kLeaf) && (rb & kLeaf);
+                front = !cand;
+            }
+        }
+        unsigned pf = warp_append(front, &C->front[0]);
+        if (front) {
+            if (pf < B.cap_front) B.front[0][pf] = make_uint4(job, ra, rb, 0u);
+            else atomicOr(&C->overflow, kOvfFrontier);
+        }
+        unsigned pc = warp_append(cand, &C->cand);
+        if (cand) {
+            if (pc < B.cap_cand) B.cand[pc] = make_uint4(job, ra & ~kLeaf, rb & ~kLeaf, 0u);
+            else atomicOr(&C->overflow, kOvfCand);
+        }
+    }
 }
 
-cudaError_t launch_init_frontier(const Bufs& b, cudaStream_t st)
+cudaError_t launch_init_frontier(const Bufs& b, int precision, cudaStream_t st)
 {
-    k_init_frontier<<<(b.njobs + 255) / 256, 256, 0, st>>>(b);
+    dim3 grid((kCutMax * kCutMax + 255) / 256, b.njobs < 65535u ? b.njobs : 65535u);
+    if (precision == 1) k_cut_pairs<true><<<grid, 256, 0, st>>>(b);
+    else k_cut_pairs<false><<<grid, 256, 0, st>>>(b);
     note_launches(1);
     return cudaGetLastError();
 }
@@ -867,11 +1311,10 @@ cudaError_t query_launch(int device, LaunchCfg* cfg)
     GI_TRY(cudaGetDeviceProperties(&prop, device));
     cfg->sms = prop.multiProcessorCount;
     int b32 = 0, b64 = 0;
-    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b32, k_traverse<false>, 256, 0));
-    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b64, k_traverse<true>, 256, 0));
-    int b = b32 < b64 ? b32 : b64;
-    if (b < 1) b = 1;
-    cfg->trav_blocks = b * cfg->sms;
+    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b32, k_traverse<false>, kTravWarps * 32, 0));
+    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b64, k_traverse<true>, kTravWarps * 32, 0));
+    cfg->trav_blocks = (b32 < 1 ? 1 : b32) * cfg->sms;
+    cfg->trav_blocks64 = (b64 < 1 ? 1 : b64) * cfg->sms;
     cfg->trav_threads = 256;
     return cudaSuccess;
 }
@@ -881,11 +1324,22 @@ cudaError_t launch_traverse(const Bufs& b, const LaunchCfg& cfg, int precision, 
     Bufs args = b;
     void* params[] = {&args};
     note_launches(1);
+    cudaError_t e;
     if (precision == 1)
-        return cudaLaunchCooperativeKernel((const void*)k_traverse<true>, dim3(cfg.trav_blocks), dim3(256), params, 0,
-                                           st);
-    return cudaLaunchCooperativeKernel((const void*)k_traverse<false>, dim3(cfg.trav_blocks), dim3(256), params, 0,
-                                       st);
+        e = cudaLaunchCooperativeKernel((const void*)k_traverse<true>, dim3(cfg.trav_blocks64),
+                                        dim3(kTravWarps * 32), params, 0, st);
+    else
+        e = cudaLaunchCooperativeKernel((const void*)k_traverse<false>, dim3(cfg.trav_blocks),
+                                        dim3(kTravWarps * 32), params, 0, st);
+    return e;
+}
+
+cudaError_t launch_filter(const Bufs& b, const LaunchCfg& cfg, int precision, cudaStream_t st)
+{
+    note_launches(1);
+    if (precision == 1) k_filter<true><<<cfg.sms * 8, 256, 0, st>>>(b);
+    else k_filter<false><<<cfg.sms * 8, 256, 0, st>>>(b);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_exact(const Bufs& b, const LaunchCfg& cfg, cudaStream_t st)
@@ -895,13 +1349,9 @@ cudaError_t launch_exact(const Bufs& b, const LaunchCfg& cfg, cudaStream_t st)
     return cudaGetLastError();
 }
 
-cudaError_t launch_segments(const Bufs& b, uint32_t nres, double* segs, uint32_t* nseg, const LaunchCfg& cfg,
-                            cudaStream_t st)
+cudaError_t launch_segments(const Bufs& b, double* segs, uint32_t* nseg, const LaunchCfg& cfg, cudaStream_t st)
 {
-    if (nres == 0) return cudaSuccess;
-    unsigned blocks = (nres + 127) / 128;
-    unsigned maxb = cfg.sms * 8;
-    k_segments<<<blocks < maxb ? blocks : maxb, 128, 0, st>>>(b, nres, segs, nseg);
+    k_segments<<<cfg.sms * 8, 128, 0, st>>>(b, segs, nseg);
     note_launches(1);
     return cudaGetLastError();
 }

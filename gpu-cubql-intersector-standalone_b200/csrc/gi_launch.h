@@ -16,7 +16,10 @@ struct MeshBuffers {
     WNode* nodes = nullptr;
     double* leafBox64 = nullptr;
     WNode64* nodes64 = nullptr;
-    uint32_t nv = 0, nt = 0, nnodes = 0, root = 0;
+    uint32_t* cutRef = nullptr;
+    float* cutBox = nullptr;
+    double* cutBox64 = nullptr;
+    uint32_t nv = 0, nt = 0, nnodes = 0, root = 0, ncut = 0;
     size_t bytes = 0;
 };
 
@@ -30,38 +33,44 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaStream_t st);
 // Intersect launch configuration.
 struct LaunchCfg {
     int sms = 0;
-    int trav_blocks = 0;  // co-resident blocks for the cooperative traversal
+    int trav_blocks = 0;    // co-resident blocks for the cooperative traversal (FP32 boxes)
+    int trav_blocks64 = 0;  // the same for FP64 boxes
     int trav_threads = 256;
 };
 cudaError_t query_launch(int device, LaunchCfg* cfg);
 
 // Runs traversal + first filter stage (cooperative), then the exact stage.
 cudaError_t launch_traverse(const Bufs& b, const LaunchCfg& cfg, int precision, cudaStream_t st);
+cudaError_t launch_filter(const Bufs& b, const LaunchCfg& cfg, int precision, cudaStream_t st);
 cudaError_t launch_exact(const Bufs& b, const LaunchCfg& cfg, cudaStream_t st);
-// Segments for res[0, nres): segs[3*i .. 3*i+2], nseg[i], kind[i].
-cudaError_t launch_segments(const Bufs& b, uint32_t nres, double* segs, uint32_t* nseg, const LaunchCfg& cfg,
-                            cudaStream_t st);
+// Segments of every result (count from the device counters):
+// segs[18*i ..] (up to 3 segments), nseg[i].
+cudaError_t launch_segments(const Bufs& b, double* segs, uint32_t* nseg, const LaunchCfg& cfg, cudaStream_t st);
 
-// Output ordering for nres results: sorted pairs (int2 per pair) and the
-// permutation; per-job counts.  Scratch is taken from `scratch` (bytes).
-struct OrderScratch {
-    void* ptr = nullptr;
-    size_t bytes = 0;
+// Output ordering (radix sort by (job, a, b), sizes from the device counters)
+// and the gather of pairs / jobs / segments in that order.
+constexpr int kOsMaxPasses = 8;
+struct OrderBufs {
+    unsigned long long* keys[2];
+    uint32_t* vals[2];
+    uint32_t* status;    // look-back status: (passes + 1) x ntiles_cap x 256
+    uint32_t* gstatus;   // look-back status of the gather tiles
+    uint32_t* hist;      // kOsMaxPasses x 256 (kept zero between calls)
+    uint32_t* base;      // kOsMaxPasses x 256
+    uint32_t* tile_ctr;  // kOsMaxPasses + 2 (per pass, the gather, the histogram blocks)
+    uint32_t ntiles_cap;
+    int passes;
+    int bits_a, bits_b;
 };
-size_t order_scratch_bytes(uint32_t nres);
-size_t scan_temp_words_host(size_t n);
-cudaError_t launch_order(const uint4* res, uint32_t nres, int bits_a, int bits_b, int bits_job, bool sort,
-                         uint32_t* perm_out, OrderScratch scratch, cudaStream_t st);
-// Gathers pairs / segments in permutation order.
-cudaError_t launch_gather(const uint4* res, const uint32_t* perm, uint32_t nres, const double* segs,
-                          const uint32_t* nseg, int32_t* pairs_out, uint32_t* job_out, double* segs_out,
-                          int32_t* segpair_out, uint32_t* seg_offsets, uint32_t* seg_scan_temp, bool want_segments,
-                          uint32_t* d_total_segs, cudaStream_t st);
-
+size_t order_scratch_bytes(uint32_t cap, int passes);
+OrderBufs make_order_bufs(void* scratch, uint32_t cap, int bits_a, int bits_b, int bits_job);
+cudaError_t launch_order_gather(const Bufs& b, const OrderBufs& O, bool sort, const double* segs,
+                                const uint32_t* nseg, int32_t* pairs_out, uint32_t* job_out, double* segs_out,
+                                int32_t* segpair_out, bool want_segments, const LaunchCfg& cfg, cudaStream_t st);
 // Number of kernels launched by the launchers of this library (monotonic).
 unsigned long long launch_count();
 
-// Init of the frontier: entry i = (i, rootA_i, rootB_i) from the job array.
-cudaError_t launch_init_frontier(const Bufs& b, cudaStream_t st);
+// Initial frontier: all overlapping pairs of the two meshes' depth-3 cuts, per job.
+cudaError_t launch_init_frontier(const Bufs& b, int precision, cudaStream_t st);
 
 }  // namespace gi
