@@ -56,8 +56,12 @@ struct gi_ctx {
     JobDev* d_jobs = nullptr;
     JobDev* h_jobs = nullptr;  // pinned
     uint32_t cap_jobs = 0;
-    uint4* front[2] = {nullptr, nullptr};
-    uint32_t cap_front = 0, cap_front1 = 0;
+    uint4* queue = nullptr;
+    unsigned* qflag = nullptr;
+    uint32_t cap_front = 0, cap_qflag = 0;
+    unsigned* cflag = nullptr;
+    uint32_t cap_cflag = 0;
+    unsigned tag = 0;
     uint4* cand = nullptr;
     uint32_t cap_cand = 0;
     uint4* res = nullptr;
@@ -182,8 +186,9 @@ extern "C" gi_status gi_destroy(gi_ctx* c)
     if (!c) return GI_ERR_INVALID_ARG;
     cudaSetDevice(c->device);
     if (c->st) cudaStreamSynchronize(c->st);
-    void* dev[] = {c->d_cnt, c->d_jobs, c->front[0], c->front[1], c->cand, c->res, c->esc, c->segs, c->nseg,
-                   c->pairs_out, c->job_out, c->segs_out, c->segpair_out, c->order_scratch};
+    void* dev[] = {c->d_cnt,   c->d_jobs,   c->queue,  c->qflag,    c->cand,        c->cflag,
+                   c->res,     c->esc,      c->segs,   c->nseg,     c->pairs_out,   c->job_out,
+                   c->segs_out, c->segpair_out, c->order_scratch};
     for (void* p : dev)
         if (p) cudaFree(p);
     if (c->h_cnt) cudaFreeHost(c->h_cnt);
@@ -506,7 +511,8 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
     memcpy(c->h_jobs, jobs.data(), sizeof(JobDev) * nj);
     CK(c, cudaMemcpyAsync(c->d_jobs, c->h_jobs, sizeof(JobDev) * nj, cudaMemcpyHostToDevice, c->st), "jobs copy");
     const bool tiny = (c->flags & GI_FLAG_TINY_BUFFERS) != 0;
-    uint32_t need_front = std::max<uint32_t>(c->cap_front, tiny ? 64u : std::max<uint32_t>(1u << 20, nj * 64u));
+    uint32_t need_front =
+        std::max<uint32_t>(c->cap_front, tiny ? 64u : (uint32_t)std::min<uint64_t>(std::max<uint64_t>(1u << 21, sumT), 1u << 26));
     uint32_t need_cand =
         std::max<uint32_t>(c->cap_cand, tiny ? 64u : (uint32_t)std::min<uint64_t>(sumT * 2 + 4096, 1u << 22));
     uint32_t need_res = std::max<uint32_t>(c->cap_res, tiny ? 64u : std::max<uint32_t>(need_cand / 4, 1u << 16));
@@ -518,9 +524,17 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
     char* hp = nullptr;
     size_t off_jobs = 0, off_segs = 0, off_segpair = 0;
     for (;; retries++) {
-        CK(c, grow(c->front[0], c->cap_front, need_front, c->st), "frontier");
-        CK(c, grow(c->front[1], c->cap_front1, need_front, c->st), "frontier");
+        CK(c, grow(c->queue, c->cap_front, need_front, c->st), "node queue");
+        if (c->cap_qflag < c->cap_front) {
+            // fresh tag words must not match any call's tag: zero them
+            CK(c, grow(c->qflag, c->cap_qflag, c->cap_front, c->st), "node queue");
+            CK(c, cudaMemsetAsync(c->qflag, 0, sizeof(unsigned) * c->cap_qflag, c->st), "node queue");
+        }
         CK(c, grow(c->cand, c->cap_cand, need_cand, c->st), "candidates");
+        if (c->cap_cflag < c->cap_cand) {
+            CK(c, grow(c->cflag, c->cap_cflag, c->cap_cand, c->st), "candidates");
+            CK(c, cudaMemsetAsync(c->cflag, 0, sizeof(unsigned) * c->cap_cflag, c->st), "candidates");
+        }
         CK(c, grow(c->res, c->cap_res, need_res, c->st), "results");
         CK(c, grow(c->esc, c->cap_esc, need_esc, c->st), "escalations");
         const uint32_t cap = c->cap_res;
@@ -550,11 +564,19 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         Bufs b;
         b.jobs = c->d_jobs;
         b.njobs = nj;
-        b.front[0] = c->front[0];
-        b.front[1] = c->front[1];
-        b.cap_front = std::min(c->cap_front, c->cap_front1);
+        b.queue = c->queue;
+        b.qflag = c->qflag;
+        b.cap_queue = std::min(c->cap_front, c->cap_qflag);
         b.cand = c->cand;
-        b.cap_cand = c->cap_cand;
+        b.cflag = c->cflag;
+        b.cap_cand = std::min(c->cap_cand, c->cap_cflag);
+        if (++c->tag == 0) {
+            // after 2^32 calls the tags wrap: clear the tag words once
+            CK(c, cudaMemsetAsync(c->qflag, 0, sizeof(unsigned) * c->cap_qflag, c->st), "node queue");
+            CK(c, cudaMemsetAsync(c->cflag, 0, sizeof(unsigned) * c->cap_cflag, c->st), "candidates");
+            c->tag = 1;
+        }
+        b.tag = c->tag;
         b.res = c->res;
         b.cap_res = c->cap_res;
         b.esc = c->esc;
@@ -565,7 +587,6 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         CK(c, launch_init_frontier(b, prec, c->st), "init frontier");
         CK(c, cudaEventRecord(c->ev[0], c->st), "event");
         CK(c, launch_traverse(b, c->cfg, prec, c->st), "traverse");
-        CK(c, launch_filter(b, c->cfg, prec, c->st), "filter");
         CK(c, cudaEventRecord(c->ev[1], c->st), "event");
         CK(c, launch_exact(b, c->cfg, c->st), "exact stage");
         CK(c, cudaEventRecord(c->ev[2], c->st), "event");
@@ -599,7 +620,7 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
                "copy segments");
         }
         CK(c, cudaStreamSynchronize(c->st), "sync");
-        if (H.err & kErrBarrier) return set_err(c, GI_ERR_TIMEOUT, "a bounded device wait ran out");
+        if (H.err & kErrTimeout) return set_err(c, GI_ERR_TIMEOUT, "a bounded device wait ran out");
         if (H.err & kErrExactCapacity) return set_err(c, GI_ERR_RANGE, "exact arithmetic capacity exceeded");
         if (H.overflow) {
             if (retries >= 12) return set_err(c, GI_ERR_CAPACITY, "intersection buffers stayed too small");
@@ -607,7 +628,7 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
                 uint64_t v = std::max<uint64_t>((uint64_t)cur * 4, (uint64_t)seen + seen / 2 + 1024);
                 return (uint32_t)std::min<uint64_t>(v, 0x7fffffffu);
             };
-            if (H.overflow & kOvfFrontier) need_front = g4(std::min(c->cap_front, c->cap_front1), 0);
+            if (H.overflow & kOvfFrontier) need_front = g4(c->cap_front, H.q_tail);
             if (H.overflow & kOvfCand) need_cand = g4(c->cap_cand, H.cand);
             if (H.overflow & (kOvfRes | kOvfCand)) need_res = g4(c->cap_res, H.res);
             if (H.overflow & (kOvfEsc | kOvfCand)) need_esc = g4(c->cap_esc, H.esc);

@@ -71,18 +71,25 @@ struct JobDev {
 
 // Device counters of one intersect launch sequence (zeroed by the host).
 struct Counters {
-    unsigned int front[3];  // rotating frontier counts
-    unsigned int cand;      // candidate leaf pairs
-    unsigned int res;       // intersecting pairs
-    unsigned int esc;       // escalated candidate indices
+    // hot counters, each on its own 128-byte line (polled and updated by every warp)
+    unsigned int q_tail;  // node-pair queue: slots reserved (pushed)
+    unsigned int pad0[31];
+    unsigned int q_head;  // slots handed out as tickets
+    unsigned int pad1[31];
+    unsigned int q_done;  // slots processed (children published)
+    unsigned int pad2[31];
+    unsigned int cand;    // candidate slots reserved
+    unsigned int pad3[31];
+    unsigned int c_head;  // candidate slots handed out as tickets
+    unsigned int pad4[31];
+    unsigned int res;     // intersecting pairs
+    unsigned int esc;     // escalated candidate indices
     unsigned int overflow;  // kOvf* bits
     unsigned int err;       // kErr* bits
-    unsigned int levels;
-    unsigned int bar_count;
-    unsigned int bar_gen;
-    unsigned int bar_stop;  // stop snapshot taken inside the grid barrier
-    unsigned int pool_next[2];  // depth-first phase: next pool entry to hand out (per round parity)
+    unsigned int abort_;    // set on overflow or a spent wait: every waiting warp stops
+    unsigned int levels;    // deepest node-pair level + 1
     unsigned int nseg;      // total segments after ordering
+    unsigned int pad5;
     unsigned long long node_pairs;
     unsigned long long filter_decided;
     unsigned long long exact_signs;
@@ -90,22 +97,25 @@ struct Counters {
 };
 
 constexpr unsigned kOvfFrontier = 1u, kOvfCand = 2u, kOvfRes = 4u, kOvfEsc = 8u;
-constexpr unsigned kErrBarrier = 1u, kErrExactCapacity = 2u;
+constexpr unsigned kErrTimeout = 1u, kErrExactCapacity = 2u;
 
 // Per-call buffers handed to the kernels.
 struct Bufs {
     const JobDev* jobs;
     uint32_t njobs;
-    uint4* front[2];
-    uint32_t cap_front;
-    uint4* cand;     // job, leaf posA, leaf posB, 0
+    uint4* queue;     // node pairs: job, node/leaf ref A, node/leaf ref B, level
+    unsigned* qflag;  // per queue slot: tag of the call that published it
+    uint32_t cap_queue;
+    uint4* cand;      // job, leaf posA, leaf posB, 0
+    unsigned* cflag;  // per candidate slot: publishing tag
     uint32_t cap_cand;
-    uint4* res;      // job, triA, triB, 0   (original triangle ids)
+    uint4* res;       // job, triA, triB, 0   (original triangle ids)
     uint32_t cap_res;
-    uint32_t* esc;   // candidate index
+    uint32_t* esc;    // candidate index
     uint32_t cap_esc;
     Counters* cnt;
-    int precision;   // 0 FP32 cascade, 1 FP64
+    unsigned tag;     // nonzero, different for every call on the context
+    int precision;    // 0 FP32 cascade, 1 FP64
 };
 
 }  // namespace gi

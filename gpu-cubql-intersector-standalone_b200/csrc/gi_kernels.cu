@@ -680,48 +680,6 @@ __device__ __forceinline__ unsigned ld_cg_u32(const unsigned* p)
     return __ldcg(p);
 }
 
-constexpr unsigned long long kBarrierSpins = 1ull << 22;
-
-// Software grid barrier for a cooperative launch (all blocks co-resident).
-// The last block to arrive takes a snapshot of the overflow / error flags
-// before it releases the others, so every block leaves with the same stop
-// decision (flags set during the next level cannot split the grid).
-// Every wait is bounded: after kBarrierSpins polls the block records
-// kErrBarrier and stops; the host then reports GI_ERR_TIMEOUT.
-__device__ bool grid_sync(Counters* C)
-{
-    __shared__ unsigned s_stop;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned* genp = &C->bar_gen;
-        unsigned g = *genp;
-        __threadfence();
-        unsigned arrived = atomicAdd(&C->bar_count, 1u);
-        unsigned timed_out = 0;
-        if (arrived == gridDim.x - 1) {
-            unsigned stop = (ld_cg_u32(&C->overflow) | ld_cg_u32(&C->err)) ? 1u : 0u;
-            atomicExch(&C->bar_stop, stop);
-            atomicExch(&C->bar_count, 0u);
-            __threadfence();
-            atomicAdd(&C->bar_gen, 1u);
-        } else {
-            unsigned long long spins = 0;
-            while (*genp == g) {
-                if (++spins > kBarrierSpins) {
-                    atomicOr(&C->err, kErrBarrier);
-                    timed_out = 1;
-                    break;
-                }
-                __nanosleep(32);
-            }
-        }
-        __threadfence();
-        s_stop = ld_cg_u32(&C->bar_stop) | timed_out;
-    }
-    __syncthreads();
-    return s_stop != 0;
-}
-
 template <bool F64>
 __device__ __forceinline__ void load_tri(const MeshDev& M, const DevPose& P, uint32_t pos, double3* out,
                                          uint32_t* tri_id)
@@ -763,114 +721,193 @@ __device__ __forceinline__ void expand_pair(const Bufs& B, const uint4& ent, uns
         }
 }
 
-constexpr int kTravWarps = 8;  // warps per block
+// ---------------------------------------------------------------------------
+// Persistent BVH4 x BVH4 traversal over a device work queue (no grid barrier).
+//
+// Node pairs live in a linear queue.  Producers reserve slots at q_tail with
+// one atomic per warp, write the entries and publish every slot by storing the
+// call's tag in its flag word after a fence.  Consumers work by tickets: a
+// warp takes 32 consecutive slots with one atomicAdd on q_head, polls the 32
+// tag words of its slots (one 128-byte line, so polling has no hot spot) and
+// processes each slot once published, one node pair per lane; it takes a new
+// ticket when all 32 are done.  q_done counts
+// processed slots and advances only after a slot's children are published,
+// so reading q_done and then q_tail and finding them equal proves that the
+// traversal is over: no slot is queued or in flight.
+// Leaf pairs go to the candidate list the same way, and warps whose node slots
+// are not ready run the first filter stage on their candidate ticket, which
+// overlaps the filter with the traversal's critical path.
+// Every wait is bounded; overflow or a spent wait raises the abort flag.
+// ---------------------------------------------------------------------------
+constexpr unsigned kIdleSpins = 1u << 22;  // consecutive idle polls of one warp (~1 s)
 
-// BVH4 x BVH4 traversal in one cooperative launch, breadth first: every level
-// is spread over all lanes (one node pair per lane) and levels are separated
-// by the bounded grid barrier.  It starts from the all-pairs test of the two
-// meshes' depth-3 cuts (k_cut_pairs), so the top levels -- too narrow to fill
-// the GPU -- cost one step instead of three.  Leaf pairs go to the candidate
-// list for k_filter.
+__device__ __forceinline__ unsigned ld_vol(const unsigned* p)
+{
+    return *(const volatile unsigned*)p;
+}
+
+__device__ __forceinline__ void publish(unsigned* flags, unsigned idx, unsigned tag)
+{
+    __threadfence();
+    *(volatile unsigned*)(flags + idx) = tag;
+}
+
+__device__ __forceinline__ unsigned take_ticket(unsigned* head)
+{
+    unsigned b = 0;
+    if ((threadIdx.x & 31) == 0) b = atomicAdd(head, 32u);
+    return __shfl_sync(0xffffffffu, b, 0);
+}
+
 template <bool F64>
-__global__ void __launch_bounds__(kTravWarps * 32) k_traverse(Bufs B)
+__global__ void __launch_bounds__(256, 2) k_traverse(Bufs B)
 {
     Counters* C = B.cnt;
     const unsigned lane = threadIdx.x & 31;
-    const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
-    unsigned long long visited = 0;
-    unsigned level = 0, n = 0;
-    bool stop = false;
-    // ---- phase 1 ----
-    for (; level < 4096; level++) {
-        const unsigned cur = level % 3, nxt = (level + 1) % 3, clr = (level + 2) % 3;
-        n = ld_cg_u32(&C->front[cur]);
-        if (n == 0 || stop) break;
-        if (n > B.cap_front) n = B.cap_front;  // an overflowed count: read only what was stored
-        if (blockIdx.x == 0 && threadIdx.x == 0) C->front[clr] = 0;
-        const uint4* in = B.front[level & 1];
-        uint4* out = B.front[(level + 1) & 1];
-        for (unsigned base = warp * 32; base < n; base += nwarps * 32) {
-            const unsigned e = base + lane;
+    unsigned long long visited = 0, decided = 0;
+    unsigned maxlev = 0, idle = 0, backoff = 32;
+    unsigned nbase = take_ticket(&C->q_head);
+    unsigned npend = 0xffffffffu;  // lanes whose node slot is still to be processed
+    unsigned cbase = 0, cpend = 0;  // candidate ticket (cpend == 0: none held)
+    for (;;) {
+        if (__any_sync(0xffffffffu, ld_vol(&C->abort_) != 0u)) break;
+        // ---- node pairs of the current ticket: poll this warp's own 32 tag words ----
+        const unsigned ns = nbase + lane;
+        const bool nready = ((npend >> lane) & 1u) && ns < B.cap_queue && ld_vol(B.qflag + ns) == B.tag;
+        const unsigned navail = __ballot_sync(0xffffffffu, nready);
+        if (navail) {
+            idle = 0;
+            backoff = 32;
             unsigned fm = 0, cm = 0;
             uint32_t ca[4], cb[4];
             uint4 ent = make_uint4(0u, kEmpty, kEmpty, 0u);
-            if (e < n) {
-                ent = __ldcg(in + e);
+            if (nready) {
+                __threadfence();
+                ent = __ldcg(B.queue + ns);
                 visited++;
+                maxlev = max(maxlev, ent.w);
                 expand_pair<F64>(B, ent, fm, cm, ca, cb);
             }
             unsigned pf, pc;
-            warp_reserve2(__popc(fm), &C->front[nxt], __popc(cm), &C->cand, &pf, &pc);
+            warp_reserve2(__popc(fm), &C->q_tail, __popc(cm), &C->cand, &pf, &pc);
+            const unsigned pf0 = pf, pc0 = pc;
             if (fm | cm) {
+                // entries first, one fence, then the tag words
 #pragma unroll
-                for (int k = 0; k < 16; k++) {
-                    const unsigned bit = 1u << k;
+                for (int q = 0; q < 16; q++) {
+                    const unsigned bit = 1u << q;
                     if (fm & bit) {
-                        if (pf < B.cap_front) out[pf] = make_uint4(ent.x, ca[k >> 2], cb[k & 3], 0u);
-                        else atomicOr(&C->overflow, kOvfFrontier);
+                        if (pf < B.cap_queue) B.queue[pf] = make_uint4(ent.x, ca[q >> 2], cb[q & 3], ent.w + 1u);
                         pf++;
                     }
                     if (cm & bit) {
-                        if (pc < B.cap_cand)
-                            B.cand[pc] = make_uint4(ent.x, ca[k >> 2] & ~kLeaf, cb[k & 3] & ~kLeaf, 0u);
-                        else atomicOr(&C->overflow, kOvfCand);
+                        if (pc < B.cap_cand) B.cand[pc] = make_uint4(ent.x, ca[q >> 2] & ~kLeaf, cb[q & 3] & ~kLeaf, 0u);
                         pc++;
                     }
                 }
+                __threadfence();
+                for (unsigned q = pf0; q < pf; q++) {
+                    if (q < B.cap_queue) *(volatile unsigned*)(B.qflag + q) = B.tag;
+                    else {
+                        atomicOr(&C->overflow, kOvfFrontier);
+                        atomicExch(&C->abort_, 1u);
+                    }
+                }
+                for (unsigned q = pc0; q < pc; q++) {
+                    if (q < B.cap_cand) *(volatile unsigned*)(B.cflag + q) = B.tag;
+                    else {
+                        atomicOr(&C->overflow, kOvfCand);
+                        atomicExch(&C->abort_, 1u);
+                    }
+                }
             }
+            __syncwarp();
+            if (lane == 0) atomicAdd(&C->q_done, (unsigned)__popc(navail));
+            npend &= ~navail;
+            if (npend == 0) {
+                nbase = take_ticket(&C->q_head);
+                npend = 0xffffffffu;
+            }
+            continue;
         }
-        stop = grid_sync(C);
+        // ---- candidates of the current candidate ticket ----
+        if (cpend == 0) {
+            cbase = take_ticket(&C->c_head);
+            cpend = 0xffffffffu;
+        }
+        const unsigned i = cbase + lane;
+        const bool cready = ((cpend >> lane) & 1u) && i < B.cap_cand && ld_vol(B.cflag + i) == B.tag;
+        const unsigned cavail = __ballot_sync(0xffffffffu, cready);
+        if (cavail) {
+            idle = 0;
+            backoff = 32;
+            int dec = DEC_NO;
+            uint32_t ta = 0, tb = 0, job = 0;
+            if (cready) {
+                __threadfence();
+                const uint4 c = __ldcg(B.cand + i);
+                job = c.x;
+                const JobDev& J = B.jobs[job];
+                double3 P[3], Q[3];
+                load_tri<F64>(J.A, J.pa, c.y, P, &ta);
+                load_tri<F64>(J.B, J.pb, c.z, Q, &tb);
+                if constexpr (F64) dec = classify_fast<double>(P, Q);
+                else dec = classify_fast<float>(P, Q);
+                decided += (dec != DEC_ESC);
+            }
+            const bool act = (cavail >> lane) & 1u;
+            const bool yes = act && dec == DEC_YES;
+            const bool esc = act && dec == DEC_ESC;
+            unsigned pr = warp_append(yes, &C->res);
+            if (yes) {
+                if (pr < B.cap_res) B.res[pr] = make_uint4(job, ta, tb, 0u);
+                else atomicOr(&C->overflow, kOvfRes);
+            }
+            unsigned pe = warp_append(esc, &C->esc);
+            if (esc) {
+                if (pe < B.cap_esc) B.esc[pe] = i;
+                else atomicOr(&C->overflow, kOvfEsc);
+            }
+            cpend &= ~cavail;
+            continue;
+        }
+        // ---- nothing ready: over, or wait.  Traversal over (q_done == q_tail,
+        // read in that order) means no slot will be published any more: the
+        // warp is done once none of its pending candidate slots lies below the
+        // final candidate count (its pending node slots are then all >= q_tail).
+        if ((idle & 3u) == 3u) {
+            unsigned over = 0, ncand = 0;
+            if (lane == 0) {
+                const unsigned d = ld_vol(&C->q_done);
+                __threadfence();
+                const unsigned t = ld_vol(&C->q_tail);
+                over = d == t;
+                ncand = min(ld_vol(&C->cand), B.cap_cand);
+            }
+            over = __shfl_sync(0xffffffffu, over, 0);
+            ncand = __shfl_sync(0xffffffffu, ncand, 0);
+            if (over && !__any_sync(0xffffffffu, ((cpend >> lane) & 1u) && i < ncand)) break;
+        }
+        if (++idle > kIdleSpins) {
+            if (lane == 0) {
+                atomicOr(&C->err, kErrTimeout);
+                atomicExch(&C->abort_, 1u);
+            }
+            break;
+        }
+        __nanosleep(backoff);
+        backoff = min(backoff * 2u, 256u);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) C->levels = level;
-    for (int o = 16; o > 0; o >>= 1) visited += __shfl_xor_sync(0xffffffffu, visited, o);
-    if (lane == 0 && visited) atomicAdd(&C->node_pairs, visited);
-}
-
-// First filter stage over all leaf pairs: FP32 (or FP64) semi-static filter of
-// the general-position case; decided pairs are final, the rest escalate.
-template <bool F64>
-__global__ void __launch_bounds__(256) k_filter(Bufs B)
-{
-    Counters* C = B.cnt;
-    const unsigned lane = threadIdx.x & 31;
-    const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
-    if (ld_cg_u32(&C->overflow) || ld_cg_u32(&C->err)) return;
-    unsigned nc = ld_cg_u32(&C->cand);
-    if (nc > B.cap_cand) nc = B.cap_cand;
-    unsigned long long decided = 0;
-    for (unsigned base = warp * 32; base < nc; base += nwarps * 32) {
-        const unsigned i = base + lane;
-        const bool have = i < nc;
-        int dec = DEC_NO;
-        uint32_t ta = 0, tb = 0, job = 0;
-        if (have) {
-            uint4 c = __ldcg(B.cand + i);
-            job = c.x;
-            const JobDev& J = B.jobs[job];
-            double3 P[3], Q[3];
-            load_tri<F64>(J.A, J.pa, c.y, P, &ta);
-            load_tri<F64>(J.B, J.pb, c.z, Q, &tb);
-            if constexpr (F64) dec = classify_fast<double>(P, Q);
-            else dec = classify_fast<float>(P, Q);
-            decided += (dec != DEC_ESC);
-        }
-        const bool yes = have && dec == DEC_YES;
-        const bool esc = have && dec == DEC_ESC;
-        unsigned pr = warp_append(yes, &C->res);
-        if (yes) {
-            if (pr < B.cap_res) B.res[pr] = make_uint4(job, ta, tb, 0u);
-            else atomicOr(&C->overflow, kOvfRes);
-        }
-        unsigned pe = warp_append(esc, &C->esc);
-        if (esc) {
-            if (pe < B.cap_esc) B.esc[pe] = i;
-            else atomicOr(&C->overflow, kOvfEsc);
-        }
+    for (int o = 16; o > 0; o >>= 1) {
+        visited += __shfl_xor_sync(0xffffffffu, visited, o);
+        decided += __shfl_xor_sync(0xffffffffu, decided, o);
+        maxlev = max(maxlev, __shfl_xor_sync(0xffffffffu, maxlev, o));
     }
-    for (int o = 16; o > 0; o >>= 1) decided += __shfl_xor_sync(0xffffffffu, decided, o);
-    if (lane == 0 && decided) atomicAdd(&C->filter_decided, decided);
+    if (lane == 0) {
+        if (visited) atomicAdd(&C->node_pairs, visited);
+        if (decided) atomicAdd(&C->filter_decided, decided);
+        atomicMax(&C->levels, maxlev + 1u);
+    }
 }
 
 // ===========================================================================
@@ -1058,7 +1095,7 @@ __device__ __forceinline__ bool lookback(unsigned* status, unsigned tile, unsign
             unsigned long long spins = 0;
             while ((v & ~kCountMask) == 0u) {
                 if (++spins > kLookbackSpins) {
-                    atomicOr(err, kErrBarrier);
+                    atomicOr(err, kErrTimeout);
                     *excl_out = 0;
                     return false;
                 }
@@ -1283,15 +1320,25 @@ __global__ void __launch_bounds__(256) k_cut_pairs(Bufs B)
                 front = !cand;
             }
         }
-        unsigned pf = warp_append(front, &C->front[0]);
+        unsigned pf = warp_append(front, &C->q_tail);
         if (front) {
-            if (pf < B.cap_front) B.front[0][pf] = make_uint4(job, ra, rb, 0u);
-            else atomicOr(&C->overflow, kOvfFrontier);
+            if (pf < B.cap_queue) {
+                B.queue[pf] = make_uint4(job, ra, rb, 0u);
+                publish(B.qflag, pf, B.tag);
+            } else {
+                atomicOr(&C->overflow, kOvfFrontier);
+                atomicExch(&C->abort_, 1u);
+            }
         }
         unsigned pc = warp_append(cand, &C->cand);
         if (cand) {
-            if (pc < B.cap_cand) B.cand[pc] = make_uint4(job, ra & ~kLeaf, rb & ~kLeaf, 0u);
-            else atomicOr(&C->overflow, kOvfCand);
+            if (pc < B.cap_cand) {
+                B.cand[pc] = make_uint4(job, ra & ~kLeaf, rb & ~kLeaf, 0u);
+                publish(B.cflag, pc, B.tag);
+            } else {
+                atomicOr(&C->overflow, kOvfCand);
+                atomicExch(&C->abort_, 1u);
+            }
         }
     }
 }
@@ -1311,34 +1358,22 @@ cudaError_t query_launch(int device, LaunchCfg* cfg)
     GI_TRY(cudaGetDeviceProperties(&prop, device));
     cfg->sms = prop.multiProcessorCount;
     int b32 = 0, b64 = 0;
-    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b32, k_traverse<false>, kTravWarps * 32, 0));
-    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b64, k_traverse<true>, kTravWarps * 32, 0));
+    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b32, k_traverse<false>, 256, 0));
+    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b64, k_traverse<true>, 256, 0));
     cfg->trav_blocks = (b32 < 1 ? 1 : b32) * cfg->sms;
     cfg->trav_blocks64 = (b64 < 1 ? 1 : b64) * cfg->sms;
     cfg->trav_threads = 256;
     return cudaSuccess;
 }
 
+// The persistent traversal needs no co-residency (nothing waits on a block
+// that has not started); the grid is the resident block count so that every
+// warp is live from the start.
 cudaError_t launch_traverse(const Bufs& b, const LaunchCfg& cfg, int precision, cudaStream_t st)
 {
-    Bufs args = b;
-    void* params[] = {&args};
     note_launches(1);
-    cudaError_t e;
-    if (precision == 1)
-        e = cudaLaunchCooperativeKernel((const void*)k_traverse<true>, dim3(cfg.trav_blocks64),
-                                        dim3(kTravWarps * 32), params, 0, st);
-    else
-        e = cudaLaunchCooperativeKernel((const void*)k_traverse<false>, dim3(cfg.trav_blocks),
-                                        dim3(kTravWarps * 32), params, 0, st);
-    return e;
-}
-
-cudaError_t launch_filter(const Bufs& b, const LaunchCfg& cfg, int precision, cudaStream_t st)
-{
-    note_launches(1);
-    if (precision == 1) k_filter<true><<<cfg.sms * 8, 256, 0, st>>>(b);
-    else k_filter<false><<<cfg.sms * 8, 256, 0, st>>>(b);
+    if (precision == 1) k_traverse<true><<<cfg.trav_blocks64, 256, 0, st>>>(b);
+    else k_traverse<false><<<cfg.trav_blocks, 256, 0, st>>>(b);
     return cudaGetLastError();
 }
 

@@ -39,9 +39,8 @@ struct LaunchCfg {
 };
 cudaError_t query_launch(int device, LaunchCfg* cfg);
 
-// Runs traversal + first filter stage (cooperative), then the exact stage.
+// Traversal + first filter stage (persistent, work queue), then the exact stage.
 cudaError_t launch_traverse(const Bufs& b, const LaunchCfg& cfg, int precision, cudaStream_t st);
-cudaError_t launch_filter(const Bufs& b, const LaunchCfg& cfg, int precision, cudaStream_t st);
 cudaError_t launch_exact(const Bufs& b, const LaunchCfg& cfg, cudaStream_t st);
 // Segments of every result (count from the device counters):
 // segs[18*i ..] (up to 3 segments), nseg[i].
