@@ -169,7 +169,7 @@ __device__ __forceinline__ int lone_index(const int s[3])
 // First stage: decides the general-position case (every vertex strictly off the
 // other triangle's plane) with filtered signs; everything else escalates.
 template <class T>
-__device__ int classify_fast(const double3* P, const double3* Q)
+static __device__ int classify_fast(const double3* P, const double3* Q)
 {
     Plane<T> pp = make_plane<T>(vdiff<T>(P[1], P[0]), vdiff<T>(P[2], P[0]));
     if (!pp.proper) return DEC_ESC;
@@ -316,7 +316,7 @@ struct Shape {
     int e0, e1;
 };
 
-__device__ __noinline__ Shape tri_shape(const double3* pts, int base, ExactSigns& S)
+static __device__ __noinline__ Shape tri_shape(const double3* pts, int base, ExactSigns& S)
 {
     Shape s;
     s.drop = -1;
@@ -364,7 +364,7 @@ __device__ __noinline__ Shape tri_shape(const double3* pts, int base, ExactSigns
     return s;
 }
 
-__device__ __noinline__ bool pt_in_tri2d(const double3* pts, int p, int t0, int drop, ExactSigns& S)
+static __device__ __noinline__ bool pt_in_tri2d(const double3* pts, int p, int t0, int drop, ExactSigns& S)
 {
     int s0 = S.o2(pts[t0], pts[t0 + 1], pts[p], drop);
     int s1 = S.o2(pts[t0 + 1], pts[t0 + 2], pts[p], drop);
@@ -372,7 +372,7 @@ __device__ __noinline__ bool pt_in_tri2d(const double3* pts, int p, int t0, int 
     bool pos = s0 > 0 || s1 > 0 || s2 > 0, neg = s0 < 0 || s1 < 0 || s2 < 0;
     return !(pos && neg);
 }
-__device__ __noinline__ bool collinear3(const double3* pts, int a, int b, int c, ExactSigns& S)
+static __device__ __noinline__ bool collinear3(const double3* pts, int a, int b, int c, ExactSigns& S)
 {
     return S.o2(pts[a], pts[b], pts[c], 0) == 0 && S.o2(pts[a], pts[b], pts[c], 1) == 0 &&
            S.o2(pts[a], pts[b], pts[c], 2) == 0;
@@ -384,7 +384,7 @@ struct ParamPt {
     int kind;  // 0: vertex w (index pt.a), 1: cut by 2D line (p,q)
 };
 // exact value of the parameter as num/den on the grid of pts (scale-free ratio)
-__device__ __noinline__ bool param_value(const double3* pts, const ParamPt& x, int e0, int e1, int m,
+static __device__ __noinline__ bool param_value(const double3* pts, const ParamPt& x, int e0, int e1, int m,
                                          const ex::Grid& g, ex::Big& num, ex::Big& den)
 {
     using namespace ex;
@@ -410,7 +410,7 @@ __device__ __noinline__ bool param_value(const double3* pts, const ParamPt& x, i
     ok &= big_addsub(num, sb, -1, den);
     return ok;
 }
-__device__ __noinline__ int param_cmp(const double3* pts, const ParamPt& x, const ParamPt& y, int e0, int e1,
+static __device__ __noinline__ int param_cmp(const double3* pts, const ParamPt& x, const ParamPt& y, int e0, int e1,
                                       int m, unsigned* err)
 {
     using namespace ex;
@@ -447,7 +447,7 @@ __device__ __forceinline__ int seg_axis(const double3& a, const double3& b)
     return m;
 }
 
-__device__ __noinline__ void seg_tri(const double3* pts, int e0, int e1, int t0, int drop, TTRes& r, ExactSigns& S)
+static __device__ __noinline__ void seg_tri(const double3* pts, int e0, int e1, int t0, int drop, TTRes& r, ExactSigns& S)
 {
     int s0 = S.o3(pts[t0], pts[t0 + 1], pts[t0 + 2], pts[e0]);
     int s1 = S.o3(pts[t0], pts[t0 + 1], pts[t0 + 2], pts[e1]);
@@ -506,7 +506,7 @@ __device__ __noinline__ void seg_tri(const double3* pts, int e0, int e1, int t0,
     }
 }
 
-__device__ __noinline__ void seg_seg(const double3* pts, int e0, int e1, int f0, int f1, TTRes& r, ExactSigns& S)
+static __device__ __noinline__ void seg_seg(const double3* pts, int e0, int e1, int f0, int f1, TTRes& r, ExactSigns& S)
 {
     r.n = 0;
     r.kind = KIND_NONE;
@@ -556,7 +556,7 @@ __device__ __noinline__ void seg_seg(const double3* pts, int e0, int e1, int f0,
     }
 }
 
-__device__ __noinline__ void coplanar_tt(const double3* pts, int drop, TTRes& r, ExactSigns& S)
+static __device__ __noinline__ void coplanar_tt(const double3* pts, int drop, TTRes& r, ExactSigns& S)
 {
     int sig1 = S.o2(pts[0], pts[1], pts[2], drop);
     int sig2 = S.o2(pts[3], pts[4], pts[5], drop);
@@ -681,7 +681,7 @@ __device__ __forceinline__ int build_interval(int T, const int s[3], int O, Line
     return 2;
 }
 
-__device__ __noinline__ void general_tt(const double3* pts, const int s1[3], const int s2[3], TTRes& r, ExactSigns& S)
+static __device__ __noinline__ void general_tt(const double3* pts, const int s1[3], const int s2[3], TTRes& r, ExactSigns& S)
 {
     LinePt I1[2], I2[2];
     int n1 = build_interval(0, s1, 3, I1);
@@ -705,7 +705,7 @@ __device__ __noinline__ void general_tt(const double3* pts, const int s1[3], con
     r.kind = r.n == 0 ? KIND_NONE : (r.n == 1 ? KIND_POINT : KIND_SEGMENT);
 }
 
-__device__ __noinline__ void classify_exact(const double3* pts, TTRes& r, ExactSigns& S)
+static __device__ __noinline__ void classify_exact(const double3* pts, TTRes& r, ExactSigns& S)
 {
     r.n = 0;
     r.kind = KIND_NONE;
@@ -828,7 +828,7 @@ __device__ __forceinline__ dd dd_div(dd x, dd y)  // DWDivDW2, rel. err <= 15u^2
 
 // orient3d(p,q,r,x) = det[p-x; q-x; r-x] in double-double; *perm receives the
 // permanent.  |error| <= 21u^2 perm (4u^2 products, 3u^2 sums); callers use 64u^2.
-__device__ __noinline__ dd o3_dd(const double3& p, const double3& q, const double3& r, const double3& x, double* perm)
+static __device__ __noinline__ dd o3_dd(const double3& p, const double3& q, const double3& r, const double3& x, double* perm)
 {
     dd adx = two_diff_dd(p.x, x.x), ady = two_diff_dd(p.y, x.y), adz = two_diff_dd(p.z, x.z);
     dd bdx = two_diff_dd(q.x, x.x), bdy = two_diff_dd(q.y, x.y), bdz = two_diff_dd(q.z, x.z);
@@ -843,7 +843,7 @@ __device__ __noinline__ dd o3_dd(const double3& p, const double3& q, const doubl
     return det;
 }
 // orient2d(p,q,x) on the projection dropping `drop`; |error| <= 15u^2 perm
-__device__ __noinline__ dd o2_dd(const double3& p, const double3& q, const double3& x, int drop, double* perm)
+static __device__ __noinline__ dd o2_dd(const double3& p, const double3& q, const double3& x, int drop, double* perm)
 {
     const double* P = &p.x;
     const double* Q = &q.x;
@@ -876,7 +876,7 @@ __device__ __forceinline__ bool ziv_round(dd x, double err, double* out)
     return false;
 }
 
-__device__ __noinline__ bool construct_exact(const double3* pts, const SymPt& s, double3& out)
+static __device__ __noinline__ bool construct_exact(const double3* pts, const SymPt& s, double3& out)
 {
     using namespace ex;
     int idx[5] = {s.p, s.q, s.r, s.a, s.b};
@@ -917,7 +917,7 @@ __device__ __noinline__ bool construct_exact(const double3* pts, const SymPt& s,
 }
 
 // returns false only on exact-arithmetic capacity failure
-__device__ __noinline__ bool construct_point(const double3* pts, const SymPt& s, double3& out, unsigned long long* nexact)
+static __device__ __noinline__ bool construct_point(const double3* pts, const SymPt& s, double3& out, unsigned long long* nexact)
 {
     if (s.kind == PK_VERTEX) {
         out = pts[s.a];

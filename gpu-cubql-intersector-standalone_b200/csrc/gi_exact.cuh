@@ -267,7 +267,7 @@ __device__ __forceinline__ long long scaled_i64(const DBits& d, int E)
 }
 
 // det[a-d; b-d; c-d] exact sign. err |= kErrExactCapacity if outside capacity.
-__device__ __noinline__ int o3_exact_sign(const double* a, const double* b, const double* c, const double* d, unsigned* err)
+static __device__ __noinline__ int o3_exact_sign(const double* a, const double* b, const double* c, const double* d, unsigned* err)
 {
     DBits bits[12];
     const double* P[4] = {a, b, c, d};
@@ -319,7 +319,7 @@ __device__ __noinline__ int o3_exact_sign(const double* a, const double* b, cons
     return big_sign(acc);
 }
 
-__device__ __noinline__ int o2_exact_sign(const double* a, const double* b, const double* c, int drop, unsigned* err)
+static __device__ __noinline__ int o2_exact_sign(const double* a, const double* b, const double* c, int drop, unsigned* err)
 {
     int u = (drop + 1) % 3, v = (drop + 2) % 3;
     double q[6] = {a[u], a[v], b[u], b[v], c[u], c[v]};
@@ -369,7 +369,7 @@ __device__ __noinline__ int o2_exact_sign(const double* a, const double* b, cons
 // ---- exact construction ------------------------------------------------------
 // Exact side values on a grid: for PLANE points sa = det[p-a; q-a; r-a] (scale 2^3E);
 // for LINE2 points sa = orient2d(p, q, a) (scale 2^2E).
-__device__ __noinline__ bool big_o3_value(const Big* P, const Big* Q, const Big* R, const Big* X, Big& out)
+static __device__ __noinline__ bool big_o3_value(const Big* P, const Big* Q, const Big* R, const Big* X, Big& out)
 {
     // det[P-X; Q-X; R-X]
     Big d[9];
@@ -392,7 +392,7 @@ __device__ __noinline__ bool big_o3_value(const Big* P, const Big* Q, const Big*
     }
     return ok;
 }
-__device__ __noinline__ bool big_o2_value(const Big* P, const Big* Q, const Big* X, int drop, Big& out)
+static __device__ __noinline__ bool big_o2_value(const Big* P, const Big* Q, const Big* X, int drop, Big& out)
 {
     int u = (drop + 1) % 3, v = (drop + 2) % 3;
     Big acu, acv, bcu, bcv, t1, t2;
@@ -408,7 +408,7 @@ __device__ __noinline__ bool big_o2_value(const Big* P, const Big* Q, const Big*
 }
 
 // Round (N / D) * 2^E to the nearest double (ties to even). D != 0.
-__device__ __noinline__ double round_quot(const Big& N, const Big& D, int E, bool* ok)
+static __device__ __noinline__ double round_quot(const Big& N, const Big& D, int E, bool* ok)
 {
     if (N.n == 0) return 0.0;
     int neg = N.neg ^ D.neg;

@@ -68,6 +68,7 @@ cudaError_t launch_order_gather(const Bufs& b, const OrderBufs& O, bool sort, co
                                 int32_t* segpair_out, bool want_segments, const LaunchCfg& cfg, cudaStream_t st);
 // Number of kernels launched by the launchers of this library (monotonic).
 unsigned long long launch_count();
+void note_launches(unsigned n);
 
 // Initial frontier: all overlapping pairs of the two meshes' depth-3 cuts, per job.
 cudaError_t launch_init_frontier(const Bufs& b, int precision, cudaStream_t st);

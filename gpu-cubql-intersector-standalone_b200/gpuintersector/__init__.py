@@ -187,6 +187,14 @@ class Context:
         self.check(rc, "gi_intersect_oneshot")
         return Result(r)
 
+    def classify_pairs(self, A, B, pose_a, pose_b, d_pairs_ptr, npairs, d_out_ptr, precision=GI_PREC_FP32_CASCADE):
+        """Exact test of npairs candidate pairs (device pointers: int32 pairs, uint8 out)."""
+        rc = self._lib.gi_classify_pairs(self.handle, A.handle, ctypes.byref(pose_a) if pose_a is not None else None,
+                                         B.handle, ctypes.byref(pose_b) if pose_b is not None else None,
+                                         ctypes.c_void_p(d_pairs_ptr), npairs, int(precision),
+                                         ctypes.c_void_p(d_out_ptr))
+        self.check(rc, "gi_classify_pairs")
+
     def server(self, max_inflight=256, want_segments=True, precision=GI_PREC_FP32_CASCADE):
         return Server(self, max_inflight, want_segments, precision)
 

@@ -26,6 +26,7 @@ EXPORTED = [
     "gi_mesh_upload", "gi_mesh_upload_device", "gi_mesh_release", "gi_mesh_info",
     "gi_pose_identity", "gi_pose_from_euler_deg", "gi_pose_apply",
     "gi_intersect_opts_default", "gi_intersect", "gi_intersect_oneshot", "gi_intersect_batch",
+    "gi_classify_pairs",
     "gi_result_pairs", "gi_result_segments", "gi_result_stats", "gi_result_free",
     "gi_server_start", "gi_server_submit", "gi_server_poll", "gi_server_wait", "gi_server_stop",
 ]
@@ -104,6 +105,8 @@ def load(path=None):
                                   ctypes.POINTER(IntersectOpts), ctypes.POINTER(vp)], st),
         "gi_intersect_batch": ([vp, ctypes.POINTER(PairJob), ctypes.c_uint32, ctypes.POINTER(IntersectOpts),
                                 ctypes.POINTER(vp)], st),
+        "gi_classify_pairs": ([vp, vp, ctypes.POINTER(Pose), vp, ctypes.POINTER(Pose), vp, ctypes.c_uint32,
+                               ctypes.c_int32, vp], st),
         "gi_result_pairs": ([vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)), ctypes.POINTER(ctypes.c_uint64)], st),
         "gi_result_segments": ([vp, ctypes.POINTER(dp), ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)),
                                 ctypes.POINTER(ctypes.c_uint64)], st),

@@ -180,6 +180,18 @@ gi_status gi_intersect_oneshot(gi_ctx* ctx, const double* vA, uint32_t nvA, cons
 gi_status gi_intersect_batch(gi_ctx* ctx, const gi_pair_job* jobs, uint32_t njobs, const gi_intersect_opts* opts,
                              gi_result** out);
 
+/* Exact closed-triangle test over an explicit candidate list: d_out[i] = 1 iff
+ * A[d_pairs[2i]] and B[d_pairs[2i+1]] intersect under the poses.  Replaces the
+ * reference's predicate kernels over a pair list plus its CPU fallback
+ * (src/GPU_exact_predicates/OriginShiftedFloatPredicate.cu:7-26,
+ *  src/GPU_exact_predicates/DoublePredicate.cu:166-201, src/CPU/YellowFilter.h:80-137).
+ * d_pairs (2 int32 per pair) and d_out (1 byte per pair) are device pointers on
+ * the context's device; scratch for the escalated pairs comes from the
+ * context's stream-ordered pool.  Bad indices give GI_ERR_INVALID_ARG. */
+gi_status gi_classify_pairs(gi_ctx* ctx, const gi_mesh* A, const gi_pose* pose_a, const gi_mesh* B,
+                            const gi_pose* pose_b, const int32_t* d_pairs, uint32_t npairs, int32_t precision_mode,
+                            uint8_t* d_out);
+
 /* ---- results -------------------------------------------------------------- */
 /* pairs_ab: 2 int32 per pair (faceA, faceB); pointer valid until gi_result_free. */
 gi_status gi_result_pairs(const gi_result* r, const int32_t** pairs_ab, uint64_t* n);

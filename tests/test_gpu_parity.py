@@ -349,3 +349,41 @@ def test_server_results_alone_and_in_mix(ctx, gi):
         assert np.array_equal(a.segments, m.segments)
     A.release()
     B.release()
+
+
+def _candidate_pairs(cfg, oc, rng, n_random=4000):
+    """Exact-box-overlapping pairs from the oracle's BVH plus random pairs."""
+    ref = oc.intersect_meshes(cfg["vA"], cfg["tA"], oracle_pose(oc, cfg["poseA"]), cfg["vB"], cfg["tB"],
+                              oracle_pose(oc, cfg["poseB"]), want_segments=False)
+    rand = np.stack([rng.integers(0, cfg["tA"].shape[0], n_random), rng.integers(0, cfg["tB"].shape[0], n_random)],
+                    axis=1)
+    return np.concatenate([ref["pairs"], rand]).astype(np.int32), ref
+
+
+def test_classify_pairs_vs_oracle(ctx, gi, oc):
+    """gi_classify_pairs over an explicit list equals the oracle's exact test."""
+    import torch
+    from gpuintersector import meshgen as mg
+
+    cfg = mg.config1(seed=11)
+    rng = np.random.default_rng(3)
+    pairs, ref = _candidate_pairs(cfg, oc, rng)
+    wA = oc.transform(oracle_pose(oc, cfg["poseA"]), cfg["vA"])
+    wB = oc.transform(oracle_pose(oc, cfg["poseB"]), cfg["vB"])
+    exp = np.array([oc.tri_tri_intersect(wA[cfg["tA"][a]], wB[cfg["tB"][b]]) for a, b in pairs], dtype=np.uint8)
+    A, B = ctx.upload(cfg["vA"], cfg["tA"]), ctx.upload(cfg["vB"], cfg["tB"])
+    d_pairs = torch.from_numpy(pairs).cuda()
+    for prec in (0, 1):
+        d_out = torch.full((len(pairs),), 7, dtype=torch.uint8, device="cuda")
+        ctx.classify_pairs(A, B, None, gi_pose(gi, cfg["poseB"]), d_pairs.data_ptr(), len(pairs), d_out.data_ptr(),
+                           precision=prec)
+        torch.cuda.synchronize()
+        assert np.array_equal(d_out.cpu().numpy(), exp)
+    assert exp[:len(ref["pairs"])].all()
+    bad = torch.tensor([[0, cfg["tB"].shape[0]]], dtype=torch.int32, device="cuda")
+    out = torch.zeros(1, dtype=torch.uint8, device="cuda")
+    with pytest.raises(gi.GIError) as e:
+        ctx.classify_pairs(A, B, None, None, bad.data_ptr(), 1, out.data_ptr())
+    assert e.value.status == 1
+    A.release()
+    B.release()
