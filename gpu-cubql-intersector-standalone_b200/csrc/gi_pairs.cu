@@ -150,3 +150,73 @@ extern "C" gi_status gi_classify_pairs(gi_ctx* c, const gi_mesh* A, const gi_pos
     cudaFreeAsync(scratch, c->st);
     return pairs_status(c, e, herr);
 }
+
+// ---------------------------------------------------------------------------
+// gi_classify_pairs_noalloc: the same cascade with scratch that is never
+// allocated at call time.
+//
+// Some callers cannot allocate device memory while they run: a pose-update
+// control loop that reserved its whole memory budget at start-up and must not
+// grow a pool afterwards, a host framework whose caching allocator already owns
+// the free HBM, or a latency-bound loop that cannot take the stall of a pool
+// growing or trimming on its stream.  For them the escalation list lives in one
+// fixed array in the module's device memory instead of the context's pool.
+//
+// Limits and rules:
+//  * at most GI_NOALLOC_MAX_PAIRS pairs per call; more is rejected with
+//    GI_ERR_CAPACITY before any work is queued;
+//  * the array is one per device, shared by every context on that device, so
+//    calls whose device work overlaps in time (two threads, or two contexts, on
+//    the same device at once) race on it and their results are undefined.
+//    A call blocks until its work is done, so calls made one after another
+//    from the host are safe;
+//  * the first call on a device looks up the array's device address (with that
+//    device current) and keeps it; make that first call before any stream
+//    capture begins.
+//  * the two head words (escalation count, error bits) must start at zero;
+//    each call clears them on its stream with a memset before the kernels.
+constexpr uint32_t kNoAllocMaxPairs = GI_NOALLOC_MAX_PAIRS;
+static_assert(kNoAllocMaxPairs == (1u << 20), "header limit and scratch size disagree");
+static __device__ __align__(256) unsigned g_pairs_scratch[kPairsScratchHead + kNoAllocMaxPairs];  // 4 MiB + 256 B
+
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static unsigned* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_pairs_scratch on c->device (which must be current).
+static gi_status noalloc_scratch(gi_ctx* c, unsigned** out)
+{
+    if (c->device < 0 || c->device >= kNoAllocMaxDevices)
+        return set_err(c, GI_ERR_INVALID_ARG, "device ordinal beyond the no-alloc scratch table");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[c->device]) {
+        unsigned* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_pairs_scratch);
+        if (e != cudaSuccess || !ptr) return set_err(c, GI_ERR_CUDA, "no-alloc scratch symbol address", e);
+        g_noalloc_ptr[c->device] = ptr;
+    }
+    *out = g_noalloc_ptr[c->device];
+    return GI_OK;
+}
+
+extern "C" gi_status gi_classify_pairs_noalloc(gi_ctx* c, const gi_mesh* A, const gi_pose* pa, const gi_mesh* B,
+                                               const gi_pose* pb, const int32_t* d_pairs, uint32_t npairs,
+                                               int32_t precision_mode, uint8_t* d_out)
+{
+    if (!c || !A || !B || A->ctx != c || B->ctx != c || (npairs && (!d_pairs || !d_out))) return GI_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (npairs > kNoAllocMaxPairs)
+        return set_err(c, GI_ERR_CAPACITY, "npairs exceeds the fixed scratch of gi_classify_pairs_noalloc "
+                                           "(at most GI_NOALLOC_MAX_PAIRS = 1048576 pairs per call)");
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return set_err(c, GI_ERR_CUDA, "set device", e);
+    JobDev J;
+    gi_status s = pairs_job(c, A, pa, B, pb, &J);
+    if (s != GI_OK) return s;
+    unsigned* scratch = nullptr;
+    s = noalloc_scratch(c, &scratch);
+    if (s != GI_OK) return s;
+    unsigned herr = 0;
+    e = run_pairs(J, d_pairs, npairs, precision_mode, d_out, scratch, c->cfg.sms, c->st, &herr);
+    return pairs_status(c, e, herr);
+}

@@ -20,7 +20,7 @@ import ctypes
 import numpy as np
 
 from . import _abi
-from ._abi import GI_PREC_FP32_CASCADE, GI_PREC_FP64
+from ._abi import GI_NOALLOC_MAX_PAIRS, GI_PREC_FP32_CASCADE, GI_PREC_FP64
 
 __all__ = ["GIError", "Context", "Mesh", "Result", "pose_identity", "pose_from_euler_deg", "pose_raw",
            "KernelBVHController", "run_grid_forest_intersection_pipeline", "compute_exact_intersection_curves",
@@ -194,6 +194,17 @@ class Context:
                                          ctypes.c_void_p(d_pairs_ptr), npairs, int(precision),
                                          ctypes.c_void_p(d_out_ptr))
         self.check(rc, "gi_classify_pairs")
+
+    def classify_pairs_noalloc(self, A, B, pose_a, pose_b, d_pairs_ptr, npairs, d_out_ptr,
+                               precision=GI_PREC_FP32_CASCADE):
+        """classify_pairs with the library's fixed per-device scratch (no allocation, at most
+        GI_NOALLOC_MAX_PAIRS pairs; concurrent calls on one device race)."""
+        rc = self._lib.gi_classify_pairs_noalloc(self.handle, A.handle,
+                                                 ctypes.byref(pose_a) if pose_a is not None else None,
+                                                 B.handle, ctypes.byref(pose_b) if pose_b is not None else None,
+                                                 ctypes.c_void_p(d_pairs_ptr), npairs, int(precision),
+                                                 ctypes.c_void_p(d_out_ptr))
+        self.check(rc, "gi_classify_pairs_noalloc")
 
     def server(self, max_inflight=256, want_segments=True, precision=GI_PREC_FP32_CASCADE):
         return Server(self, max_inflight, want_segments, precision)

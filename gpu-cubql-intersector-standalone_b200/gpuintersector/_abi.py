@@ -19,6 +19,7 @@ GI_FLAG_TINY_BUFFERS = 1
 
 GI_PREC_FP32_CASCADE = 0
 GI_PREC_FP64 = 1
+GI_NOALLOC_MAX_PAIRS = 1 << 20
 
 # every symbol include/gi/gi.h declares (checked by the CPU tests)
 EXPORTED = [
@@ -26,7 +27,7 @@ EXPORTED = [
     "gi_mesh_upload", "gi_mesh_upload_device", "gi_mesh_release", "gi_mesh_info",
     "gi_pose_identity", "gi_pose_from_euler_deg", "gi_pose_apply",
     "gi_intersect_opts_default", "gi_intersect", "gi_intersect_oneshot", "gi_intersect_batch",
-    "gi_classify_pairs",
+    "gi_classify_pairs", "gi_classify_pairs_noalloc",
     "gi_result_pairs", "gi_result_segments", "gi_result_stats", "gi_result_free",
     "gi_server_start", "gi_server_submit", "gi_server_poll", "gi_server_wait", "gi_server_stop",
 ]
@@ -107,6 +108,8 @@ def load(path=None):
                                 ctypes.POINTER(vp)], st),
         "gi_classify_pairs": ([vp, vp, ctypes.POINTER(Pose), vp, ctypes.POINTER(Pose), vp, ctypes.c_uint32,
                                ctypes.c_int32, vp], st),
+        "gi_classify_pairs_noalloc": ([vp, vp, ctypes.POINTER(Pose), vp, ctypes.POINTER(Pose), vp, ctypes.c_uint32,
+                                       ctypes.c_int32, vp], st),
         "gi_result_pairs": ([vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)), ctypes.POINTER(ctypes.c_uint64)], st),
         "gi_result_segments": ([vp, ctypes.POINTER(dp), ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)),
                                 ctypes.POINTER(ctypes.c_uint64)], st),

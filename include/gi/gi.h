@@ -192,6 +192,23 @@ gi_status gi_classify_pairs(gi_ctx* ctx, const gi_mesh* A, const gi_pose* pose_a
                             const gi_pose* pose_b, const int32_t* d_pairs, uint32_t npairs, int32_t precision_mode,
                             uint8_t* d_out);
 
+/* gi_classify_pairs without any allocation at call time.  No counterpart in
+ * the reference: it is an addition for callers that may not allocate device
+ * memory while they run (a control loop whose memory budget is fixed at
+ * start-up, or a host framework whose caching allocator owns the free HBM).
+ * Same arguments, semantics and results as gi_classify_pairs; the escalation
+ * scratch is one fixed 4 MiB array in the library's device memory per device.
+ *  - npairs above GI_NOALLOC_MAX_PAIRS -> GI_ERR_CAPACITY, nothing queued;
+ *  - the first call on a device does a one-time set-up (looks up the array's
+ *    device address); make it before any stream capture begins;
+ *  - the array is shared by all contexts on a device: calls whose device work
+ *    overlaps in time race on it.  Calls are blocking, so calls issued one
+ *    after another are safe. */
+#define GI_NOALLOC_MAX_PAIRS 1048576u
+gi_status gi_classify_pairs_noalloc(gi_ctx* ctx, const gi_mesh* A, const gi_pose* pose_a, const gi_mesh* B,
+                                    const gi_pose* pose_b, const int32_t* d_pairs, uint32_t npairs,
+                                    int32_t precision_mode, uint8_t* d_out);
+
 /* ---- results -------------------------------------------------------------- */
 /* pairs_ab: 2 int32 per pair (faceA, faceB); pointer valid until gi_result_free. */
 gi_status gi_result_pairs(const gi_result* r, const int32_t** pairs_ab, uint64_t* n);
