@@ -30,6 +30,15 @@
  * Predicates" (1997).  Signs are exact and constructed points are correctly
  * rounded (round to nearest, ties to even) for inputs inside the supported
  * domain: finite coordinates with |x| <= 2^200 and x == 0 or |x| >= 2^-200.
+ *
+ * PARITY UNPINNED by reference artefacts: the reference ships no golden
+ * vectors, known-answer tests or stored outputs for this path (its TestSuite
+ * compares against live CGAL), and its path cannot be built here (CGAL, Boost,
+ * TBB and cuBQL are absent), so no reference output pins this restatement.
+ * It is checked instead against an independent exact-rational restatement
+ * (tests/fraction_ref.py, Python fractions: Sutherland-Hodgman clipping and
+ * exact hulls), against hand-derived known answers, and against brute force
+ * over all pairs (tests/golden/, tests/test_oracle.py).
  */
 #ifndef GI_ORACLE_H
 #define GI_ORACLE_H
