@@ -44,8 +44,8 @@ METRIC = "ms/intersect at 2×1.3M tris & tri-pair tests/s; pose-update p50/p99 v
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--level", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -73,52 +73,75 @@ def step_poses(cfg, rng, n):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock, power and clock-event reasons sampled through NVML every 2 ms
+    while the timed region runs (nvidia-smi's fastest period, 200 ms, is longer
+    than a short timed region).  Reading counters only; no setting is changed."""
 
-    def __init__(self, index):
-        self.index = index
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
+
+    def __init__(self, cuda_index):
+        self.index = cuda_index
         self.rows = []
-        self.proc = None
+        self.max_mhz = None
+        self.stop = threading.Event()
+        self.nv = None
+
+    def _handle(self):
+        import pynvml as nv
+        import torch
+
+        nv.nvmlInit()
+        self.nv = nv
+        try:
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.index)
 
     def __enter__(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            self.h = self._handle()
+            self.max_mhz = float(self.nv.nvmlDeviceGetMaxClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+            self.t = threading.Thread(target=self._run, daemon=True)
             self.t.start()
-        except Exception:
-            self.proc = None
+        except Exception as e:  # no NVML: report unsampled
+            self.err = repr(e)
+            self.h = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+    def _run(self):
+        nv = self.nv
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+                self.rows.append((float(sm), int(rs), pw))
+            except Exception:
+                pass
+            self.stop.wait(0.002)
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        self.stop.set()
+        if self.h is not None:
+            self.t.join(timeout=2)
 
     def summary(self):
         if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
         reasons = set()
-        for r in self.rows:
-            for k, n in enumerate(names):
-                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
-                    reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+        for _, rs, _ in self.rows:
+            for name, const in self.REASONS:
+                if rs & getattr(self.nv, const, 0):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median([r[0] for r in self.rows])), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(self.rows), "source": "nvml, 2 ms period",
+                "power_w_max": float(max(r[2] for r in self.rows))}
 
 
 def cpu_oracle_run(cfg, poses, nthreads):
@@ -250,6 +273,21 @@ def main():
         t0 = time.perf_counter()
         last_e2e = ctx.intersect_oneshot(cfg["vA"], cfg["tA"], cfg["vB"], cfg["tB"], None, gi.pose_raw(R, C, T))
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    # where the end-to-end time goes (one extra instrumented call, not in the mean)
+    R, C, T = poses[args.warmup]
+    t0 = time.perf_counter()
+    eA = ctx.upload(cfg["vA"], cfg["tA"])
+    t1 = time.perf_counter()
+    eB = ctx.upload(cfg["vB"], cfg["tB"])
+    t2 = time.perf_counter()
+    er = ctx.intersect(eA, eB, None, gi.pose_raw(R, C, T), want_segments=True)
+    t3 = time.perf_counter()
+    eA.release()
+    eB.release()
+    t4 = time.perf_counter()
+    e2e_split = {"upload_build_a_ms": (t1 - t0) * 1e3, "upload_build_b_ms": (t2 - t1) * 1e3,
+                 "intersect_ms": (t3 - t2) * 1e3, "release_ms": (t4 - t3) * 1e3,
+                 "intersect_device_ms": er.stats["ms_total"]}
     h2d = int(cfg["vA"].nbytes + cfg["tA"].astype(np.uint32).nbytes + cfg["vB"].nbytes +
               cfg["tB"].astype(np.uint32).nbytes)
     d2h = int(last_e2e.pairs.nbytes + last_e2e.segments.nbytes + last_e2e.seg_pair.nbytes)
@@ -292,7 +330,8 @@ def main():
         "fp64_form": {"value": float(np.mean(fp64_ms)), "unit": "ms",
                       "speedup_fp32_cascade": float(np.mean(fp64_ms) / max(1e-9, np.mean(dev_ms)))},
         "e2e": {"value": float(np.mean(e2e_ms)), "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "what": "gi_intersect_oneshot from host arrays (upload + BVH build + intersect + results)"},
+                "what": "gi_intersect_oneshot from host arrays (upload + BVH build + intersect + results)",
+                "samples_ms": [round(x, 3) for x in e2e_ms], "split": e2e_split},
         "gpu_launches": int(np.sum([s["launches"] for s in stats])),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "kernel": "k_traverse", "peak_source": peak_src,

@@ -62,12 +62,12 @@ extern "C" gi_status gi_device_count(int32_t* n)
 }
 
 template <class T>
-static cudaError_t grow(T*& p, uint32_t& cap, uint32_t need, cudaStream_t st)
+static cudaError_t grow(T*& p, uint32_t& cap, uint32_t need, cudaMemPool_t pool, cudaStream_t st)
 {
     if (need <= cap && p) return cudaSuccess;
     if (p) cudaFreeAsync(p, st);
     p = nullptr;
-    cudaError_t e = cudaMallocAsync((void**)&p, sizeof(T) * (size_t)need, st);
+    cudaError_t e = pool_alloc(&p, sizeof(T) * (size_t)need, pool, st);
     if (e == cudaSuccess) cap = need;
     else cap = 0;
     return e;
@@ -90,6 +90,20 @@ extern "C" gi_status gi_create(const gi_options* opts, gi_ctx** out)
     }
     cudaSetDevice(c->device);
     cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+        // the context's own stream-ordered pool: memory freed by one call (a
+        // released mesh, a grown buffer) is reused by the next without being
+        // unmapped and mapped again, up to the release threshold
+        cudaMemPoolProps pp = {};
+        pp.allocType = cudaMemAllocationTypePinned;
+        pp.location.type = cudaMemLocationTypeDevice;
+        pp.location.id = c->device;
+        e = cudaMemPoolCreate(&c->pool, &pp);
+        if (e == cudaSuccess) {
+            uint64_t keep = c->budget ? c->budget : (16ull << 30);
+            e = cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     if (e == cudaSuccess) e = query_launch(c->device, &c->cfg);
     if (e == cudaSuccess) e = cudaMalloc(&c->d_cnt, sizeof(Counters));
     if (e == cudaSuccess) e = cudaMallocHost(&c->h_cnt, sizeof(Counters));
@@ -107,11 +121,15 @@ extern "C" gi_status gi_destroy(gi_ctx* c)
     if (!c) return GI_ERR_INVALID_ARG;
     cudaSetDevice(c->device);
     if (c->st) cudaStreamSynchronize(c->st);
-    void* dev[] = {c->d_cnt,   c->d_jobs,   c->queue,  c->qflag,    c->cand,        c->cflag,
-                   c->res,     c->esc,      c->segs,   c->nseg,     c->pairs_out,   c->job_out,
-                   c->segs_out, c->segpair_out, c->order_scratch};
-    for (void* p : dev)
-        if (p) cudaFree(p);
+    if (c->d_cnt) cudaFree(c->d_cnt);
+    if (c->d_jobs) cudaFree(c->d_jobs);
+    void* pooled[] = {c->queue, c->qflag,     c->cand,         c->cflag,   c->res,
+                      c->esc,   c->segs,      c->nseg,         c->pairs_out, c->job_out,
+                      c->segs_out, c->segpair_out, c->order_scratch};
+    for (void* p : pooled)
+        if (p) cudaFreeAsync(p, c->st);
+    if (c->st) cudaStreamSynchronize(c->st);
+    if (c->pool) cudaMemPoolDestroy(c->pool);
     if (c->h_cnt) cudaFreeHost(c->h_cnt);
     if (c->h_jobs) cudaFreeHost(c->h_jobs);
     if (c->h_stage) cudaFreeHost(c->h_stage);
@@ -125,10 +143,12 @@ extern "C" gi_status gi_destroy(gi_ctx* c)
 // ---------------------------------------------------------------------------
 // Meshes
 // ---------------------------------------------------------------------------
+static void mesh_free(gi_ctx* c, gi_mesh* m);
+
 static gi_status mesh_finish(gi_ctx* c, gi_mesh* m, gi_mesh** out)
 {
     unsigned* d_err = nullptr;
-    CK(c, cudaMallocAsync(&d_err, sizeof(unsigned), c->st), "alloc");
+    CK(c, pool_alloc(&d_err, sizeof(unsigned), c->pool, c->st), "alloc");
     CK(c, cudaMemsetAsync(d_err, 0, sizeof(unsigned), c->st), "memset");
     CK(c, launch_validate(m->b.verts, m->b.nv, m->b.tris, m->b.nt, d_err, c->st), "validate");
     unsigned herr = 0;
@@ -136,19 +156,19 @@ static gi_status mesh_finish(gi_ctx* c, gi_mesh* m, gi_mesh** out)
     CK(c, cudaStreamSynchronize(c->st), "sync");
     cudaFreeAsync(d_err, c->st);
     if (herr) {
-        gi_mesh_release(c, m);
+        mesh_free(c, m);
         return set_err(c, (herr & 1u) ? GI_ERR_INVALID_ARG : GI_ERR_RANGE,
                        (herr & 1u) ? "triangle index out of range" : "vertex coordinate outside the supported domain");
     }
-    cudaError_t e = build_bvh(m->b, false, c->st);
+    cudaError_t e = build_bvh(m->b, false, c->pool, c->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
     if (e != cudaSuccess) {
-        gi_mesh_release(c, m);
+        mesh_free(c, m);
         return set_err(c, e == cudaErrorMemoryAllocation ? GI_ERR_OOM : GI_ERR_CUDA, "BVH build", e);
     }
     c->mesh_bytes += m->b.bytes;
     if (c->budget && c->mesh_bytes > c->budget) {
-        gi_mesh_release(c, m);
+        mesh_free(c, m);
         return set_err(c, GI_ERR_OOM, "HBM budget exceeded by mesh upload");
     }
     *out = m;
@@ -167,8 +187,8 @@ static gi_status mesh_alloc(gi_ctx* c, uint32_t nv, uint32_t nt, gi_mesh** pm)
         delete m;
         return set_err(c, GI_ERR_OOM, "HBM budget exceeded by mesh upload");
     }
-    cudaError_t e = cudaMallocAsync(&m->b.verts, vb, c->st);
-    if (e == cudaSuccess) e = cudaMallocAsync(&m->b.tris, tb, c->st);
+    cudaError_t e = pool_alloc(&m->b.verts, vb, c->pool, c->st);
+    if (e == cudaSuccess) e = pool_alloc(&m->b.tris, tb, c->pool, c->st);
     if (e != cudaSuccess) {
         if (m->b.verts) cudaFreeAsync(m->b.verts, c->st);
         delete m;
@@ -211,17 +231,24 @@ extern "C" gi_status gi_mesh_upload_device(gi_ctx* c, const double* d_verts, uin
     return mesh_finish(c, m, out);
 }
 
-extern "C" gi_status gi_mesh_release(gi_ctx* c, gi_mesh* m)
+// Frees a mesh's buffers in stream order (the caller holds c->mu).
+static void mesh_free(gi_ctx* c, gi_mesh* m)
 {
-    if (!c || !m || m->ctx != c) return GI_ERR_INVALID_ARG;
     cudaSetDevice(c->device);
-    cudaStreamSynchronize(c->st);
+    // stream-ordered: work already queued on the context's stream still sees the mesh
     void* p[] = {m->b.verts,     m->b.tris,    m->b.leafTri, m->b.leafBox, m->b.nodes,
                  m->b.leafBox64, m->b.nodes64, m->b.cutRef,  m->b.cutBox,  m->b.cutBox64};
     for (void* q : p)
-        if (q) cudaFree(q);
+        if (q) cudaFreeAsync(q, c->st);
     if (m->b.bytes <= c->mesh_bytes) c->mesh_bytes -= m->b.bytes;
     delete m;
+}
+
+extern "C" gi_status gi_mesh_release(gi_ctx* c, gi_mesh* m)
+{
+    if (!c || !m || m->ctx != c) return GI_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    mesh_free(c, m);
     return GI_OK;
 }
 
@@ -379,7 +406,7 @@ static gi_status ensure_fp64(gi_ctx* c, gi_mesh* m)
         m->has64 = true;
         return GI_OK;
     }
-    cudaError_t e = build_bvh(m->b, true, c->st);
+    cudaError_t e = build_bvh(m->b, true, c->pool, c->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
     if (e != cudaSuccess) return set_err(c, GI_ERR_CUDA, "FP64 BVH build", e);
     m->has64 = true;
@@ -444,32 +471,36 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
     uint32_t nres = 0, nsegs = 0;
     char* hp = nullptr;
     size_t off_jobs = 0, off_segs = 0, off_segpair = 0;
-    for (;; retries++) {
-        CK(c, grow(c->queue, c->cap_front, need_front, c->st), "node queue");
+    // ordering path: one cooperative launch when the previous call's count says
+    // the result will be small (the kernel refuses, and this loop reruns on the
+    // radix path, if it is not)
+    bool small_order = ba + bb + bj <= 63 && c->pred_pairs <= kOrderSmallMax - kOrderSmallMax / 4;
+    for (;;) {
+        CK(c, grow(c->queue, c->cap_front, need_front, c->pool, c->st), "node queue");
         if (c->cap_qflag < c->cap_front) {
             // fresh tag words must not match any call's tag: zero them
-            CK(c, grow(c->qflag, c->cap_qflag, c->cap_front, c->st), "node queue");
+            CK(c, grow(c->qflag, c->cap_qflag, c->cap_front, c->pool, c->st), "node queue");
             CK(c, cudaMemsetAsync(c->qflag, 0, sizeof(unsigned) * c->cap_qflag, c->st), "node queue");
         }
-        CK(c, grow(c->cand, c->cap_cand, need_cand, c->st), "candidates");
+        CK(c, grow(c->cand, c->cap_cand, need_cand, c->pool, c->st), "candidates");
         if (c->cap_cflag < c->cap_cand) {
-            CK(c, grow(c->cflag, c->cap_cflag, c->cap_cand, c->st), "candidates");
+            CK(c, grow(c->cflag, c->cap_cflag, c->cap_cand, c->pool, c->st), "candidates");
             CK(c, cudaMemsetAsync(c->cflag, 0, sizeof(unsigned) * c->cap_cflag, c->st), "candidates");
         }
-        CK(c, grow(c->res, c->cap_res, need_res, c->st), "results");
-        CK(c, grow(c->esc, c->cap_esc, need_esc, c->st), "escalations");
+        CK(c, grow(c->res, c->cap_res, need_res, c->pool, c->st), "results");
+        CK(c, grow(c->esc, c->cap_esc, need_esc, c->pool, c->st), "escalations");
         const uint32_t cap = c->cap_res;
         if (cap > c->cap_out) {
             void* old[] = {c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out, c->segpair_out};
             for (void* p : old)
                 if (p) cudaFreeAsync(p, c->st);
             c->cap_out = 0;
-            CK(c, cudaMallocAsync(&c->segs, sizeof(double) * 18 * (size_t)cap, c->st), "segments");
-            CK(c, cudaMallocAsync(&c->nseg, sizeof(uint32_t) * cap, c->st), "segments");
-            CK(c, cudaMallocAsync(&c->pairs_out, sizeof(int32_t) * 2 * (size_t)cap, c->st), "pairs");
-            CK(c, cudaMallocAsync(&c->job_out, sizeof(uint32_t) * cap, c->st), "pairs");
-            CK(c, cudaMallocAsync(&c->segs_out, sizeof(double) * 18 * (size_t)cap, c->st), "segments");
-            CK(c, cudaMallocAsync(&c->segpair_out, sizeof(int32_t) * 3 * (size_t)cap, c->st), "segments");
+            CK(c, pool_alloc(&c->segs, sizeof(double) * 18 * (size_t)cap, c->pool, c->st), "segments");
+            CK(c, pool_alloc(&c->nseg, sizeof(uint32_t) * cap, c->pool, c->st), "segments");
+            CK(c, pool_alloc(&c->pairs_out, sizeof(int32_t) * 2 * (size_t)cap, c->pool, c->st), "pairs");
+            CK(c, pool_alloc(&c->job_out, sizeof(uint32_t) * cap, c->pool, c->st), "pairs");
+            CK(c, pool_alloc(&c->segs_out, sizeof(double) * 18 * (size_t)cap, c->pool, c->st), "segments");
+            CK(c, pool_alloc(&c->segpair_out, sizeof(int32_t) * 3 * (size_t)cap, c->pool, c->st), "segments");
             c->cap_out = cap;
         }
         size_t osb = order_scratch_bytes(cap, kOsMaxPasses);
@@ -477,7 +508,7 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
             if (c->order_scratch) cudaFreeAsync(c->order_scratch, c->st);
             c->order_scratch = nullptr;
             c->order_scratch_bytes = 0;
-            CK(c, cudaMallocAsync(&c->order_scratch, osb, c->st), "order scratch");
+            CK(c, pool_alloc(&c->order_scratch, osb, c->pool, c->st), "order scratch");
             CK(c, cudaMemsetAsync(c->order_scratch, 0, osb, c->st), "order scratch");
             c->order_scratch_bytes = osb;
         }
@@ -513,9 +544,14 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         CK(c, cudaEventRecord(c->ev[2], c->st), "event");
         if (want_segs) CK(c, launch_segments(b, c->segs, c->nseg, c->cfg, c->st), "segments");
         CK(c, cudaEventRecord(c->ev[3], c->st), "event");
-        CK(c, launch_order_gather(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
-                                  c->segpair_out, want_segs, c->cfg, c->st),
-           "ordering");
+        if (small_order)
+            CK(c, launch_order_small(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
+                                     c->segpair_out, want_segs, c->st),
+               "ordering");
+        else
+            CK(c, launch_order_gather(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
+                                      c->segpair_out, want_segs, c->cfg, c->st),
+               "ordering");
         CK(c, cudaEventRecord(c->ev[4], c->st), "event");
         // speculative copy at the previous call's size
         uint32_t pp = std::min<uint32_t>(cap, (uint32_t)std::min<uint64_t>(c->pred_pairs + c->pred_pairs / 4 + 1024,
@@ -545,6 +581,7 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         if (H.err & kErrExactCapacity) return set_err(c, GI_ERR_RANGE, "exact arithmetic capacity exceeded");
         if (H.overflow) {
             if (retries >= 12) return set_err(c, GI_ERR_CAPACITY, "intersection buffers stayed too small");
+            retries++;
             auto g4 = [](uint32_t cur, uint32_t seen) {
                 uint64_t v = std::max<uint64_t>((uint64_t)cur * 4, (uint64_t)seen + seen / 2 + 1024);
                 return (uint32_t)std::min<uint64_t>(v, 0x7fffffffu);
@@ -553,6 +590,11 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
             if (H.overflow & kOvfCand) need_cand = g4(c->cap_cand, H.cand);
             if (H.overflow & (kOvfRes | kOvfCand)) need_res = g4(c->cap_res, H.res);
             if (H.overflow & (kOvfEsc | kOvfCand)) need_esc = g4(c->cap_esc, H.esc);
+            continue;
+        }
+        if (H.order_redo) {
+            if (!small_order) return set_err(c, GI_ERR_CAPACITY, "ordering path refused twice");
+            small_order = false;
             continue;
         }
         nres = H.res;

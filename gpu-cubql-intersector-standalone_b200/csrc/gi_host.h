@@ -30,6 +30,7 @@ struct gi_result {
 struct gi_ctx {
     int device = 0;
     cudaStream_t st = nullptr;
+    cudaMemPool_t pool = nullptr;  // stream-ordered allocations of this context
     gi::LaunchCfg cfg;
     uint64_t budget = 0;
     uint32_t flags = 0;

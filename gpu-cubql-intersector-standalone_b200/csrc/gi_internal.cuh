@@ -89,7 +89,9 @@ struct Counters {
     unsigned int abort_;    // set on overflow or a spent wait: every waiting warp stops
     unsigned int levels;    // deepest node-pair level + 1
     unsigned int nseg;      // total segments after ordering
-    unsigned int pad5;
+    unsigned int obar;      // grid barrier of the small-count ordering kernel
+    unsigned int order_redo;  // small-count ordering refused (too many results): rerun on the radix path
+    unsigned int pad5[3];
     unsigned long long node_pairs;
     unsigned long long filter_decided;
     unsigned long long exact_signs;

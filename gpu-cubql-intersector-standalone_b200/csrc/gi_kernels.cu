@@ -339,7 +339,7 @@ cudaError_t launch_validate(const double* verts, uint32_t nv, const uint32_t* tr
         if (e_ != cudaSuccess) return e_;        \
     } while (0)
 
-cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaStream_t st)
+cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaMemPool_t pool, cudaStream_t st)
 {
     const uint32_t n = m.nt;
     if (n == 0) {
@@ -359,15 +359,15 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaStream_t st)
     void* nodeBox = nullptr;
     size_t cw = radix_counts_words(n);
     size_t sw = scan_temp_words(cw > n ? cw : n);
-    GI_TRY(cudaMallocAsync(&box, sizeof(float) * 6 * n, st));
-    if (fp64) GI_TRY(cudaMallocAsync(&box64, sizeof(double) * 6 * n, st));
-    GI_TRY(cudaMallocAsync(&cb, sizeof(unsigned) * 8, st));
-    GI_TRY(cudaMallocAsync(&k0, sizeof(uint32_t) * n, st));
-    GI_TRY(cudaMallocAsync(&v0, sizeof(uint32_t) * n, st));
-    GI_TRY(cudaMallocAsync(&k1, sizeof(uint32_t) * n, st));
-    GI_TRY(cudaMallocAsync(&v1, sizeof(uint32_t) * n, st));
-    GI_TRY(cudaMallocAsync(&counts, sizeof(uint32_t) * cw, st));
-    GI_TRY(cudaMallocAsync(&stemp, sizeof(uint32_t) * sw, st));
+    GI_TRY(pool_alloc(&box, sizeof(float) * 6 * n, pool, st));
+    if (fp64) GI_TRY(pool_alloc(&box64, sizeof(double) * 6 * n, pool, st));
+    GI_TRY(pool_alloc(&cb, sizeof(unsigned) * 8, pool, st));
+    GI_TRY(pool_alloc(&k0, sizeof(uint32_t) * n, pool, st));
+    GI_TRY(pool_alloc(&v0, sizeof(uint32_t) * n, pool, st));
+    GI_TRY(pool_alloc(&k1, sizeof(uint32_t) * n, pool, st));
+    GI_TRY(pool_alloc(&v1, sizeof(uint32_t) * n, pool, st));
+    GI_TRY(pool_alloc(&counts, sizeof(uint32_t) * cw, pool, st));
+    GI_TRY(pool_alloc(&stemp, sizeof(uint32_t) * sw, pool, st));
     unsigned cbinit[8] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u, 0u, 0u};
     GI_TRY(cudaMemcpyAsync(cb, cbinit, sizeof(cbinit), cudaMemcpyHostToDevice, st));
     int tb = 256;
@@ -377,23 +377,23 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaStream_t st)
     radix_sort<uint32_t>(k0, v0, k1, v1, n, 30, counts, stemp, st);
     // leaves in sorted order
     if (!fp64) {
-        GI_TRY(cudaMallocAsync(&m.leafBox, sizeof(float) * 6 * n, st));
-        GI_TRY(cudaMallocAsync(&m.leafTri, sizeof(uint4) * n, st));
+        GI_TRY(pool_alloc(&m.leafBox, sizeof(float) * 6 * n, pool, st));
+        GI_TRY(pool_alloc(&m.leafTri, sizeof(uint4) * n, pool, st));
         k_leaves<float><<<gb, tb, 0, st>>>(v0, n, m.tris, box, m.leafBox, m.leafTri);
     } else {
-        GI_TRY(cudaMallocAsync(&m.leafBox64, sizeof(double) * 6 * n, st));
+        GI_TRY(pool_alloc(&m.leafBox64, sizeof(double) * 6 * n, pool, st));
         k_leaves<double><<<gb, tb, 0, st>>>(v0, n, m.tris, box64, m.leafBox64, nullptr);
     }
     if (n == 1) {
         m.root = kLeaf | 0u;
         m.nnodes = 0;
     } else {
-        GI_TRY(cudaMallocAsync(&child, sizeof(uint2) * (n - 1), st));
-        GI_TRY(cudaMallocAsync(&parent, sizeof(int) * (2 * (size_t)n - 1), st));
-        GI_TRY(cudaMallocAsync(&flags, sizeof(unsigned) * (n - 1), st));
-        GI_TRY(cudaMallocAsync(&even, sizeof(uint32_t) * (n - 1), st));
-        GI_TRY(cudaMallocAsync(&widx, sizeof(uint32_t) * (n - 1), st));
-        GI_TRY(cudaMallocAsync(&nodeBox, (fp64 ? sizeof(double) : sizeof(float)) * 6 * (n - 1), st));
+        GI_TRY(pool_alloc(&child, sizeof(uint2) * (n - 1), pool, st));
+        GI_TRY(pool_alloc(&parent, sizeof(int) * (2 * (size_t)n - 1), pool, st));
+        GI_TRY(pool_alloc(&flags, sizeof(unsigned) * (n - 1), pool, st));
+        GI_TRY(pool_alloc(&even, sizeof(uint32_t) * (n - 1), pool, st));
+        GI_TRY(pool_alloc(&widx, sizeof(uint32_t) * (n - 1), pool, st));
+        GI_TRY(pool_alloc(&nodeBox, (fp64 ? sizeof(double) : sizeof(float)) * 6 * (n - 1), pool, st));
         GI_TRY(cudaMemsetAsync(flags, 0, sizeof(unsigned) * (n - 1), st));
         int gi_ = (int)((n - 1 + tb - 1) / tb);
         k_karras<<<gi_, tb, 0, st>>>(k0, (int)n, child, parent);
@@ -410,11 +410,11 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaStream_t st)
         GI_TRY(cudaStreamSynchronize(st));
         uint32_t nw = last[0] + last[1];
         if (!fp64) {
-            GI_TRY(cudaMallocAsync(&m.nodes, sizeof(WNode) * (size_t)nw, st));
+            GI_TRY(pool_alloc(&m.nodes, sizeof(WNode) * (size_t)nw, pool, st));
             k_collapse<float, WNode><<<gi_, tb, 0, st>>>((int)n, child, even, widx, m.leafBox, (float*)nodeBox,
                                                          m.nodes);
         } else {
-            GI_TRY(cudaMallocAsync(&m.nodes64, sizeof(WNode64) * (size_t)nw, st));
+            GI_TRY(pool_alloc(&m.nodes64, sizeof(WNode64) * (size_t)nw, pool, st));
             k_collapse<double, WNode64><<<gi_, tb, 0, st>>>((int)n, child, even, widx, m.leafBox64,
                                                             (double*)nodeBox, m.nodes64);
         }
@@ -424,13 +424,13 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaStream_t st)
     // depth-3 cut (refs shared by both precisions; boxes per precision)
     {
         uint32_t* d_n = nullptr;
-        GI_TRY(cudaMallocAsync(&d_n, sizeof(uint32_t), st));
-        if (!m.cutRef) GI_TRY(cudaMallocAsync(&m.cutRef, sizeof(uint32_t) * kCutMax, st));
+        GI_TRY(pool_alloc(&d_n, sizeof(uint32_t), pool, st));
+        if (!m.cutRef) GI_TRY(pool_alloc(&m.cutRef, sizeof(uint32_t) * kCutMax, pool, st));
         if (!fp64) {
-            GI_TRY(cudaMallocAsync(&m.cutBox, sizeof(float) * 6 * kCutMax, st));
+            GI_TRY(pool_alloc(&m.cutBox, sizeof(float) * 6 * kCutMax, pool, st));
             k_cut<float, WNode><<<1, 32, 0, st>>>(m.nodes, m.leafBox, m.root, m.cutRef, m.cutBox, d_n);
         } else {
-            GI_TRY(cudaMallocAsync(&m.cutBox64, sizeof(double) * 6 * kCutMax, st));
+            GI_TRY(pool_alloc(&m.cutBox64, sizeof(double) * 6 * kCutMax, pool, st));
             k_cut<double, WNode64><<<1, 32, 0, st>>>(m.nodes64, m.leafBox64, m.root, m.cutRef, m.cutBox64, d_n);
         }
         uint32_t hn = 0;
@@ -1230,7 +1230,7 @@ size_t order_scratch_bytes(uint32_t cap, int passes)
     size_t ntiles = (cap + kOsTile - 1) / kOsTile;
     return 2 * sizeof(unsigned long long) * (size_t)cap + 2 * sizeof(uint32_t) * (size_t)cap +
            sizeof(uint32_t) * ((size_t)(passes + 1) * ntiles * 256 + 2 * kOsMaxPasses * 256 + kOsMaxPasses + 2 +
-                               (size_t)cap / kOsGatherTile + 1) +
+                               (size_t)cap / kOsGatherTile + 1 + kOrderSmallBlocks) +
            8192;
 }
 
@@ -1258,6 +1258,7 @@ OrderBufs make_order_bufs(void* scratch, uint32_t cap, int bits_a, int bits_b, i
     O.hist = (uint32_t*)take(sizeof(uint32_t) * kOsMaxPasses * 256);
     O.base = (uint32_t*)take(sizeof(uint32_t) * kOsMaxPasses * 256);
     O.tile_ctr = (uint32_t*)take(sizeof(uint32_t) * (kOsMaxPasses + 2));
+    O.tile_tot = (uint32_t*)take(sizeof(uint32_t) * kOrderSmallBlocks);
     return O;
 }
 
@@ -1281,6 +1282,189 @@ cudaError_t launch_order_gather(const Bufs& b, const OrderBufs& O, bool sort, co
                                                   want_segments ? 1 : 0, sort ? 1 : 0);
     note_launches(1);
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Small-count ordering (up to kOrderSmallMax results) in one cooperative launch.
+//
+// At a few thousand to a few tens of thousands of results the radix passes
+// above are bound by launch and look-back latency, not by bytes.  Here each of
+// kOrderSmallBlocks blocks sorts one run of kOrderSmallRun keys in shared
+// memory (bitonic network), and since the (job, a, b) keys are unique, the
+// final position of a key is its index in its own run plus its lower bound in
+// every other run (binary searches in L2).  A third phase gathers the pairs
+// and places the segments (block scan + the preceding runs' totals).  The
+// phases are separated by grid barriers; the launch is cooperative, so all
+// blocks are co-resident, and every barrier wait is bounded all the same.
+// ---------------------------------------------------------------------------
+constexpr int kOrderSmallThreads = 1024;
+static_assert(kOrderSmallRun == 2 * kOrderSmallThreads, "two keys per thread");
+
+// Arrive at grid barrier `k` (1-based) of the launch; waits bounded.  On a spent
+// wait the error bit is set and later barriers of the block no longer wait.
+__device__ __forceinline__ void grid_barrier(unsigned* ctr, unsigned k, unsigned* err, unsigned* s_ok)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(ctr, 1u);
+        const unsigned target = k * gridDim.x;
+        unsigned long long spins = 0;
+        while (*s_ok && ld_vol(ctr) < target) {
+            if (++spins > kLookbackSpins) {
+                atomicOr(err, kErrTimeout);
+                *s_ok = 0u;
+                break;
+            }
+            __nanosleep(64);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kOrderSmallThreads, 1)
+    k_order_small(Bufs B, OrderBufs O, const double* __restrict__ segs, const uint32_t* __restrict__ nseg,
+                  int32_t* pairs_out, uint32_t* job_out, double* segs_out, int32_t* segpair_out, int want_segments,
+                  int sorted)
+{
+    __shared__ unsigned long long sk[kOrderSmallRun];
+    __shared__ uint32_t sv[kOrderSmallRun];
+    __shared__ uint32_t sw[33];
+    __shared__ unsigned s_ok, s_base;
+    Counters* C = B.cnt;
+    const unsigned n = res_count(B);
+    if (n > kOrderSmallMax) {  // same decision in every block: no barrier is reached
+        if (blockIdx.x == 0 && threadIdx.x == 0) C->order_redo = 1u;
+        return;
+    }
+    if (threadIdx.x == 0) s_ok = 1u;
+    const unsigned nruns = (n + kOrderSmallRun - 1) / kOrderSmallRun;
+    const unsigned t = blockIdx.x;
+    const unsigned base = t * kOrderSmallRun;
+    const unsigned len = t < nruns ? min((unsigned)kOrderSmallRun, n - base) : 0u;
+    uint32_t* perm = O.vals[1];
+    unsigned bar = 0;
+    if (sorted) {
+        // ---- phase 1: sort this block's run (padding keys sort last) ----
+        for (unsigned i = threadIdx.x; i < kOrderSmallRun; i += kOrderSmallThreads) {
+            if (i < len) {
+                sk[i] = order_key(__ldcg(B.res + base + i), O);
+                sv[i] = base + i;
+            } else {
+                sk[i] = ~0ull;
+                sv[i] = 0xffffffffu;
+            }
+        }
+        __syncthreads();
+        if (len > 1) {  // uniform in the block
+            for (unsigned k = 2; k <= (unsigned)kOrderSmallRun; k <<= 1)
+                for (unsigned j = k >> 1; j > 0; j >>= 1) {
+                    const unsigned i = threadIdx.x;
+                    const unsigned lo = 2 * i - (i & (j - 1));
+                    const unsigned hi = lo + j;
+                    const bool up = (lo & k) == 0;
+                    const unsigned long long a = sk[lo], b = sk[hi];
+                    if ((a > b) == up) {
+                        sk[lo] = b;
+                        sk[hi] = a;
+                        const uint32_t va = sv[lo];
+                        sv[lo] = sv[hi];
+                        sv[hi] = va;
+                    }
+                    __syncthreads();
+                }
+        }
+        for (unsigned i = threadIdx.x; i < len; i += kOrderSmallThreads) O.keys[0][base + i] = sk[i];
+        grid_barrier(&C->obar, ++bar, &C->err, &s_ok);
+        // ---- phase 2: final position = own index + lower bounds in the other runs ----
+        for (unsigned i = threadIdx.x; i < len; i += kOrderSmallThreads) {
+            const unsigned long long x = sk[i];
+            unsigned pos = i;
+            for (unsigned s0 = 0; s0 < nruns; s0 += 8) {
+                unsigned lo[8], hi[8];
+#pragma unroll
+                for (int r = 0; r < 8; r++) {
+                    const unsigned s = s0 + r;
+                    lo[r] = 0u;
+                    hi[r] = (s < nruns && s != t) ? min((unsigned)kOrderSmallRun, n - s * kOrderSmallRun) : 0u;
+                }
+                for (int step = 0; step < 12; step++) {  // 2^11 < kOrderSmallRun + 1 <= 2^12
+#pragma unroll
+                    for (int r = 0; r < 8; r++) {
+                        if (lo[r] < hi[r]) {
+                            const unsigned mid = (lo[r] + hi[r]) >> 1;
+                            const unsigned long long v = __ldcg(O.keys[0] + (size_t)(s0 + r) * kOrderSmallRun + mid);
+                            if (v < x) lo[r] = mid + 1u;
+                            else hi[r] = mid;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < 8; r++) pos += lo[r];
+            }
+            if (pos < n) perm[pos] = sv[i];
+        }
+        grid_barrier(&C->obar, ++bar, &C->err, &s_ok);
+    }
+    // ---- phase 3: gather pairs, place segments (two sorted positions per thread) ----
+    unsigned src[2], cnt[2];
+    uint4 rr[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const unsigned local = 2 * threadIdx.x + q;
+        const bool ok = local < len;
+        src[q] = ok ? (sorted ? __ldcg(perm + base + local) : base + local) : 0u;
+        if (src[q] >= n) src[q] = 0u;
+        cnt[q] = (ok && want_segments) ? __ldcg(nseg + src[q]) : 0u;
+        rr[q] = ok ? __ldcg(B.res + src[q]) : make_uint4(0u, 0u, 0u, 0u);
+    }
+    unsigned tot;
+    const unsigned ex = block_exclusive_scan(cnt[0] + cnt[1], sw, &tot);
+    if (threadIdx.x == 0) O.tile_tot[t] = tot;
+    grid_barrier(&C->obar, ++bar, &C->err, &s_ok);
+    if (threadIdx.x == 0) {
+        unsigned b0 = 0;
+        for (unsigned s = 0; s < t; s++) b0 += __ldcg(O.tile_tot + s);
+        s_base = b0;
+        if (nruns && t == nruns - 1) C->nseg = b0 + tot;
+    }
+    __syncthreads();
+    unsigned off = s_base + ex;
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const unsigned local = 2 * threadIdx.x + q;
+        if (local >= len) continue;
+        const unsigned k = base + local;
+        pairs_out[2 * (size_t)k] = (int32_t)rr[q].y;
+        pairs_out[2 * (size_t)k + 1] = (int32_t)rr[q].z;
+        job_out[k] = rr[q].x;
+        for (unsigned e = 0; e < cnt[q]; e++) {
+            const double2* sp = reinterpret_cast<const double2*>(segs + 18 * (size_t)src[q] + 6 * e);
+            double2* dp = reinterpret_cast<double2*>(segs_out + 6 * (size_t)(off + e));
+            dp[0] = __ldcg(sp);
+            dp[1] = __ldcg(sp + 1);
+            dp[2] = __ldcg(sp + 2);
+            segpair_out[off + e] = (int32_t)k;
+        }
+        off += cnt[q];
+    }
+}
+
+cudaError_t launch_order_small(const Bufs& b, const OrderBufs& O, bool sort, const double* segs,
+                               const uint32_t* nseg, int32_t* pairs_out, uint32_t* job_out, double* segs_out,
+                               int32_t* segpair_out, bool want_segments, cudaStream_t st)
+{
+    Bufs bb = b;
+    OrderBufs oo = O;
+    const double* a_segs = segs;
+    const uint32_t* a_nseg = nseg;
+    int ws = want_segments ? 1 : 0, so = sort ? 1 : 0;
+    void* args[] = {&bb, &oo, &a_segs, &a_nseg, &pairs_out, &job_out, &segs_out, &segpair_out, &ws, &so};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_order_small, dim3(kOrderSmallBlocks),
+                                                dim3(kOrderSmallThreads), args, 0, st);
+    note_launches(1);
+    return e;
 }
 
 // ===========================================================================

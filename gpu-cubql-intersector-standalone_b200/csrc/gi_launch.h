@@ -23,12 +23,24 @@ struct MeshBuffers {
     size_t bytes = 0;
 };
 
+// Stream-ordered allocation from the context's own pool (the device's default
+// pool when none is given).
+inline cudaError_t pool_alloc(void** p, size_t bytes, cudaMemPool_t pool, cudaStream_t st)
+{
+    return pool ? cudaMallocFromPoolAsync(p, bytes, pool, st) : cudaMallocAsync(p, bytes, st);
+}
+template <class T>
+inline cudaError_t pool_alloc(T** p, size_t bytes, cudaMemPool_t pool, cudaStream_t st)
+{
+    return pool_alloc(reinterpret_cast<void**>(p), bytes, pool, st);
+}
+
 // Validates indices / coordinate domain (err bit 1: bad index, 2: out of domain).
 cudaError_t launch_validate(const double* verts, uint32_t nv, const uint32_t* tris, uint32_t nt, unsigned* d_err,
                             cudaStream_t st);
 
 // Builds the 4-wide BVH (FP32 boxes) or, with fp64 = true, the FP64 node copy.
-cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaStream_t st);
+cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaMemPool_t pool, cudaStream_t st);
 
 // Intersect launch configuration.
 struct LaunchCfg {
@@ -57,6 +69,7 @@ struct OrderBufs {
     uint32_t* hist;      // kOsMaxPasses x 256 (kept zero between calls)
     uint32_t* base;      // kOsMaxPasses x 256
     uint32_t* tile_ctr;  // kOsMaxPasses + 2 (per pass, the gather, the histogram blocks)
+    uint32_t* tile_tot;  // kOrderSmallBlocks: segment totals per run (small-count path)
     uint32_t ntiles_cap;
     int passes;
     int bits_a, bits_b;
@@ -66,6 +79,16 @@ OrderBufs make_order_bufs(void* scratch, uint32_t cap, int bits_a, int bits_b, i
 cudaError_t launch_order_gather(const Bufs& b, const OrderBufs& O, bool sort, const double* segs,
                                 const uint32_t* nseg, int32_t* pairs_out, uint32_t* job_out, double* segs_out,
                                 int32_t* segpair_out, bool want_segments, const LaunchCfg& cfg, cudaStream_t st);
+// Small-count ordering: one cooperative launch of kOrderSmallBlocks blocks,
+// each sorting a run of kOrderSmallRun keys, for up to kOrderSmallMax results.
+// If the call produced more, the kernel only sets Counters::order_redo and the
+// caller reruns with launch_order_gather.  Keys must fit in 63 bits.
+constexpr int kOrderSmallRun = 2048;
+constexpr int kOrderSmallBlocks = 32;
+constexpr uint32_t kOrderSmallMax = (uint32_t)kOrderSmallRun * kOrderSmallBlocks;
+cudaError_t launch_order_small(const Bufs& b, const OrderBufs& O, bool sort, const double* segs,
+                               const uint32_t* nseg, int32_t* pairs_out, uint32_t* job_out, double* segs_out,
+                               int32_t* segpair_out, bool want_segments, cudaStream_t st);
 // Number of kernels launched by the launchers of this library (monotonic).
 unsigned long long launch_count();
 void note_launches(unsigned n);

@@ -143,7 +143,7 @@ extern "C" gi_status gi_classify_pairs(gi_ctx* c, const gi_mesh* A, const gi_pos
     gi_status s = pairs_job(c, A, pa, B, pb, &J);
     if (s != GI_OK) return s;
     unsigned* scratch = nullptr;
-    cudaError_t e = cudaMallocAsync(&scratch, sizeof(unsigned) * (kPairsScratchHead + (size_t)npairs), c->st);
+    cudaError_t e = pool_alloc(&scratch, sizeof(unsigned) * (kPairsScratchHead + (size_t)npairs), c->pool, c->st);
     if (e != cudaSuccess) return set_err(c, GI_ERR_OOM, "classify pairs scratch", e);
     unsigned herr = 0;
     e = run_pairs(J, d_pairs, npairs, precision_mode, d_out, scratch, c->cfg.sms, c->st, &herr);

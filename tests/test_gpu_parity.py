@@ -132,6 +132,43 @@ def test_config3_full_vs_oracle(ctx, gi, oc):
     assert_same(r, ref)
 
 
+def test_ordering_paths_and_redo(gi, oc):
+    """Both ordering paths on a fresh context.  The path follows the previous
+    call's result count: the first call predicts a small result and takes the
+    one-launch path; a large result then overruns it, the kernel refuses and the
+    call reruns on the radix path; the next (small) call takes the radix path,
+    the one after it the one-launch path again.  All equal the oracle, sorted
+    and unsorted."""
+    from gpuintersector import meshgen as mg
+
+    small = mg.config1(seed=21)
+    large = mg.config3(n=256, seed=5)
+
+    def unsorted_same(c, A, B, ref):
+        ru = c.intersect(A, B, None, gi_pose(gi, small["poseB"]), sort_output=False)
+        assert set(map(tuple, ru.pairs.tolist())) == set(map(tuple, ref["pairs"].tolist()))
+        # segments: renumber the unsorted pair indices to the oracle's order, then compare canonically
+        index = {ab: k for k, ab in enumerate(map(tuple, ref["pairs"].tolist()))}
+        remap = np.array([index[ab] for ab in map(tuple, ru.pairs.tolist())], dtype=np.int64)
+        gp, gs = canonical(ru.segments, remap[np.asarray(ru.seg_pair, dtype=np.int64)])
+        ep, es = canonical(ref["segs"], ref["seg_pair"])
+        assert np.array_equal(gp, ep) and np.array_equal(gs, es)
+
+    with gi.Context(0) as c:
+        r1, ref1 = run_cfg(c, gi, oc, small)          # one-launch path
+        assert_same(r1, ref1)
+        r2, ref2 = run_cfg(c, gi, oc, large)          # one-launch refused -> radix path
+        assert len(ref2["pairs"]) > 65536
+        assert_same(r2, ref2)
+        A, B = c.upload(small["vA"], small["tA"]), c.upload(small["vB"], small["tB"])
+        unsorted_same(c, A, B, ref1)                   # radix path, unsorted
+        unsorted_same(c, A, B, ref1)                   # one-launch path, unsorted
+        r3 = c.intersect(A, B, None, gi_pose(gi, small["poseB"]))
+        assert_same(r3, ref1)
+        A.release()
+        B.release()
+
+
 def test_fp64_form_identical(ctx, gi, oc):
     from gpuintersector import meshgen as mg
 
