@@ -7,7 +7,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/gi/gi.h"
+#include "gi/gi.h"
 #include "gi_launch.h"
 
 using gi::Counters;
