@@ -446,6 +446,7 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
     }
     int ba = bits_for(maxA), bb = bits_for(maxB), bj = nj > 1 ? bits_for(nj) : 0;
     if (ba + bb + bj > 64) return set_err(c, GI_ERR_INVALID_ARG, "batch too large for 64-bit ordering keys");
+    if (nj > (1u << 19)) return set_err(c, GI_ERR_INVALID_ARG, "at most 2^19 jobs per batch");
     if (nj > c->cap_jobs) {
         if (c->d_jobs) cudaFree(c->d_jobs);
         if (c->h_jobs) cudaFreeHost(c->h_jobs);
@@ -536,7 +537,6 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         b.cnt = c->d_cnt;
         b.precision = prec;
         CK(c, cudaMemsetAsync(c->d_cnt, 0, sizeof(Counters), c->st), "counters");
-        CK(c, launch_init_frontier(b, prec, c->st), "init frontier");
         CK(c, cudaEventRecord(c->ev[0], c->st), "event");
         CK(c, launch_traverse(b, c->cfg, prec, c->st), "traverse");
         CK(c, cudaEventRecord(c->ev[1], c->st), "event");
@@ -668,7 +668,7 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         s2.segments = r->seg_pair.size();
         // launch-wide counters (shared by all jobs of a batch)
         s2.node_pairs = H.node_pairs;
-        s2.candidates = H.cand;
+        s2.candidates = H.tested;
         s2.filter_decided = H.filter_decided;
         s2.escalated = H.esc;
         s2.exact_signs = H.exact_signs;

@@ -53,7 +53,7 @@ struct gi_ctx {
     uint32_t cap_cand = 0;
     uint4* res = nullptr;
     uint32_t cap_res = 0;
-    uint32_t* esc = nullptr;
+    uint4* esc = nullptr;
     uint32_t cap_esc = 0;
     // outputs
     double* segs = nullptr;  // 18 per result slot

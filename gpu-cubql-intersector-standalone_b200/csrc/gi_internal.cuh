@@ -74,9 +74,9 @@ struct Counters {
     // hot counters, each on its own 128-byte line (polled and updated by every warp)
     unsigned int q_tail;  // node-pair queue: slots reserved (pushed)
     unsigned int pad0[31];
-    unsigned int q_head;  // slots handed out as tickets
+    unsigned int q_head;  // queue slots handed out as tickets
     unsigned int pad1[31];
-    unsigned int q_done;  // slots processed (children published)
+    unsigned int work;    // node pairs that exist (made, not yet expanded), modulo 2^32
     unsigned int pad2[31];
     unsigned int cand;    // candidate slots reserved
     unsigned int pad3[31];
@@ -91,11 +91,14 @@ struct Counters {
     unsigned int nseg;      // total segments after ordering
     unsigned int obar;      // grid barrier of the small-count ordering kernel
     unsigned int order_redo;  // small-count ordering refused (too many results): rerun on the radix path
-    unsigned int pad5[3];
+    unsigned int seed_head;  // seed tests claimed (chunks of 32)
+    unsigned int seed_done;  // seed tests finished and published
+    unsigned int pad5;
     unsigned long long node_pairs;
     unsigned long long filter_decided;
     unsigned long long exact_signs;
     unsigned long long exact_points;
+    unsigned long long tested;  // candidates run through the first filter stage
 };
 
 constexpr unsigned kOvfFrontier = 1u, kOvfCand = 2u, kOvfRes = 4u, kOvfEsc = 8u;
@@ -113,7 +116,7 @@ struct Bufs {
     uint32_t cap_cand;
     uint4* res;       // job, triA, triB, 0   (original triangle ids)
     uint32_t cap_res;
-    uint32_t* esc;    // candidate index
+    uint4* esc;       // escalated candidates: job, leaf posA, leaf posB, 0
     uint32_t cap_esc;
     Counters* cnt;
     unsigned tag;     // nonzero, different for every call on the context

@@ -532,85 +532,111 @@ struct Prec<true> {
     static __device__ __forceinline__ const S* leafBox(const MeshDev& M) { return M.leafBox64; }
 };
 
-// Children of a node reference in the mesh-local frame: a wide node gives up
-// to four (one 128-byte line, loaded as seven 16-byte vectors); a leaf
-// reference stands for itself.
-__device__ __forceinline__ void load_kids(const MeshDev& M, uint32_t ref, Box<float> b[4], uint32_t c[4])
+// Children of a node reference in the mesh-local frame, structure of arrays
+// (slot i of every array is child i).  A wide node gives up to four (one
+// 128-byte line loaded as seven 16-byte vectors, or two lines for FP64); a
+// leaf reference stands for itself in slot 0.  Every array is indexed by
+// constants only, so the whole set lives in registers.
+template <class S>
+struct Kids {
+    S lx[4], ly[4], lz[4], hx[4], hy[4], hz[4];
+    uint32_t c[4];
+};
+
+__device__ __forceinline__ void put4(float (&d)[4], const float4& v)
+{
+    d[0] = v.x;
+    d[1] = v.y;
+    d[2] = v.z;
+    d[3] = v.w;
+}
+__device__ __forceinline__ void put4(double (&d)[4], const double2& a, const double2& b)
+{
+    d[0] = a.x;
+    d[1] = a.y;
+    d[2] = b.x;
+    d[3] = b.y;
+}
+
+__device__ __forceinline__ void load_kids(const MeshDev& M, uint32_t ref, Kids<float>& k)
 {
     if (ref & kLeaf) {
         const float2* lb = reinterpret_cast<const float2*>(M.leafBox + 6 * (size_t)(ref & ~kLeaf));
-        float2 a = __ldg(lb), bb = __ldg(lb + 1), cc = __ldg(lb + 2);
-        b[0].lo[0] = a.x;
-        b[0].lo[1] = a.y;
-        b[0].lo[2] = bb.x;
-        b[0].hi[0] = bb.y;
-        b[0].hi[1] = cc.x;
-        b[0].hi[2] = cc.y;
-        c[0] = ref;
-        c[1] = c[2] = c[3] = kEmpty;
+        const float2 a = __ldg(lb), b = __ldg(lb + 1), c = __ldg(lb + 2);
+        put4(k.lx, make_float4(a.x, 0.f, 0.f, 0.f));
+        put4(k.ly, make_float4(a.y, 0.f, 0.f, 0.f));
+        put4(k.lz, make_float4(b.x, 0.f, 0.f, 0.f));
+        put4(k.hx, make_float4(b.y, 0.f, 0.f, 0.f));
+        put4(k.hy, make_float4(c.x, 0.f, 0.f, 0.f));
+        put4(k.hz, make_float4(c.y, 0.f, 0.f, 0.f));
+        k.c[0] = ref;
+        k.c[1] = k.c[2] = k.c[3] = kEmpty;
         return;
     }
     const float4* p = reinterpret_cast<const float4*>(M.nodes + ref);
-    float4 lx = __ldg(p), ly = __ldg(p + 1), lz = __ldg(p + 2), hx = __ldg(p + 3), hy = __ldg(p + 4),
-           hz = __ldg(p + 5);
-    uint4 ch = __ldg(reinterpret_cast<const uint4*>(p + 6));
-    const float* LX = &lx.x;
-    const float* LY = &ly.x;
-    const float* LZ = &lz.x;
-    const float* HX = &hx.x;
-    const float* HY = &hy.x;
-    const float* HZ = &hz.x;
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        b[i].lo[0] = LX[i];
-        b[i].lo[1] = LY[i];
-        b[i].lo[2] = LZ[i];
-        b[i].hi[0] = HX[i];
-        b[i].hi[1] = HY[i];
-        b[i].hi[2] = HZ[i];
-    }
-    c[0] = ch.x;
-    c[1] = ch.y;
-    c[2] = ch.z;
-    c[3] = ch.w;
+    put4(k.lx, __ldg(p));
+    put4(k.ly, __ldg(p + 1));
+    put4(k.lz, __ldg(p + 2));
+    put4(k.hx, __ldg(p + 3));
+    put4(k.hy, __ldg(p + 4));
+    put4(k.hz, __ldg(p + 5));
+    const uint4 ch = __ldg(reinterpret_cast<const uint4*>(p + 6));
+    k.c[0] = ch.x;
+    k.c[1] = ch.y;
+    k.c[2] = ch.z;
+    k.c[3] = ch.w;
 }
-__device__ __forceinline__ void load_kids(const MeshDev& M, uint32_t ref, Box<double> b[4], uint32_t c[4])
+__device__ __forceinline__ void load_kids(const MeshDev& M, uint32_t ref, Kids<double>& k)
 {
     if (ref & kLeaf) {
         const double2* lb = reinterpret_cast<const double2*>(M.leafBox64 + 6 * (size_t)(ref & ~kLeaf));
-        double2 a = __ldg(lb), bb = __ldg(lb + 1), cc = __ldg(lb + 2);
-        b[0].lo[0] = a.x;
-        b[0].lo[1] = a.y;
-        b[0].lo[2] = bb.x;
-        b[0].hi[0] = bb.y;
-        b[0].hi[1] = cc.x;
-        b[0].hi[2] = cc.y;
-        c[0] = ref;
-        c[1] = c[2] = c[3] = kEmpty;
+        const double2 a = __ldg(lb), b = __ldg(lb + 1), c = __ldg(lb + 2);
+        const double2 z = make_double2(0.0, 0.0);
+        put4(k.lx, make_double2(a.x, 0.0), z);
+        put4(k.ly, make_double2(a.y, 0.0), z);
+        put4(k.lz, make_double2(b.x, 0.0), z);
+        put4(k.hx, make_double2(b.y, 0.0), z);
+        put4(k.hy, make_double2(c.x, 0.0), z);
+        put4(k.hz, make_double2(c.y, 0.0), z);
+        k.c[0] = ref;
+        k.c[1] = k.c[2] = k.c[3] = kEmpty;
         return;
     }
     const double2* p = reinterpret_cast<const double2*>(M.nodes64 + ref);
-    double v[24];
-#pragma unroll
-    for (int k = 0; k < 12; k++) {
-        double2 q = __ldg(p + k);
-        v[2 * k] = q.x;
-        v[2 * k + 1] = q.y;
-    }
-    uint4 ch = __ldg(reinterpret_cast<const uint4*>(p + 12));
+    put4(k.lx, __ldg(p), __ldg(p + 1));
+    put4(k.ly, __ldg(p + 2), __ldg(p + 3));
+    put4(k.lz, __ldg(p + 4), __ldg(p + 5));
+    put4(k.hx, __ldg(p + 6), __ldg(p + 7));
+    put4(k.hy, __ldg(p + 8), __ldg(p + 9));
+    put4(k.hz, __ldg(p + 10), __ldg(p + 11));
+    const uint4 ch = __ldg(reinterpret_cast<const uint4*>(p + 12));
+    k.c[0] = ch.x;
+    k.c[1] = ch.y;
+    k.c[2] = ch.z;
+    k.c[3] = ch.w;
+}
+
+// Maps the four child boxes to the world frame (same bound as world_box).
+template <class S>
+__device__ __forceinline__ void world_kids(const DevPose& P, Kids<S>& k)
+{
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        b[i].lo[0] = v[i];
-        b[i].lo[1] = v[4 + i];
-        b[i].lo[2] = v[8 + i];
-        b[i].hi[0] = v[12 + i];
-        b[i].hi[1] = v[16 + i];
-        b[i].hi[2] = v[20 + i];
+        Box<S> b;
+        b.lo[0] = k.lx[i];
+        b.lo[1] = k.ly[i];
+        b.lo[2] = k.lz[i];
+        b.hi[0] = k.hx[i];
+        b.hi[1] = k.hy[i];
+        b.hi[2] = k.hz[i];
+        world_box(P, b);
+        k.lx[i] = b.lo[0];
+        k.ly[i] = b.lo[1];
+        k.lz[i] = b.lo[2];
+        k.hx[i] = b.hi[0];
+        k.hy[i] = b.hi[1];
+        k.hz[i] = b.hi[2];
     }
-    c[0] = ch.x;
-    c[1] = ch.y;
-    c[2] = ch.z;
-    c[3] = ch.w;
 }
 
 template <class S>
@@ -632,49 +658,6 @@ __device__ __forceinline__ unsigned warp_append(bool pred, unsigned* counter)
     return base + __popc(m & ((1u << lane) - 1u));
 }
 
-// Reserves `cnt` consecutive slots per lane with one atomic per warp.
-__device__ __forceinline__ unsigned warp_reserve(unsigned cnt, unsigned* counter)
-{
-    const unsigned lane = threadIdx.x & 31;
-    unsigned incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= (unsigned)o) incl += y;
-    }
-    unsigned total = __shfl_sync(0xffffffffu, incl, 31);
-    unsigned base = 0;
-    if (lane == 31 && total) base = atomicAdd(counter, total);
-    base = __shfl_sync(0xffffffffu, base, 31);
-    return base + incl - cnt;
-}
-
-// Two reservations with their atomics issued back to back (one round trip).
-__device__ __forceinline__ void warp_reserve2(unsigned c1, unsigned* ctr1, unsigned c2, unsigned* ctr2,
-                                              unsigned* p1, unsigned* p2)
-{
-    const unsigned lane = threadIdx.x & 31;
-    unsigned i1 = c1, i2 = c2;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        unsigned y1 = __shfl_up_sync(0xffffffffu, i1, o);
-        unsigned y2 = __shfl_up_sync(0xffffffffu, i2, o);
-        if (lane >= (unsigned)o) {
-            i1 += y1;
-            i2 += y2;
-        }
-    }
-    unsigned b1 = 0, b2 = 0;
-    if (lane == 31) {
-        if (i1) b1 = atomicAdd(ctr1, i1);
-        if (i2) b2 = atomicAdd(ctr2, i2);
-    }
-    b1 = __shfl_sync(0xffffffffu, b1, 31);
-    b2 = __shfl_sync(0xffffffffu, b2, 31);
-    *p1 = b1 + i1 - c1;
-    *p2 = b2 + i2 - c2;
-}
-
 __device__ __forceinline__ unsigned ld_cg_u32(const unsigned* p)
 {
     return __ldcg(p);
@@ -691,65 +674,97 @@ __device__ __forceinline__ void load_tri(const MeshDev& M, const DevPose& P, uin
     *tri_id = t.w;
 }
 
-// One node pair per lane: load both nodes (2 x 128 B), map the child boxes to
-// the world frame, test the 4 x 4 child pairs.  fm / cm: bit 4i+j set when
+// Bit i of `x` (i < 4) spread over nibble i: the child pairs (i, *).
+__device__ __forceinline__ unsigned rows4(unsigned x)
+{
+    return ((x & 1u) ? 0x000Fu : 0u) | ((x & 2u) ? 0x00F0u : 0u) | ((x & 4u) ? 0x0F00u : 0u) |
+           ((x & 8u) ? 0xF000u : 0u);
+}
+
+__device__ __forceinline__ uint32_t sel4(const uint32_t (&a)[4], unsigned k)
+{
+    return k == 0u ? a[0] : k == 1u ? a[1] : k == 2u ? a[2] : a[3];
+}
+
+// One node pair: load both nodes, map the child boxes to the world frame and
+// test the 4 x 4 child pairs without branches.  fm / cm: bit 4i+j set when
 // child pair (i, j) overlaps and leads to a node pair / a leaf pair.
 template <bool F64>
 __device__ __forceinline__ void expand_pair(const Bufs& B, const uint4& ent, unsigned& fm, unsigned& cm,
-                                            uint32_t ca[4], uint32_t cb[4])
+                                            uint32_t (&ca)[4], uint32_t (&cb)[4])
 {
     using S = typename Prec<F64>::S;
-    Box<S> ba[4], bb[4];
     const JobDev& J = B.jobs[ent.x];
-    load_kids(J.A, ent.y, ba, ca);
-    load_kids(J.B, ent.z, bb, cb);
-    const bool ia = J.pa.identity, ib = J.pb.identity;
+    Kids<S> a, b;
+    load_kids(J.A, ent.y, a);
+    load_kids(J.B, ent.z, b);
+    if (!J.pa.identity) world_kids(J.pa, a);
+    if (!J.pb.identity) world_kids(J.pb, b);
+    unsigned m = 0, va = 0, vb = 0, la = 0, lb = 0;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        if (!ia && ca[i] != kEmpty) world_box(J.pa, ba[i]);
-        if (!ib && cb[i] != kEmpty) world_box(J.pb, bb[i]);
-    }
-    fm = cm = 0;
-#pragma unroll
-    for (int i = 0; i < 4; i++)
+        ca[i] = a.c[i];
+        cb[i] = b.c[i];
+        va |= (a.c[i] != kEmpty ? 1u : 0u) << i;
+        vb |= (b.c[i] != kEmpty ? 1u : 0u) << i;
+        la |= ((a.c[i] & kLeaf) && a.c[i] != kEmpty ? 1u : 0u) << i;
+        lb |= ((b.c[i] & kLeaf) && b.c[i] != kEmpty ? 1u : 0u) << i;
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            if (ca[i] == kEmpty || cb[j] == kEmpty || !overlap(ba[i], bb[j])) continue;
-            const unsigned bit = 1u << (4 * i + j);
-            if ((ca[i] & kLeaf) && (cb[j] & kLeaf)) cm |= bit;
-            else fm |= bit;
+            const bool ov = (a.lx[i] <= b.hx[j]) & (b.lx[j] <= a.hx[i]) & (a.ly[i] <= b.hy[j]) &
+                            (b.ly[j] <= a.hy[i]) & (a.lz[i] <= b.hz[j]) & (b.lz[j] <= a.hz[i]);
+            m |= (ov ? 1u : 0u) << (4 * i + j);
         }
+    }
+    m &= rows4(va) & (vb * 0x1111u);
+    const unsigned leafpair = rows4(la) & (lb * 0x1111u);
+    cm = m & leafpair;
+    fm = m & ~leafpair;
 }
 
 // ---------------------------------------------------------------------------
-// Persistent BVH4 x BVH4 traversal over a device work queue (no grid barrier).
+// Persistent BVH4 x BVH4 traversal: a small warp stack in front of a device
+// work queue (no grid barrier).
 //
-// Node pairs live in a linear queue.  Producers reserve slots at q_tail with
-// one atomic per warp, write the entries and publish every slot by storing the
-// call's tag in its flag word after a fence.  Consumers work by tickets: a
-// warp takes 32 consecutive slots with one atomicAdd on q_head, polls the 32
-// tag words of its slots (one 128-byte line, so polling has no hot spot) and
-// processes each slot once published, one node pair per lane; it takes a new
-// ticket when all 32 are done.  q_done counts
-// processed slots and advances only after a slot's children are published,
-// so reading q_done and then q_tail and finding them equal proves that the
-// traversal is over: no slot is queued or in flight.
-// Leaf pairs go to the candidate list the same way, and warps whose node slots
-// are not ready run the first filter stage on their candidate ticket, which
-// overlaps the filter with the traversal's critical path.
-// Every wait is bounded; overflow or a spent wait raises the abort flag.
+// Each warp expands up to 32 node pairs per iteration (one per lane).  It
+// keeps up to 32 of their children on its own shared-memory stack for its next
+// iteration, with no global round trip, and publishes the rest to the global
+// queue; leaf pairs (candidates) always go to the global candidate list, so
+// the first filter stage runs on warps that have no node pair at hand.  The
+// launch first seeds the queue: every overlapping pair of the two meshes'
+// depth-3 cut entries becomes a node pair (a leaf pair, a candidate).
+//
+// Slot protocol (queue and candidate list): producers reserve slots with one
+// atomic per warp, write the entries and, after a release fence, store the
+// call's tag in each slot's flag word.  A warp takes a ticket of 32
+// consecutive slots (one atomicAdd on the head counter), polls their 32 tag
+// words (one 128-byte line, so polling has no hot spot) and keeps the ticket
+// until all 32 slots are processed.  Only warps with empty stacks take node
+// tickets, and ready queue slots come before stack entries, so queued work
+// never waits behind a warp that is busy with its own.
+//
+// Termination: `work` is the number of node pairs that exist.  Seeds add to it
+// before the seed count completes; an expansion adds (children - expanded
+// pairs) in one atomic, issued before any child is published, so the count
+// never passes through zero while a node pair exists.  Reading seed_done ==
+// all seed tests and then work == 0 proves the traversal is over.  Every wait
+// is bounded; overflow or a spent wait raises the abort flag.
 // ---------------------------------------------------------------------------
-constexpr unsigned kIdleSpins = 1u << 22;  // consecutive idle polls of one warp (~1 s)
+constexpr unsigned kIdleSpins = 1u << 22;     // consecutive idle polls of one warp (~1 s)
+constexpr unsigned kWarpStack = 32;           // node pairs a warp keeps for its next iteration
+constexpr int kTravThreads = 256;
+constexpr int kTravWarps = kTravThreads / 32;
 
 __device__ __forceinline__ unsigned ld_vol(const unsigned* p)
 {
     return *(const volatile unsigned*)p;
 }
 
-__device__ __forceinline__ void publish(unsigned* flags, unsigned idx, unsigned tag)
+// Release / acquire fence at GPU scope: orders entry stores before the tag
+// stores that follow, and an observed tag before the entry loads that follow.
+__device__ __forceinline__ void fence_acq_rel()
 {
-    __threadfence();
-    *(volatile unsigned*)(flags + idx) = tag;
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
 }
 
 __device__ __forceinline__ unsigned take_ticket(unsigned* head)
@@ -759,129 +774,287 @@ __device__ __forceinline__ unsigned take_ticket(unsigned* head)
     return __shfl_sync(0xffffffffu, b, 0);
 }
 
+// Seeds the queue: pair (i, j) of the depth-3 cut entries of every job.  Warps
+// claim chunks of 32 seed tests with one atomic, so only warps that run do the
+// work (nothing waits for a block that never becomes resident); seed_done
+// counts finished tests after their node pairs are counted in `work`.
 template <bool F64>
-__global__ void __launch_bounds__(256, 2) k_traverse(Bufs B)
+__device__ __forceinline__ void seed_cut_pairs(const Bufs& B, unsigned total)
 {
+    using S = typename Prec<F64>::S;
     Counters* C = B.cnt;
     const unsigned lane = threadIdx.x & 31;
-    unsigned long long visited = 0, decided = 0;
-    unsigned maxlev = 0, idle = 0, backoff = 32;
-    unsigned nbase = take_ticket(&C->q_head);
-    unsigned npend = 0xffffffffu;  // lanes whose node slot is still to be processed
-    unsigned cbase = 0, cpend = 0;  // candidate ticket (cpend == 0: none held)
+    const unsigned per_job = (unsigned)kCutMax * kCutMax;
     for (;;) {
-        if (__any_sync(0xffffffffu, ld_vol(&C->abort_) != 0u)) break;
-        // ---- node pairs of the current ticket: poll this warp's own 32 tag words ----
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(&C->seed_head, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total) break;
+        const unsigned g = base + lane;
+        bool front = false, cand = false;
+        uint32_t ra = 0, rb = 0, job = 0;
+        if (g < total) {
+            job = g / per_job;
+            const unsigned t = g % per_job;
+            const JobDev& J = B.jobs[job];
+            const unsigned nA = (J.A.nt && J.B.nt) ? J.A.ncut : 0u, nB = J.B.ncut;
+            if (t < nA * nB) {
+                const unsigned i = t / nB, j = t % nB;
+                const S* ba_ = F64 ? (const S*)J.A.cutBox64 : (const S*)J.A.cutBox;
+                const S* bb_ = F64 ? (const S*)J.B.cutBox64 : (const S*)J.B.cutBox;
+                Box<S> ba, bb;
+                for (int k = 0; k < 3; k++) {
+                    ba.lo[k] = ba_[6 * i + k];
+                    ba.hi[k] = ba_[6 * i + 3 + k];
+                    bb.lo[k] = bb_[6 * j + k];
+                    bb.hi[k] = bb_[6 * j + 3 + k];
+                }
+                if (!J.pa.identity) world_box(J.pa, ba);
+                if (!J.pb.identity) world_box(J.pb, bb);
+                if (overlap(ba, bb)) {
+                    ra = J.A.cutRef[i];
+                    rb = J.B.cutRef[j];
+                    cand = (ra & kLeaf) && (rb & kLeaf);
+                    front = !cand;
+                }
+            }
+        }
+        const unsigned nfront = __popc(__ballot_sync(0xffffffffu, front));
+        unsigned pf = warp_append(front, &C->q_tail);
+        if (front) {
+            if (pf < B.cap_queue) B.queue[pf] = make_uint4(job, ra, rb, 0u);
+            else {
+                atomicOr(&C->overflow, kOvfFrontier);
+                atomicExch(&C->abort_, 1u);
+            }
+        }
+        unsigned pc = warp_append(cand, &C->cand);
+        if (cand) {
+            if (pc < B.cap_cand) B.cand[pc] = make_uint4(job, ra & ~kLeaf, rb & ~kLeaf, 0u);
+            else {
+                atomicOr(&C->overflow, kOvfCand);
+                atomicExch(&C->abort_, 1u);
+            }
+        }
+        if (lane == 0 && nfront) atomicAdd(&C->work, nfront);  // counted before any seed is published
+        __syncwarp();
+        fence_acq_rel();
+        if (front && pf < B.cap_queue) *(volatile unsigned*)(B.qflag + pf) = B.tag;
+        if (cand && pc < B.cap_cand) *(volatile unsigned*)(B.cflag + pc) = B.tag;
+        __syncwarp();
+        if (lane == 0) {
+            fence_acq_rel();
+            atomicAdd(&C->seed_done, min(32u, total - base));
+        }
+    }
+}
+
+// First filter stage on one candidate per lane (have = lane holds one):
+// intersecting pairs go to the result list, undecided ones to the escalation
+// list (one atomic per list per warp).
+template <bool F64>
+__device__ __forceinline__ void filter_candidates(const Bufs& B, bool have, const uint4& c,
+                                                  unsigned long long& decided, unsigned long long& tested)
+{
+    Counters* C = B.cnt;
+    int dec = DEC_NO;
+    uint32_t ta = 0, tb = 0;
+    if (have) {
+        tested++;
+        const JobDev& J = B.jobs[c.x];
+        double3 P[3], Q[3];
+        load_tri<F64>(J.A, J.pa, c.y, P, &ta);
+        load_tri<F64>(J.B, J.pb, c.z, Q, &tb);
+        if constexpr (F64) dec = classify_fast<double>(P, Q);
+        else dec = classify_fast<float>(P, Q);
+        decided += (dec != DEC_ESC);
+    }
+    const bool yes = have && dec == DEC_YES;
+    const bool esc = have && dec == DEC_ESC;
+    const unsigned pr = warp_append(yes, &C->res);
+    if (yes) {
+        if (pr < B.cap_res) B.res[pr] = make_uint4(c.x, ta, tb, 0u);
+        else atomicOr(&C->overflow, kOvfRes);
+    }
+    const unsigned pe = warp_append(esc, &C->esc);
+    if (esc) {
+        if (pe < B.cap_esc) B.esc[pe] = make_uint4(c.x, c.y, c.z, 0u);
+        else atomicOr(&C->overflow, kOvfEsc);
+    }
+}
+
+template <bool F64>
+__global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
+{
+    __shared__ uint4 stk[kTravWarps][kWarpStack];
+    Counters* C = B.cnt;
+    const unsigned lane = threadIdx.x & 31;
+    uint4* S = stk[threadIdx.x >> 5];
+    const unsigned seed_total = B.njobs * (unsigned)(kCutMax * kCutMax);
+    seed_cut_pairs<F64>(B, seed_total);
+    unsigned long long visited = 0, decided = 0, tested = 0;
+    unsigned maxlev = 0, idle = 0, backoff = 32;
+    unsigned sn = 0;         // node pairs on this warp's stack (warp-uniform, <= kWarpStack)
+    bool ticket = false;     // holds a node-queue ticket
+    unsigned nbase = 0, npend = 0;
+    unsigned cbase = take_ticket(&C->c_head);
+    unsigned cpend = 0xffffffffu;  // lanes whose candidate slot is still to be processed
+    unsigned iter = 0;
+    for (;;) {
+        ++iter;
+        if (!ticket && sn == 0u) {
+            nbase = take_ticket(&C->q_head);
+            npend = 0xffffffffu;
+            ticket = true;
+        }
         const unsigned ns = nbase + lane;
-        const bool nready = ((npend >> lane) & 1u) && ns < B.cap_queue && ld_vol(B.qflag + ns) == B.tag;
-        const unsigned navail = __ballot_sync(0xffffffffu, nready);
-        if (navail) {
+        const unsigned i = cbase + lane;
+        const bool nslot = ticket && ((npend >> lane) & 1u) && ns < B.cap_queue;
+        const bool cslot = ((cpend >> lane) & 1u) && i < B.cap_cand;
+        // everything this pass polls, issued together.  The abort flag is one
+        // line that every warp reads, so it is read every 8th pass only; its
+        // round trip overlaps the node loads of a warp that works from its stack.
+        unsigned ab = 0;
+        if (lane == 0 && (iter & 7u) == 0u) ab = ld_vol(&C->abort_);
+        const unsigned ntag = nslot ? ld_vol(B.qflag + ns) : 0u;
+        const unsigned ctag = cslot ? ld_vol(B.cflag + i) : 0u;
+        const bool from_queue = nslot && ntag == B.tag;
+        const unsigned qmask = __ballot_sync(0xffffffffu, from_queue);
+        if (sn != 0u || qmask != 0u) {
             idle = 0;
             backoff = 32;
+            // ready queue slots first (queued work is what idle warps wait
+            // for), the other lanes pop the stack
+            const unsigned take = min(sn, 32u - (unsigned)__popc(qmask));
+            const unsigned rank = (unsigned)__popc(~qmask & ((1u << lane) - 1u));
+            const bool from_stack = !from_queue && rank < take;
+            uint4 ent = make_uint4(0u, kEmpty, kEmpty, 0u);
+            if (from_stack) {
+                ent = S[sn - 1u - rank];
+            } else if (from_queue) {
+                fence_acq_rel();
+                ent = __ldcg(B.queue + ns);
+            }
+            sn -= take;
+            __syncwarp();  // popped entries are read before the pushes below reuse their slots
+            const bool have = from_stack || from_queue;
             unsigned fm = 0, cm = 0;
             uint32_t ca[4], cb[4];
-            uint4 ent = make_uint4(0u, kEmpty, kEmpty, 0u);
-            if (nready) {
-                __threadfence();
-                ent = __ldcg(B.queue + ns);
+            if (have) {
                 visited++;
                 maxlev = max(maxlev, ent.w);
                 expand_pair<F64>(B, ent, fm, cm, ca, cb);
             }
-            unsigned pf, pc;
-            warp_reserve2(__popc(fm), &C->q_tail, __popc(cm), &C->cand, &pf, &pc);
-            const unsigned pf0 = pf, pc0 = pc;
-            if (fm | cm) {
-                // entries first, one fence, then the tag words
+            // children: node pairs onto the stack (up to keep), the rest to the
+            // queue; candidates to the global candidate list
+            const unsigned nf = __popc(fm), nc = __popc(cm);
+            unsigned incf = nf, incc = nc;
 #pragma unroll
-                for (int q = 0; q < 16; q++) {
-                    const unsigned bit = 1u << q;
-                    if (fm & bit) {
-                        if (pf < B.cap_queue) B.queue[pf] = make_uint4(ent.x, ca[q >> 2], cb[q & 3], ent.w + 1u);
-                        pf++;
-                    }
-                    if (cm & bit) {
-                        if (pc < B.cap_cand) B.cand[pc] = make_uint4(ent.x, ca[q >> 2] & ~kLeaf, cb[q & 3] & ~kLeaf, 0u);
-                        pc++;
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned yf = __shfl_up_sync(0xffffffffu, incf, o);
+                const unsigned yc = __shfl_up_sync(0xffffffffu, incc, o);
+                if (lane >= (unsigned)o) {
+                    incf += yf;
+                    incc += yc;
+                }
+            }
+            const unsigned kf = __shfl_sync(0xffffffffu, incf, 31);
+            const unsigned kc = __shfl_sync(0xffffffffu, incc, 31);
+            const unsigned done = __popc(__ballot_sync(0xffffffffu, have));
+            const unsigned keep = min(kf, kWarpStack - sn);
+            unsigned qb = 0, cg = 0;
+            if (lane == 31) {
+                // node pairs made minus expanded, before any child is published
+                if (kf != done) atomicAdd(&C->work, kf - done);
+                if (kf > keep) qb = atomicAdd(&C->q_tail, kf - keep);
+                if (kc) cg = atomicAdd(&C->cand, kc);
+            }
+            qb = __shfl_sync(0xffffffffu, qb, 31);
+            cg = __shfl_sync(0xffffffffu, cg, 31);
+            const unsigned f0 = incf - nf;  // this lane's first node child in the warp's order
+            const unsigned c0 = cg + incc - nc;  // this lane's first candidate slot
+            {
+                unsigned g = f0, h = c0;
+                for (unsigned mm = fm | cm; mm != 0u; mm &= mm - 1u) {
+                    const unsigned q = (unsigned)__ffs(mm) - 1u;
+                    const uint32_t ra = sel4(ca, q >> 2), rb = sel4(cb, q & 3u);
+                    if ((fm >> q) & 1u) {
+                        const uint4 e = make_uint4(ent.x, ra, rb, ent.w + 1u);
+                        if (g < keep) {
+                            S[sn + g] = e;
+                        } else {
+                            const unsigned sl = qb + (g - keep);
+                            if (sl < B.cap_queue) B.queue[sl] = e;
+                        }
+                        g++;
+                    } else {
+                        if (h < B.cap_cand) B.cand[h] = make_uint4(ent.x, ra & ~kLeaf, rb & ~kLeaf, 0u);
+                        h++;
                     }
                 }
-                __threadfence();
-                for (unsigned q = pf0; q < pf; q++) {
-                    if (q < B.cap_queue) *(volatile unsigned*)(B.qflag + q) = B.tag;
-                    else {
+            }
+            __syncwarp();  // the work count above precedes every tag store below
+            const unsigned qx0 = max(f0, keep), qx1 = f0 + nf;
+            if (qx0 < qx1 || nc != 0u) {
+                fence_acq_rel();
+                for (unsigned x = qx0; x < qx1; x++) {
+                    const unsigned sl = qb + (x - keep);
+                    if (sl < B.cap_queue) {
+                        *(volatile unsigned*)(B.qflag + sl) = B.tag;
+                    } else {
                         atomicOr(&C->overflow, kOvfFrontier);
                         atomicExch(&C->abort_, 1u);
                     }
                 }
-                for (unsigned q = pc0; q < pc; q++) {
-                    if (q < B.cap_cand) *(volatile unsigned*)(B.cflag + q) = B.tag;
-                    else {
+                for (unsigned x = c0; x < c0 + nc; x++) {
+                    if (x < B.cap_cand) {
+                        *(volatile unsigned*)(B.cflag + x) = B.tag;
+                    } else {
                         atomicOr(&C->overflow, kOvfCand);
                         atomicExch(&C->abort_, 1u);
                     }
                 }
             }
-            __syncwarp();
-            if (lane == 0) atomicAdd(&C->q_done, (unsigned)__popc(navail));
-            npend &= ~navail;
-            if (npend == 0) {
-                nbase = take_ticket(&C->q_head);
-                npend = 0xffffffffu;
+            __syncwarp();  // stack pushes visible to the whole warp
+            sn += keep;
+            if (ticket) {
+                npend &= ~qmask;
+                if (npend == 0u) ticket = false;
             }
+            if (__any_sync(0xffffffffu, ab != 0u)) break;
             continue;
         }
-        // ---- candidates of the current candidate ticket ----
-        if (cpend == 0) {
-            cbase = take_ticket(&C->c_head);
-            cpend = 0xffffffffu;
-        }
-        const unsigned i = cbase + lane;
-        const bool cready = ((cpend >> lane) & 1u) && i < B.cap_cand && ld_vol(B.cflag + i) == B.tag;
+        if (__any_sync(0xffffffffu, ab != 0u)) break;
+        // ---- no node pair: candidates of the candidate ticket ----
+        const bool cready = cslot && ctag == B.tag;
         const unsigned cavail = __ballot_sync(0xffffffffu, cready);
         if (cavail) {
             idle = 0;
             backoff = 32;
-            int dec = DEC_NO;
-            uint32_t ta = 0, tb = 0, job = 0;
+            uint4 c = make_uint4(0u, 0u, 0u, 0u);
             if (cready) {
-                __threadfence();
-                const uint4 c = __ldcg(B.cand + i);
-                job = c.x;
-                const JobDev& J = B.jobs[job];
-                double3 P[3], Q[3];
-                load_tri<F64>(J.A, J.pa, c.y, P, &ta);
-                load_tri<F64>(J.B, J.pb, c.z, Q, &tb);
-                if constexpr (F64) dec = classify_fast<double>(P, Q);
-                else dec = classify_fast<float>(P, Q);
-                decided += (dec != DEC_ESC);
+                fence_acq_rel();
+                c = __ldcg(B.cand + i);
             }
-            const bool act = (cavail >> lane) & 1u;
-            const bool yes = act && dec == DEC_YES;
-            const bool esc = act && dec == DEC_ESC;
-            unsigned pr = warp_append(yes, &C->res);
-            if (yes) {
-                if (pr < B.cap_res) B.res[pr] = make_uint4(job, ta, tb, 0u);
-                else atomicOr(&C->overflow, kOvfRes);
-            }
-            unsigned pe = warp_append(esc, &C->esc);
-            if (esc) {
-                if (pe < B.cap_esc) B.esc[pe] = i;
-                else atomicOr(&C->overflow, kOvfEsc);
-            }
+            filter_candidates<F64>(B, cready, c, decided, tested);
             cpend &= ~cavail;
+            if (cpend == 0u) {
+                cbase = take_ticket(&C->c_head);
+                cpend = 0xffffffffu;
+            }
             continue;
         }
-        // ---- nothing ready: over, or wait.  Traversal over (q_done == q_tail,
-        // read in that order) means no slot will be published any more: the
-        // warp is done once none of its pending candidate slots lies below the
-        // final candidate count (its pending node slots are then all >= q_tail).
+        // ---- nothing ready: over, or wait.  Over (all seed tests done, then
+        // work == 0, read in that order) means no node pair exists any more and
+        // no slot will be published: the warp is done once none of its pending
+        // candidate slots lies below the final candidate count.
         if ((idle & 3u) == 3u) {
             unsigned over = 0, ncand = 0;
             if (lane == 0) {
-                const unsigned d = ld_vol(&C->q_done);
-                __threadfence();
-                const unsigned t = ld_vol(&C->q_tail);
-                over = d == t;
+                const unsigned sd = ld_vol(&C->seed_done);
+                fence_acq_rel();
+                const unsigned w = ld_vol(&C->work);
+                over = sd == seed_total && w == 0u;
                 ncand = min(ld_vol(&C->cand), B.cap_cand);
             }
             over = __shfl_sync(0xffffffffu, over, 0);
@@ -901,11 +1074,13 @@ __global__ void __launch_bounds__(256, 2) k_traverse(Bufs B)
     for (int o = 16; o > 0; o >>= 1) {
         visited += __shfl_xor_sync(0xffffffffu, visited, o);
         decided += __shfl_xor_sync(0xffffffffu, decided, o);
+        tested += __shfl_xor_sync(0xffffffffu, tested, o);
         maxlev = max(maxlev, __shfl_xor_sync(0xffffffffu, maxlev, o));
     }
     if (lane == 0) {
         if (visited) atomicAdd(&C->node_pairs, visited);
         if (decided) atomicAdd(&C->filter_decided, decided);
+        if (tested) atomicAdd(&C->tested, tested);
         atomicMax(&C->levels, maxlev + 1u);
     }
 }
@@ -928,7 +1103,7 @@ __global__ void __launch_bounds__(128) k_exact(Bufs B)
         bool yes = false;
         uint32_t ta = 0, tb = 0, job = 0;
         if (have) {
-            uint4 c = __ldcg(B.cand + __ldcg(B.esc + i));
+            uint4 c = __ldcg(B.esc + i);
             job = c.x;
             const JobDev& J = B.jobs[job];
             double3 pts[6];
@@ -1470,71 +1645,6 @@ cudaError_t launch_order_small(const Bufs& b, const OrderBufs& O, bool sort, con
 // ===========================================================================
 // Launchers
 // ===========================================================================
-// Initial frontier: every pair of cut entries (one thread each) whose world
-// boxes overlap becomes a node pair (or, if both are leaves, a candidate).
-template <bool F64>
-__global__ void __launch_bounds__(256) k_cut_pairs(Bufs B)
-{
-    using S = typename Prec<F64>::S;
-    Counters* C = B.cnt;
-    for (unsigned job = blockIdx.y; job < B.njobs; job += gridDim.y) {
-        const JobDev& J = B.jobs[job];
-        const unsigned nA = (J.A.nt && J.B.nt) ? J.A.ncut : 0u, nB = J.B.ncut;
-        const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
-        const bool have = t < nA * nB;
-        bool front = false, cand = false;
-        uint32_t ra = 0, rb = 0;
-        if (have) {
-            const unsigned i = t / nB, j = t % nB;
-            const S* ba_ = F64 ? (const S*)J.A.cutBox64 : (const S*)J.A.cutBox;
-            const S* bb_ = F64 ? (const S*)J.B.cutBox64 : (const S*)J.B.cutBox;
-            Box<S> ba, bb;
-            for (int k = 0; k < 3; k++) {
-                ba.lo[k] = ba_[6 * i + k];
-                ba.hi[k] = ba_[6 * i + 3 + k];
-                bb.lo[k] = bb_[6 * j + k];
-                bb.hi[k] = bb_[6 * j + 3 + k];
-            }
-            if (!J.pa.identity) world_box(J.pa, ba);
-            if (!J.pb.identity) world_box(J.pb, bb);
-            if (overlap(ba, bb)) {
-                ra = J.A.cutRef[i];
-                rb = J.B.cutRef[j];
-                cand = (ra & kLeaf) && (rb & kLeaf);
-                front = !cand;
-            }
-        }
-        unsigned pf = warp_append(front, &C->q_tail);
-        if (front) {
-            if (pf < B.cap_queue) {
-                B.queue[pf] = make_uint4(job, ra, rb, 0u);
-                publish(B.qflag, pf, B.tag);
-            } else {
-                atomicOr(&C->overflow, kOvfFrontier);
-                atomicExch(&C->abort_, 1u);
-            }
-        }
-        unsigned pc = warp_append(cand, &C->cand);
-        if (cand) {
-            if (pc < B.cap_cand) {
-                B.cand[pc] = make_uint4(job, ra & ~kLeaf, rb & ~kLeaf, 0u);
-                publish(B.cflag, pc, B.tag);
-            } else {
-                atomicOr(&C->overflow, kOvfCand);
-                atomicExch(&C->abort_, 1u);
-            }
-        }
-    }
-}
-
-cudaError_t launch_init_frontier(const Bufs& b, int precision, cudaStream_t st)
-{
-    dim3 grid((kCutMax * kCutMax + 255) / 256, b.njobs < 65535u ? b.njobs : 65535u);
-    if (precision == 1) k_cut_pairs<true><<<grid, 256, 0, st>>>(b);
-    else k_cut_pairs<false><<<grid, 256, 0, st>>>(b);
-    note_launches(1);
-    return cudaGetLastError();
-}
 
 cudaError_t query_launch(int device, LaunchCfg* cfg)
 {
@@ -1556,8 +1666,8 @@ cudaError_t query_launch(int device, LaunchCfg* cfg)
 cudaError_t launch_traverse(const Bufs& b, const LaunchCfg& cfg, int precision, cudaStream_t st)
 {
     note_launches(1);
-    if (precision == 1) k_traverse<true><<<cfg.trav_blocks64, 256, 0, st>>>(b);
-    else k_traverse<false><<<cfg.trav_blocks, 256, 0, st>>>(b);
+    if (precision == 1) k_traverse<true><<<cfg.trav_blocks64, kTravThreads, 0, st>>>(b);
+    else k_traverse<false><<<cfg.trav_blocks, kTravThreads, 0, st>>>(b);
     return cudaGetLastError();
 }
 

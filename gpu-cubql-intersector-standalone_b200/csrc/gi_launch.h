@@ -93,7 +93,5 @@ cudaError_t launch_order_small(const Bufs& b, const OrderBufs& O, bool sort, con
 unsigned long long launch_count();
 void note_launches(unsigned n);
 
-// Initial frontier: all overlapping pairs of the two meshes' depth-3 cuts, per job.
-cudaError_t launch_init_frontier(const Bufs& b, int precision, cudaStream_t st);
 
 }  // namespace gi
