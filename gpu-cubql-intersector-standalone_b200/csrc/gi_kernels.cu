@@ -1464,16 +1464,18 @@ cudaError_t launch_order_gather(const Bufs& b, const OrderBufs& O, bool sort, co
 //
 // At a few thousand to a few tens of thousands of results the radix passes
 // above are bound by launch and look-back latency, not by bytes.  Here each of
-// kOrderSmallBlocks blocks sorts one run of kOrderSmallRun keys in shared
-// memory (bitonic network), and since the (job, a, b) keys are unique, the
-// final position of a key is its index in its own run plus its lower bound in
-// every other run (binary searches in L2).  A third phase gathers the pairs
+// kOrderSmallBlocks blocks sorts one run of kOrderSmallRun keys, one key per
+// thread, with a bitonic network whose partner distances below 32 are warp
+// shuffles (only the longer ones go through shared memory).  The (job, a, b)
+// keys are unique, so the final position of a key is its rank in its own run
+// plus its lower bound in every other run: each block copies all sorted runs
+// into shared memory and searches them there.  A third phase gathers the pairs
 // and places the segments (block scan + the preceding runs' totals).  The
 // phases are separated by grid barriers; the launch is cooperative, so all
 // blocks are co-resident, and every barrier wait is bounded all the same.
 // ---------------------------------------------------------------------------
-constexpr int kOrderSmallThreads = 1024;
-static_assert(kOrderSmallRun == 2 * kOrderSmallThreads, "two keys per thread");
+constexpr int kOrderSmallThreads = kOrderSmallRun;  // one key per thread
+constexpr size_t kOrderSmallDyn = sizeof(unsigned long long) * kOrderSmallMax;  // all runs, phase 2
 
 // Arrive at grid barrier `k` (1-based) of the launch; waits bounded.  On a spent
 // wait the error bit is set and later barriers of the block no longer wait.
@@ -1503,6 +1505,7 @@ __global__ void __launch_bounds__(kOrderSmallThreads, 1)
                   int32_t* pairs_out, uint32_t* job_out, double* segs_out, int32_t* segpair_out, int want_segments,
                   int sorted)
 {
+    extern __shared__ unsigned long long allk[];  // every sorted run (phase 2)
     __shared__ unsigned long long sk[kOrderSmallRun];
     __shared__ uint32_t sv[kOrderSmallRun];
     __shared__ uint32_t sw[33];
@@ -1514,6 +1517,7 @@ __global__ void __launch_bounds__(kOrderSmallThreads, 1)
         return;
     }
     if (threadIdx.x == 0) s_ok = 1u;
+    const unsigned tid = threadIdx.x;
     const unsigned nruns = (n + kOrderSmallRun - 1) / kOrderSmallRun;
     const unsigned t = blockIdx.x;
     const unsigned base = t * kOrderSmallRun;
@@ -1522,107 +1526,108 @@ __global__ void __launch_bounds__(kOrderSmallThreads, 1)
     unsigned bar = 0;
     if (sorted) {
         // ---- phase 1: sort this block's run (padding keys sort last) ----
-        for (unsigned i = threadIdx.x; i < kOrderSmallRun; i += kOrderSmallThreads) {
-            if (i < len) {
-                sk[i] = order_key(__ldcg(B.res + base + i), O);
-                sv[i] = base + i;
-            } else {
-                sk[i] = ~0ull;
-                sv[i] = 0xffffffffu;
-            }
-        }
-        __syncthreads();
+        unsigned long long key = tid < len ? order_key(__ldcg(B.res + base + tid), O) : ~0ull;
+        uint32_t val = tid < len ? base + tid : 0xffffffffu;
         if (len > 1) {  // uniform in the block
             for (unsigned k = 2; k <= (unsigned)kOrderSmallRun; k <<= 1)
                 for (unsigned j = k >> 1; j > 0; j >>= 1) {
-                    const unsigned i = threadIdx.x;
-                    const unsigned lo = 2 * i - (i & (j - 1));
-                    const unsigned hi = lo + j;
-                    const bool up = (lo & k) == 0;
-                    const unsigned long long a = sk[lo], b = sk[hi];
-                    if ((a > b) == up) {
-                        sk[lo] = b;
-                        sk[hi] = a;
-                        const uint32_t va = sv[lo];
-                        sv[lo] = sv[hi];
-                        sv[hi] = va;
+                    unsigned long long pk;
+                    uint32_t pv;
+                    if (j >= 32u) {
+                        __syncthreads();  // the previous stage's reads are done
+                        sk[tid] = key;
+                        sv[tid] = val;
+                        __syncthreads();
+                        pk = sk[tid ^ j];
+                        pv = sv[tid ^ j];
+                    } else {
+                        pk = __shfl_xor_sync(0xffffffffu, key, j);
+                        pv = __shfl_xor_sync(0xffffffffu, val, j);
                     }
-                    __syncthreads();
+                    // the lower index of an ascending pair (or the upper of a
+                    // descending one) keeps the smaller key
+                    const bool keep_min = ((tid & j) == 0u) == ((tid & k) == 0u);
+                    if (keep_min ? (pk < key) : (pk > key)) {
+                        key = pk;
+                        val = pv;
+                    }
                 }
         }
-        for (unsigned i = threadIdx.x; i < len; i += kOrderSmallThreads) O.keys[0][base + i] = sk[i];
+        if (tid < len) O.keys[0][base + tid] = key;
         grid_barrier(&C->obar, ++bar, &C->err, &s_ok);
-        // ---- phase 2: final position = own index + lower bounds in the other runs ----
-        for (unsigned i = threadIdx.x; i < len; i += kOrderSmallThreads) {
-            const unsigned long long x = sk[i];
-            unsigned pos = i;
-            for (unsigned s0 = 0; s0 < nruns; s0 += 8) {
-                unsigned lo[8], hi[8];
+        // ---- phase 2: final position = own rank + lower bounds in the other runs ----
+        // all runs into shared memory: every copy is issued before any is
+        // waited for (asynchronous 16-byte copies through L2 only: the key
+        // buffer is rewritten by every call, so no L1 copy of it may be used;
+        // an odd last key is loaded the same way, through L2)
+        for (unsigned c = tid; c < n / 2u; c += kOrderSmallThreads) {
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(allk + 2u * c);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(O.keys[0] + 2u * c)
+                         : "memory");
+        }
+        if ((n & 1u) && tid == 0) allk[n - 1u] = __ldcg(O.keys[0] + (n - 1u));
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        __syncthreads();
+        if (tid < len) {
+            unsigned pos = tid;
+            for (unsigned s0 = 0; s0 < nruns; s0 += 4) {
+                unsigned lo[4], hi[4];
 #pragma unroll
-                for (int r = 0; r < 8; r++) {
+                for (int r = 0; r < 4; r++) {
                     const unsigned s = s0 + r;
-                    lo[r] = 0u;
-                    hi[r] = (s < nruns && s != t) ? min((unsigned)kOrderSmallRun, n - s * kOrderSmallRun) : 0u;
+                    lo[r] = s * kOrderSmallRun;
+                    hi[r] = (s < nruns && s != t) ? lo[r] + min((unsigned)kOrderSmallRun, n - s * kOrderSmallRun)
+                                                  : lo[r];
                 }
-                for (int step = 0; step < 12; step++) {  // 2^11 < kOrderSmallRun + 1 <= 2^12
 #pragma unroll
-                    for (int r = 0; r < 8; r++) {
+                for (int r = 0; r < 4; r++) pos -= lo[r];  // counts are relative to each run's start
+                for (int step = 0; step < 10; step++) {  // 2^9 < kOrderSmallRun + 1 <= 2^10
+#pragma unroll
+                    for (int r = 0; r < 4; r++) {
                         if (lo[r] < hi[r]) {
                             const unsigned mid = (lo[r] + hi[r]) >> 1;
-                            const unsigned long long v = __ldcg(O.keys[0] + (size_t)(s0 + r) * kOrderSmallRun + mid);
-                            if (v < x) lo[r] = mid + 1u;
+                            if (allk[mid] < key) lo[r] = mid + 1u;
                             else hi[r] = mid;
                         }
                     }
                 }
 #pragma unroll
-                for (int r = 0; r < 8; r++) pos += lo[r];
+                for (int r = 0; r < 4; r++) pos += lo[r];
             }
-            if (pos < n) perm[pos] = sv[i];
+            if (pos < n) perm[pos] = val;
         }
         grid_barrier(&C->obar, ++bar, &C->err, &s_ok);
     }
-    // ---- phase 3: gather pairs, place segments (two sorted positions per thread) ----
-    unsigned src[2], cnt[2];
-    uint4 rr[2];
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-        const unsigned local = 2 * threadIdx.x + q;
-        const bool ok = local < len;
-        src[q] = ok ? (sorted ? __ldcg(perm + base + local) : base + local) : 0u;
-        if (src[q] >= n) src[q] = 0u;
-        cnt[q] = (ok && want_segments) ? __ldcg(nseg + src[q]) : 0u;
-        rr[q] = ok ? __ldcg(B.res + src[q]) : make_uint4(0u, 0u, 0u, 0u);
-    }
+    // ---- phase 3: gather pairs, place segments (one sorted position per thread) ----
+    const unsigned k = base + tid;
+    const bool ok = tid < len;
+    unsigned src = ok ? (sorted ? __ldcg(perm + k) : k) : 0u;
+    if (src >= n) src = 0u;
+    const unsigned cnt = (ok && want_segments) ? __ldcg(nseg + src) : 0u;
+    const uint4 rr = ok ? __ldcg(B.res + src) : make_uint4(0u, 0u, 0u, 0u);
     unsigned tot;
-    const unsigned ex = block_exclusive_scan(cnt[0] + cnt[1], sw, &tot);
-    if (threadIdx.x == 0) O.tile_tot[t] = tot;
+    const unsigned ex = block_exclusive_scan(cnt, sw, &tot);
+    if (tid == 0) O.tile_tot[t] = tot;
     grid_barrier(&C->obar, ++bar, &C->err, &s_ok);
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         unsigned b0 = 0;
         for (unsigned s = 0; s < t; s++) b0 += __ldcg(O.tile_tot + s);
         s_base = b0;
         if (nruns && t == nruns - 1) C->nseg = b0 + tot;
     }
     __syncthreads();
-    unsigned off = s_base + ex;
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-        const unsigned local = 2 * threadIdx.x + q;
-        if (local >= len) continue;
-        const unsigned k = base + local;
-        pairs_out[2 * (size_t)k] = (int32_t)rr[q].y;
-        pairs_out[2 * (size_t)k + 1] = (int32_t)rr[q].z;
-        job_out[k] = rr[q].x;
-        for (unsigned e = 0; e < cnt[q]; e++) {
-            const double2* sp = reinterpret_cast<const double2*>(segs + 18 * (size_t)src[q] + 6 * e);
-            double2* dp = reinterpret_cast<double2*>(segs_out + 6 * (size_t)(off + e));
-            dp[0] = __ldcg(sp);
-            dp[1] = __ldcg(sp + 1);
-            dp[2] = __ldcg(sp + 2);
-            segpair_out[off + e] = (int32_t)k;
-        }
-        off += cnt[q];
+    if (!ok) return;
+    pairs_out[2 * (size_t)k] = (int32_t)rr.y;
+    pairs_out[2 * (size_t)k + 1] = (int32_t)rr.z;
+    job_out[k] = rr.x;
+    const unsigned off = s_base + ex;
+    for (unsigned e = 0; e < cnt; e++) {
+        const double2* sp = reinterpret_cast<const double2*>(segs + 18 * (size_t)src + 6 * e);
+        double2* dp = reinterpret_cast<double2*>(segs_out + 6 * (size_t)(off + e));
+        dp[0] = __ldcg(sp);
+        dp[1] = __ldcg(sp + 1);
+        dp[2] = __ldcg(sp + 2);
+        segpair_out[off + e] = (int32_t)k;
     }
 }
 
@@ -1630,14 +1635,17 @@ cudaError_t launch_order_small(const Bufs& b, const OrderBufs& O, bool sort, con
                                const uint32_t* nseg, int32_t* pairs_out, uint32_t* job_out, double* segs_out,
                                int32_t* segpair_out, bool want_segments, cudaStream_t st)
 {
+    cudaError_t e = cudaFuncSetAttribute((const void*)k_order_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kOrderSmallDyn);
+    if (e != cudaSuccess) return e;
     Bufs bb = b;
     OrderBufs oo = O;
     const double* a_segs = segs;
     const uint32_t* a_nseg = nseg;
     int ws = want_segments ? 1 : 0, so = sort ? 1 : 0;
     void* args[] = {&bb, &oo, &a_segs, &a_nseg, &pairs_out, &job_out, &segs_out, &segpair_out, &ws, &so};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_order_small, dim3(kOrderSmallBlocks),
-                                                dim3(kOrderSmallThreads), args, 0, st);
+    e = cudaLaunchCooperativeKernel((const void*)k_order_small, dim3(kOrderSmallBlocks), dim3(kOrderSmallThreads),
+                                    args, kOrderSmallDyn, st);
     note_launches(1);
     return e;
 }

@@ -83,8 +83,8 @@ cudaError_t launch_order_gather(const Bufs& b, const OrderBufs& O, bool sort, co
 // each sorting a run of kOrderSmallRun keys, for up to kOrderSmallMax results.
 // If the call produced more, the kernel only sets Counters::order_redo and the
 // caller reruns with launch_order_gather.  Keys must fit in 63 bits.
-constexpr int kOrderSmallRun = 2048;
-constexpr int kOrderSmallBlocks = 32;
+constexpr int kOrderSmallRun = 512;
+constexpr int kOrderSmallBlocks = 48;
 constexpr uint32_t kOrderSmallMax = (uint32_t)kOrderSmallRun * kOrderSmallBlocks;
 cudaError_t launch_order_small(const Bufs& b, const OrderBufs& O, bool sort, const double* segs,
                                const uint32_t* nseg, int32_t* pairs_out, uint32_t* job_out, double* segs_out,
