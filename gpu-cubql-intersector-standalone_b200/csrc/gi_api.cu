@@ -132,7 +132,6 @@ extern "C" gi_status gi_destroy(gi_ctx* c)
     if (c->pool) cudaMemPoolDestroy(c->pool);
     if (c->h_cnt) cudaFreeHost(c->h_cnt);
     if (c->h_jobs) cudaFreeHost(c->h_jobs);
-    if (c->h_stage) cudaFreeHost(c->h_stage);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->st) cudaStreamDestroy(c->st);
@@ -413,18 +412,14 @@ static gi_status ensure_fp64(gi_ctx* c, gi_mesh* m)
     return GI_OK;
 }
 
-static gi_status ensure_pinned(gi_ctx* c, size_t bytes)
+// A pinned block of at least `need` bytes for this call's results in *buf
+// (the block held so far goes back to the pool if it is too small).
+static gi_status pinned_for(gi_ctx* c, PinnedBuf** buf, size_t need)
 {
-    if (bytes <= c->h_stage_bytes) return GI_OK;
-    if (c->h_stage) cudaFreeHost(c->h_stage);
-    c->h_stage = nullptr;
-    size_t want = std::max(bytes, (size_t)1 << 20);
-    if (cudaMallocHost(&c->h_stage, want) != cudaSuccess) {
-        c->h_stage_bytes = 0;
-        return set_err(c, GI_ERR_OOM, "pinned staging");
-    }
-    c->h_stage_bytes = want;
-    return GI_OK;
+    if (*buf && (*buf)->bytes >= need) return GI_OK;
+    if (*buf) c->pinned->put(*buf);
+    *buf = c->pinned->get(need);
+    return *buf ? GI_OK : set_err(c, GI_ERR_OOM, "pinned result staging");
 }
 
 // Core: runs the job list on the device and fills per-job results.
@@ -472,6 +467,16 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
     uint32_t nres = 0, nsegs = 0;
     char* hp = nullptr;
     size_t off_jobs = 0, off_segs = 0, off_segpair = 0;
+    // pinned block the results land in; returned to the pool on every early exit
+    PinnedBuf* buf = nullptr;
+    struct BufGuard {
+        gi_ctx* c;
+        PinnedBuf*& b;
+        ~BufGuard()
+        {
+            if (b) c->pinned->put(b);
+        }
+    } guard{c, buf};
     // ordering path: one cooperative launch when the previous call's count says
     // the result will be small (the kernel refuses, and this loop reruns on the
     // radix path, if it is not)
@@ -561,9 +566,9 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         off_segs = off_jobs + (nj > 1 ? sizeof(uint32_t) * (size_t)pp : 0);
         off_segs = (off_segs + 15) & ~(size_t)15;
         off_segpair = off_segs + sizeof(double) * 6 * (size_t)ps;
-        gi_status s = ensure_pinned(c, off_segpair + sizeof(int32_t) * (size_t)ps + 64);
+        gi_status s = pinned_for(c, &buf, off_segpair + sizeof(int32_t) * (size_t)ps + 64);
         if (s != GI_OK) return s;
-        hp = (char*)c->h_stage;
+        hp = (char*)buf->p;
         CK(c, cudaMemcpyAsync(c->h_cnt, c->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, c->st), "counters");
         CK(c, cudaMemcpyAsync(hp, c->pairs_out, off_jobs, cudaMemcpyDeviceToHost, c->st), "copy pairs");
         if (nj > 1)
@@ -604,9 +609,9 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
             off_jobs = sizeof(int32_t) * 2 * (size_t)nres;
             off_segs = (off_jobs + (nj > 1 ? sizeof(uint32_t) * (size_t)nres : 0) + 15) & ~(size_t)15;
             off_segpair = off_segs + sizeof(double) * 6 * (size_t)nsegs;
-            s = ensure_pinned(c, off_segpair + sizeof(int32_t) * (size_t)nsegs + 64);
+            s = pinned_for(c, &buf, off_segpair + sizeof(int32_t) * (size_t)nsegs + 64);
             if (s != GI_OK) return s;
-            hp = (char*)c->h_stage;
+            hp = (char*)buf->p;
             if (nres) CK(c, cudaMemcpyAsync(hp, c->pairs_out, off_jobs, cudaMemcpyDeviceToHost, c->st), "copy pairs");
             if (nres && nj > 1)
                 CK(c, cudaMemcpyAsync(hp + off_jobs, c->job_out, sizeof(uint32_t) * nres, cudaMemcpyDeviceToHost,
@@ -641,23 +646,37 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         for (uint32_t k = 0; k < nres; k++) job_start[hj[k] + 1]++;
         for (uint32_t j = 0; j < nj; j++) job_start[j + 1] += job_start[j];
     }
+    // results are views into the pinned block (no further copy); a batch's
+    // segment pair indices are rebased to each job in place
     const int32_t* hpairs = (const int32_t*)hp;
     const double* hsegs = (const double*)(hp + off_segs);
-    const int32_t* hsegpair = (const int32_t*)(hp + off_segpair);
+    int32_t* hsegpair = (int32_t*)(hp + off_segpair);
+    for (uint32_t j = 0; j < nj; j++) {
+        outs[j] = new (std::nothrow) gi_result();
+        if (!outs[j]) {
+            for (uint32_t k = 0; k < j; k++) {
+                delete outs[k];
+                outs[k] = nullptr;
+            }
+            return set_err(c, GI_ERR_OOM, "result");
+        }
+    }
+    buf->refs.store((int)nj);
+    buf->home = c->pinned;
     size_t sp = 0;
     for (uint32_t j = 0; j < nj; j++) {
-        gi_result* r = new (std::nothrow) gi_result();
-        if (!r) return GI_ERR_OOM;
+        gi_result* r = outs[j];
+        r->buf = buf;
         uint32_t a = job_start[j], e = job_start[j + 1];
-        r->pairs.assign(hpairs + 2 * (size_t)a, hpairs + 2 * (size_t)e);
+        r->pairs = hpairs + 2 * (size_t)a;
+        r->npairs = e - a;
         size_t s0 = sp;
         while (sp < nsegs && (uint32_t)hsegpair[sp] < e) sp++;
-        if (sp > s0) {
-            r->segs.assign(hsegs + 6 * s0, hsegs + 6 * sp);
-            r->seg_pair.assign(hsegpair + s0, hsegpair + sp);
-            if (a)
-                for (auto& q : r->seg_pair) q -= (int32_t)a;
-        }
+        r->segs = hsegs + 6 * s0;
+        r->seg_pair = hsegpair + s0;
+        r->nsegs = sp - s0;
+        if (a)
+            for (size_t q = s0; q < sp; q++) hsegpair[q] -= (int32_t)a;
         gi_stats& s2 = r->stats;
         memset(&s2, 0, sizeof s2);
         s2.tris_a = jobs[j].A.nt;
@@ -665,7 +684,7 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         s2.nodes_a = jobs[j].A.nnodes;
         s2.nodes_b = jobs[j].B.nnodes;
         s2.pairs = e - a;
-        s2.segments = r->seg_pair.size();
+        s2.segments = r->nsegs;
         // launch-wide counters (shared by all jobs of a batch)
         s2.node_pairs = H.node_pairs;
         s2.candidates = H.tested;
@@ -681,8 +700,8 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         s2.ms_segments = ms_seg;
         s2.ms_sort = ms_sort;
         s2.ms_total = ms_total;
-        outs[j] = r;
     }
+    buf = nullptr;  // now held by the results
     return GI_OK;
 }
 
@@ -760,16 +779,16 @@ extern "C" gi_status gi_intersect_oneshot(gi_ctx* c, const double* vA, uint32_t 
 extern "C" gi_status gi_result_pairs(const gi_result* r, const int32_t** p, uint64_t* n)
 {
     if (!r || !p || !n) return GI_ERR_INVALID_ARG;
-    *p = r->pairs.data();
-    *n = r->pairs.size() / 2;
+    *p = r->pairs;
+    *n = r->npairs;
     return GI_OK;
 }
 extern "C" gi_status gi_result_segments(const gi_result* r, const double** s, const int32_t** sp, uint64_t* n)
 {
     if (!r || !s || !n) return GI_ERR_INVALID_ARG;
-    *s = r->segs.data();
-    if (sp) *sp = r->seg_pair.data();
-    *n = r->seg_pair.size();
+    *s = r->segs;
+    if (sp) *sp = r->seg_pair;
+    *n = r->nsegs;
     return GI_OK;
 }
 extern "C" gi_status gi_result_stats(const gi_result* r, gi_stats* out)
@@ -781,6 +800,7 @@ extern "C" gi_status gi_result_stats(const gi_result* r, gi_stats* out)
 extern "C" gi_status gi_result_free(gi_result* r)
 {
     if (!r) return GI_ERR_INVALID_ARG;
+    pinned_release(r->buf);
     delete r;
     return GI_OK;
 }

@@ -2,6 +2,7 @@
 // (shared by the translation units that implement the C ABI).
 #pragma once
 #include <atomic>
+#include <memory>
 #include <cstdio>
 #include <mutex>
 #include <string>
@@ -20,10 +21,92 @@ struct gi_mesh {
     bool has64 = false;
 };
 
+// Pinned host blocks that results are copied into.  A call takes one block
+// from its context's pool; the results of that call point into it (no further
+// copy) and the block goes back to the pool when the last of them is freed,
+// even after the context itself is gone.
+struct PinnedPool;
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    std::atomic<int> refs{0};
+    std::shared_ptr<PinnedPool> home;  // set while results hold the block
+};
+struct PinnedPool {
+    std::mutex mu;
+    std::vector<PinnedBuf*> free_list;
+    static constexpr size_t kKeepFree = 4;  // blocks kept for reuse; more are released
+    ~PinnedPool()
+    {
+        for (PinnedBuf* b : free_list) {
+            cudaFreeHost(b->p);
+            delete b;
+        }
+    }
+    // smallest free block of at least `bytes`, or a new one (nullptr: out of pinned memory)
+    PinnedBuf* get(size_t bytes)
+    {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            size_t best = free_list.size();
+            for (size_t i = 0; i < free_list.size(); i++)
+                if (free_list[i]->bytes >= bytes && (best == free_list.size() || free_list[i]->bytes < free_list[best]->bytes))
+                    best = i;
+            if (best != free_list.size()) {
+                PinnedBuf* b = free_list[best];
+                free_list.erase(free_list.begin() + (long)best);
+                return b;
+            }
+        }
+        PinnedBuf* b = new (std::nothrow) PinnedBuf();
+        if (!b) return nullptr;
+        const size_t want = bytes + bytes / 4 > ((size_t)1 << 20) ? bytes + bytes / 4 : ((size_t)1 << 20);
+        if (cudaMallocHost(&b->p, want) != cudaSuccess) {
+            delete b;
+            return nullptr;
+        }
+        b->bytes = want;
+        return b;
+    }
+    void put(PinnedBuf* b)
+    {
+        PinnedBuf* drop = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            free_list.push_back(b);
+            if (free_list.size() > kKeepFree) {  // release the smallest
+                size_t k = 0;
+                for (size_t i = 1; i < free_list.size(); i++)
+                    if (free_list[i]->bytes < free_list[k]->bytes) k = i;
+                drop = free_list[k];
+                free_list.erase(free_list.begin() + (long)k);
+            }
+        }
+        if (drop) {
+            cudaFreeHost(drop->p);
+            delete drop;
+        }
+    }
+};
+// Drops one result's hold on a block (the block returns to its pool at zero).
+inline void pinned_release(PinnedBuf* b)
+{
+    if (!b || b->refs.fetch_sub(1) != 1) return;
+    std::shared_ptr<PinnedPool> pool = std::move(b->home);
+    if (pool) pool->put(b);
+    else {
+        cudaFreeHost(b->p);
+        delete b;
+    }
+}
+
 struct gi_result {
-    std::vector<int32_t> pairs;
-    std::vector<double> segs;
-    std::vector<int32_t> seg_pair;
+    PinnedBuf* buf = nullptr;  // storage of the arrays below (shared by the results of one call)
+    const int32_t* pairs = nullptr;
+    uint64_t npairs = 0;
+    const double* segs = nullptr;
+    const int32_t* seg_pair = nullptr;
+    uint64_t nsegs = 0;
     gi_stats stats;
 };
 
@@ -66,9 +149,8 @@ struct gi_ctx {
     uint64_t pred_pairs = 0, pred_segs = 0;  // result sizes of the previous call
     void* order_scratch = nullptr;
     size_t order_scratch_bytes = 0;
-    // pinned staging for results
-    void* h_stage = nullptr;
-    size_t h_stage_bytes = 0;
+    // pinned blocks the results are copied into
+    std::shared_ptr<PinnedPool> pinned = std::make_shared<PinnedPool>();
     cudaEvent_t ev[8] = {};
 };
 

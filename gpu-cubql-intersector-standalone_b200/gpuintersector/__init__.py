@@ -244,30 +244,68 @@ class Mesh:
             pass
 
 
+class _ResultOwner:
+    """Holds a gi_result handle; frees it when the last view of its arrays is gone."""
+
+    __slots__ = ("handle",)
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    def __del__(self):
+        try:
+            lib().gi_result_free(self.handle)
+        except Exception:
+            pass
+
+
+class _View:
+    """numpy array interface over memory owned by a gi_result (keeps it alive)."""
+
+    __slots__ = ("__array_interface__", "owner")
+
+    def __init__(self, owner, addr, shape, dtype):
+        self.owner = owner
+        self.__array_interface__ = {"shape": shape, "typestr": np.dtype(dtype).str, "data": (addr, False),
+                                    "version": 3}
+
+
 class Result:
-    """Pairs (n, 2) int32 sorted by (a, b); segments (m, 6) float64; seg_pair (m,)."""
+    """Pairs (n, 2) int32 sorted by (a, b); segments (m, 6) float64; seg_pair (m,).
+
+    Results up to ZERO_COPY_BYTES are numpy views of the library's pinned result
+    block (no copy; the block is released when the last view is dropped);
+    larger ones are copied out and the block is released at once, so holding
+    many large results pins no host memory."""
+
+    ZERO_COPY_BYTES = 4 << 20
 
     def __init__(self, handle):
         L = lib()
         p = ctypes.POINTER(ctypes.c_int32)()
         n = ctypes.c_uint64()
         L.gi_result_pairs(handle, ctypes.byref(p), ctypes.byref(n))
-        self.pairs = (np.ctypeslib.as_array(p, shape=(n.value * 2,)).reshape(-1, 2).copy()
-                      if n.value else np.zeros((0, 2), dtype=np.int32))
         sp = ctypes.POINTER(ctypes.c_double)()
         spp = ctypes.POINTER(ctypes.c_int32)()
         m = ctypes.c_uint64()
         L.gi_result_segments(handle, ctypes.byref(sp), ctypes.byref(spp), ctypes.byref(m))
-        if m.value:
-            self.segments = np.ctypeslib.as_array(sp, shape=(m.value * 6,)).reshape(-1, 6).copy()
-            self.seg_pair = np.ctypeslib.as_array(spp, shape=(m.value,)).copy()
-        else:
-            self.segments = np.zeros((0, 6))
-            self.seg_pair = np.zeros((0,), dtype=np.int32)
         st = _abi.Stats()
         L.gi_result_stats(handle, ctypes.byref(st))
         self.stats = st.as_dict()
-        L.gi_result_free(handle)
+        npairs, nsegs = n.value, m.value
+        owner = _ResultOwner(handle)
+        zero_copy = 8 * npairs + 52 * nsegs <= self.ZERO_COPY_BYTES
+
+        def arr(ptr, shape, dtype, count):
+            if count == 0:
+                return np.zeros(shape, dtype=dtype)
+            a = np.asarray(_View(owner, ctypes.cast(ptr, ctypes.c_void_p).value, shape, dtype))
+            return a if zero_copy else a.copy()
+
+        self.pairs = arr(p, (npairs, 2), np.int32, npairs)
+        self.segments = arr(sp, (nsegs, 6), np.float64, nsegs)
+        self.seg_pair = arr(spp, (nsegs,), np.int32, nsegs)
+        del owner  # freed here if every array was copied or empty
 
 
 class Server:
