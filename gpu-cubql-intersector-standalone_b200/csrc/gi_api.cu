@@ -358,6 +358,32 @@ DevPose make_dev_pose(const gi_pose& p)
         d.padm[r] = nextafterf((float)d.padm64[r], INFINITY);
     }
     for (int i = 0; i < 9; i++) d.Rf[i] = (float)d.R[i];
+    // inverse map, used to test boxes in this mesh's own frame as well
+    if (!d.identity) {
+        double eta = 0.0;
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) {
+                double g = 0.0;
+                for (int k = 0; k < 3; k++) g += d.R[3 * k + i] * d.R[3 * k + j];
+                eta = std::max(eta, fabs(g - (i == j ? 1.0 : 0.0)));
+            }
+        d.inv_eta = eta;
+        d.inv_ok = eta <= 0x1p-30 ? 1 : 0;
+        for (int r = 0; r < 3; r++)
+            for (int k = 0; k < 3; k++) d.Ri64[3 * r + k] = d.R[3 * k + r];
+        for (int r = 0; r < 3; r++) {
+            double acc = 0.0, m = fabs(d.C[r]);
+            for (int k = 0; k < 3; k++) {
+                acc += d.Ri64[3 * r + k] * (d.C[k] + d.T[k]);
+                m += fabs(d.Ri64[3 * r + k]) * (fabs(d.C[k]) + fabs(d.T[k]));
+            }
+            d.bi64[r] = d.C[r] - acc;
+            d.padmi64[r] = m * (1.0 + 0x1p-40);
+            d.bif[r] = (float)d.bi64[r];
+            d.padmi[r] = nextafterf((float)d.padmi64[r], INFINITY);
+        }
+        for (int i = 0; i < 9; i++) d.Rif[i] = (float)d.Ri64[i];
+    }
     return d;
 }
 
@@ -541,6 +567,7 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         b.cap_esc = c->cap_esc;
         b.cnt = c->d_cnt;
         b.precision = prec;
+        b.two_frame = nj > 1 ? 1 : 0;
         CK(c, cudaMemsetAsync(c->d_cnt, 0, sizeof(Counters), c->st), "counters");
         CK(c, cudaEventRecord(c->ev[0], c->st), "event");
         CK(c, launch_traverse(b, c->cfg, prec, c->st), "traverse");

@@ -42,6 +42,12 @@ struct DevPose {
     double padm64[3];  // |C| + |T| + |R||C| (FP64), magnitude term of the pad
     float Rf[9], bf[3], padm[3];
     int identity;
+    // world -> local (inverse) map for a near-orthonormal R: local = Ri*w + bi
+    // with Ri = R^T; inv_ok = 0 when R is not orthonormal within 2^-30
+    int inv_ok;
+    double inv_eta;    // max |R^T R - I| entry: error of R^T as the inverse
+    double Ri64[9], bi64[3], padmi64[3];
+    float Rif[9], bif[3], padmi[3];
     int pad_[3];
 };
 
@@ -121,6 +127,7 @@ struct Bufs {
     Counters* cnt;
     unsigned tag;     // nonzero, different for every call on the context
     int precision;    // 0 FP32 cascade, 1 FP64
+    int two_frame;    // also test child boxes in B's own frame (fewer pairs, more work per pair)
 };
 
 }  // namespace gi

@@ -515,6 +515,52 @@ __device__ __forceinline__ void world_box(const DevPose& P, Box<double>& b)
     }
 }
 
+// World box -> conservative box in the local frame of pose P (inverse map
+// local = Ri*w + bi, Ri = R^T).  Same construction and bound as world_box; the
+// pad also covers the error of R^T as the inverse (inv_eta <= 2^-30) and the
+// FP64 rounding of the posed vertices.
+__device__ __forceinline__ void local_box(const DevPose& P, Box<float>& b)
+{
+    float c[3], h[3];
+    for (int k = 0; k < 3; k++) {
+        c[k] = 0.5f * b.lo[k] + 0.5f * b.hi[k];
+        h[k] = 0.5f * b.hi[k] - 0.5f * b.lo[k];
+    }
+    for (int r = 0; r < 3; r++) {
+        float wc = P.bif[r], wh = 0.0f, mag = P.padmi[r];
+        for (int k = 0; k < 3; k++) {
+            float a = P.Rif[3 * r + k];
+            wc = fmaf(a, c[k], wc);
+            wh = fmaf(fabsf(a), h[k], wh);
+            mag = fmaf(fabsf(a), fabsf(c[k]) + h[k], mag);
+        }
+        float pad = fmaf(0x1p-19f, mag, 0x1p-120f);
+        b.lo[r] = wc - wh - pad;
+        b.hi[r] = wc + wh + pad;
+    }
+}
+__device__ __forceinline__ void local_box(const DevPose& P, Box<double>& b)
+{
+    double c[3], h[3];
+    for (int k = 0; k < 3; k++) {
+        c[k] = 0.5 * b.lo[k] + 0.5 * b.hi[k];
+        h[k] = 0.5 * b.hi[k] - 0.5 * b.lo[k];
+    }
+    const double rel = 0x1p-48 + P.inv_eta;
+    for (int r = 0; r < 3; r++) {
+        double wc = P.bi64[r], wh = 0.0, mag = P.padmi64[r];
+        for (int k = 0; k < 3; k++) {
+            double a = P.Ri64[3 * r + k];
+            wc = fma(a, c[k], wc);
+            wh = fma(fabs(a), h[k], wh);
+            mag = fma(fabs(a), fabs(c[k]) + h[k], mag);
+        }
+        double pad = fma(rel, mag, 0x1p-300);
+        b.lo[r] = wc - wh - pad;
+        b.hi[r] = wc + wh + pad;
+    }
+}
+
 template <bool F64>
 struct Prec;
 template <>
@@ -674,6 +720,45 @@ __device__ __forceinline__ void load_tri(const MeshDev& M, const DevPose& P, uin
     *tri_id = t.w;
 }
 
+// Maps the four child boxes (world frame) into the local frame of pose P.
+template <class S>
+__device__ __forceinline__ void local_kids(const DevPose& P, Kids<S>& k)
+{
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        Box<S> b;
+        b.lo[0] = k.lx[i];
+        b.lo[1] = k.ly[i];
+        b.lo[2] = k.lz[i];
+        b.hi[0] = k.hx[i];
+        b.hi[1] = k.hy[i];
+        b.hi[2] = k.hz[i];
+        local_box(P, b);
+        k.lx[i] = b.lo[0];
+        k.ly[i] = b.lo[1];
+        k.lz[i] = b.lo[2];
+        k.hx[i] = b.hi[0];
+        k.hy[i] = b.hi[1];
+        k.hz[i] = b.hi[2];
+    }
+}
+
+// 16-bit mask of the overlapping child pairs (bit 4i+j: a's child i, b's child j).
+template <class S>
+__device__ __forceinline__ unsigned overlap_mask(const Kids<S>& a, const Kids<S>& b)
+{
+    unsigned m = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const bool ov = (a.lx[i] <= b.hx[j]) & (b.lx[j] <= a.hx[i]) & (a.ly[i] <= b.hy[j]) &
+                            (b.ly[j] <= a.hy[i]) & (a.lz[i] <= b.hz[j]) & (b.lz[j] <= a.hz[i]);
+            m |= (ov ? 1u : 0u) << (4 * i + j);
+        }
+    return m;
+}
+
 // Bit i of `x` (i < 4) spread over nibble i: the child pairs (i, *).
 __device__ __forceinline__ unsigned rows4(unsigned x)
 {
@@ -699,8 +784,21 @@ __device__ __forceinline__ void expand_pair(const Bufs& B, const uint4& ent, uns
     load_kids(J.A, ent.y, a);
     load_kids(J.B, ent.z, b);
     if (!J.pa.identity) world_kids(J.pa, a);
+    // a posed B can also be tested in its own frame (A's world boxes mapped
+    // back through B's pose against B's stored boxes): the world box of a
+    // rotated box is wider than the box, and each test alone is conservative.
+    // It removes about a quarter of the pairs for about a third more work per
+    // pair, which pays where the traversal is bound by work (batches), not by
+    // the latency of its levels (one pair).
+    unsigned m = 0xFFFFu;
+    if (B.two_frame && J.pb.inv_ok) {
+        Kids<S> al = a;
+        local_kids(J.pb, al);
+        m = overlap_mask(al, b);
+    }
     if (!J.pb.identity) world_kids(J.pb, b);
-    unsigned m = 0, va = 0, vb = 0, la = 0, lb = 0;
+    m &= overlap_mask(a, b);
+    unsigned va = 0, vb = 0, la = 0, lb = 0;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         ca[i] = a.c[i];
@@ -709,12 +807,6 @@ __device__ __forceinline__ void expand_pair(const Bufs& B, const uint4& ent, uns
         vb |= (b.c[i] != kEmpty ? 1u : 0u) << i;
         la |= ((a.c[i] & kLeaf) && a.c[i] != kEmpty ? 1u : 0u) << i;
         lb |= ((b.c[i] & kLeaf) && b.c[i] != kEmpty ? 1u : 0u) << i;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const bool ov = (a.lx[i] <= b.hx[j]) & (b.lx[j] <= a.hx[i]) & (a.ly[i] <= b.hy[j]) &
-                            (b.ly[j] <= a.hy[i]) & (a.lz[i] <= b.hz[j]) & (b.lz[j] <= a.hz[i]);
-            m |= (ov ? 1u : 0u) << (4 * i + j);
-        }
     }
     m &= rows4(va) & (vb * 0x1111u);
     const unsigned leafpair = rows4(la) & (lb * 0x1111u);
