@@ -84,6 +84,7 @@ extern "C" gi_status gi_create(const gi_options* opts, gi_ctx** out)
     c->device = opts ? opts->device : 0;
     c->budget = opts ? opts->hbm_budget_bytes : 0;
     c->flags = opts ? opts->flags : 0;
+    if (c->flags & GI_FLAG_FIXED_SHAPE) c->fixed_shape = (int)((c->flags >> 9) & 3u);
     if (c->device < 0 || c->device >= ndev) {
         delete c;
         return GI_ERR_INVALID_ARG;
@@ -507,6 +508,8 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
     // the result will be small (the kernel refuses, and this loop reruns on the
     // radix path, if it is not)
     bool small_order = ba + bb + bj <= 63 && c->pred_pairs <= kOrderSmallMax - kOrderSmallMax / 4;
+    const uint32_t tune_key = TravTuner::key(prec, nj, sumT);
+    const int shape = c->fixed_shape >= 0 ? c->fixed_shape : c->tuner.pick(tune_key);
     for (;;) {
         CK(c, grow(c->queue, c->cap_front, need_front, c->pool, c->st), "node queue");
         if (c->cap_qflag < c->cap_front) {
@@ -570,7 +573,7 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         b.two_frame = nj > 1 ? 1 : 0;
         CK(c, cudaMemsetAsync(c->d_cnt, 0, sizeof(Counters), c->st), "counters");
         CK(c, cudaEventRecord(c->ev[0], c->st), "event");
-        CK(c, launch_traverse(b, c->cfg, prec, c->st), "traverse");
+        CK(c, launch_traverse(b, c->cfg, prec, trav_shape(shape), c->st), "traverse");
         CK(c, cudaEventRecord(c->ev[1], c->st), "event");
         CK(c, launch_exact(b, c->cfg, c->st), "exact stage");
         CK(c, cudaEventRecord(c->ev[2], c->st), "event");
@@ -664,6 +667,7 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
     cudaEventElapsedTime(&ms_seg, c->ev[2], c->ev[3]);
     cudaEventElapsedTime(&ms_sort, c->ev[3], c->ev[4]);
     cudaEventElapsedTime(&ms_total, c->ev[0], c->ev[4]);
+    if (c->fixed_shape < 0) c->tuner.report(tune_key, shape, ms_trav);
     // split per job (sorted by job first)
     std::vector<uint32_t> job_start(nj + 1, 0);
     if (nj == 1) {
@@ -722,6 +726,7 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         s2.levels = H.levels;
         s2.retries = (uint32_t)retries;
         s2.launches = (uint32_t)(launch_count() - launches0);
+        s2.traverse_shape = (uint32_t)shape;
         s2.ms_traverse = ms_trav;
         s2.ms_exact = ms_exact;
         s2.ms_segments = ms_seg;

@@ -2,6 +2,7 @@
 // (shared by the translation units that implement the C ABI).
 #pragma once
 #include <atomic>
+#include <map>
 #include <memory>
 #include <cstdio>
 #include <mutex>
@@ -110,6 +111,53 @@ struct gi_result {
     gi_stats stats;
 };
 
+// Traversal autotuner: per workload class (precision, number of jobs, total
+// triangles), each traversal shape is timed on the context's own calls (the
+// best of kTries traversals, CUDA events on the context's stream); after that
+// the fastest shape is used.  Every shape gives the same result.
+struct TravTuner {
+    static constexpr int kTries = 2;
+    struct Entry {
+        float best[gi::kTravShapes];
+        int tries[gi::kTravShapes];
+        int choice = -1;
+        Entry()
+        {
+            for (int k = 0; k < gi::kTravShapes; k++) {
+                best[k] = 3.0e38f;
+                tries[k] = 0;
+            }
+        }
+    };
+    std::map<uint32_t, Entry> table;
+    static uint32_t key(int precision, uint32_t njobs, uint64_t tris)
+    {
+        const uint32_t jc = njobs <= 1 ? 0u : njobs < 16 ? 1u : njobs < 256 ? 2u : 3u;
+        uint32_t lg = 0;
+        while (lg < 40 && (2ull << lg) <= tris) lg++;
+        return (uint32_t)(precision & 1) | (jc << 1) | (lg << 3);
+    }
+    int pick(uint32_t k)
+    {
+        Entry& e = table[k];
+        if (e.choice >= 0) return e.choice;
+        for (int s = 0; s < gi::kTravShapes; s++)
+            if (e.tries[s] < kTries) return s;
+        int b = 0;
+        for (int s = 1; s < gi::kTravShapes; s++)
+            if (e.best[s] < e.best[b]) b = s;
+        e.choice = b;
+        return b;
+    }
+    void report(uint32_t k, int s, float ms)
+    {
+        Entry& e = table[k];
+        if (e.choice >= 0 || s < 0 || s >= gi::kTravShapes) return;
+        e.tries[s]++;
+        if (ms < e.best[s]) e.best[s] = ms;
+    }
+};
+
 struct gi_ctx {
     int device = 0;
     cudaStream_t st = nullptr;
@@ -151,6 +199,8 @@ struct gi_ctx {
     size_t order_scratch_bytes = 0;
     // pinned blocks the results are copied into
     std::shared_ptr<PinnedPool> pinned = std::make_shared<PinnedPool>();
+    TravTuner tuner;
+    int fixed_shape = -1;  // >= 0: traversal shape forced (tests), else tuned
     cudaEvent_t ev[8] = {};
 };
 

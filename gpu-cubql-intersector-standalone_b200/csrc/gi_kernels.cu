@@ -815,6 +815,123 @@ __device__ __forceinline__ void expand_pair(const Bufs& B, const uint4& ent, uns
 }
 
 // ---------------------------------------------------------------------------
+// Quad-cooperative expansion: the four lanes of a quad share one node pair and
+// lane k (= lane & 3) owns child k of both nodes.  Each lane loads one child
+// slot of each node (the four lanes of a quad read one 16-byte segment per
+// field of the structure-of-arrays node), maps its own boxes to the world
+// frame, receives B's four child boxes from its quad by width-4 shuffles and
+// tests its A child against them: four tests instead of sixteen, one box
+// transform instead of four, so the dependent chain of one expansion is a
+// fraction of the one-lane form's.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void load_kid(const MeshDev& M, uint32_t ref, unsigned k, Box<float>& b, uint32_t& c)
+{
+    if (ref & kLeaf) {
+        if (k == 0u) {
+            const float* lb = M.leafBox + 6 * (size_t)(ref & ~kLeaf);
+            for (int q = 0; q < 3; q++) {
+                b.lo[q] = __ldg(lb + q);
+                b.hi[q] = __ldg(lb + 3 + q);
+            }
+            c = ref;
+        } else {
+            for (int q = 0; q < 3; q++) b.lo[q] = b.hi[q] = 0.0f;
+            c = kEmpty;
+        }
+        return;
+    }
+    const float* p = reinterpret_cast<const float*>(M.nodes + ref);
+    for (int q = 0; q < 3; q++) {
+        b.lo[q] = __ldg(p + 4 * q + k);
+        b.hi[q] = __ldg(p + 12 + 4 * q + k);
+    }
+    c = __ldg(reinterpret_cast<const uint32_t*>(p + 24) + k);
+}
+__device__ __forceinline__ void load_kid(const MeshDev& M, uint32_t ref, unsigned k, Box<double>& b, uint32_t& c)
+{
+    if (ref & kLeaf) {
+        if (k == 0u) {
+            const double* lb = M.leafBox64 + 6 * (size_t)(ref & ~kLeaf);
+            for (int q = 0; q < 3; q++) {
+                b.lo[q] = __ldg(lb + q);
+                b.hi[q] = __ldg(lb + 3 + q);
+            }
+            c = ref;
+        } else {
+            for (int q = 0; q < 3; q++) b.lo[q] = b.hi[q] = 0.0;
+            c = kEmpty;
+        }
+        return;
+    }
+    const double* p = reinterpret_cast<const double*>(M.nodes64 + ref);
+    for (int q = 0; q < 3; q++) {
+        b.lo[q] = __ldg(p + 4 * q + k);
+        b.hi[q] = __ldg(p + 12 + 4 * q + k);
+    }
+    c = __ldg(reinterpret_cast<const uint32_t*>(p + 24) + k);
+}
+
+template <class S>
+__device__ __forceinline__ void shfl_box(const Box<S>& src, Box<S>& dst, unsigned j)
+{
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        dst.lo[q] = __shfl_sync(0xffffffffu, src.lo[q], (int)j, 4);
+        dst.hi[q] = __shfl_sync(0xffffffffu, src.hi[q], (int)j, 4);
+    }
+}
+
+// Called by all 32 lanes (the shuffles need them); lanes of a quad without a
+// node pair pass have = false and get no children.  fm / cm: bit j set when
+// (own A child, B child j) overlap and lead to a node pair / a leaf pair;
+// cb[j] receives B's child refs.
+template <bool F64>
+__device__ __forceinline__ void expand_quad(const Bufs& B, const uint4& ent, bool have, unsigned sub, unsigned& fm,
+                                            unsigned& cm, uint32_t& ca, uint32_t (&cb)[4])
+{
+    using S = typename Prec<F64>::S;
+    const JobDev& J = B.jobs[have ? ent.x : 0u];
+    Box<S> a, b;
+    uint32_t mb = kEmpty;
+    ca = kEmpty;
+    for (int q = 0; q < 3; q++) a.lo[q] = a.hi[q] = b.lo[q] = b.hi[q] = S(0);
+    if (have) {
+        load_kid(J.A, ent.y, sub, a, ca);
+        load_kid(J.B, ent.z, sub, b, mb);
+        if (ca != kEmpty && !J.pa.identity) world_box(J.pa, a);
+    }
+    // optional second test in B's own frame (see expand_pair)
+    unsigned m2 = 0xFu;
+    if (B.two_frame) {  // uniform over the launch
+        const bool twof = have && J.pb.inv_ok;
+        Box<S> al = a;
+        if (twof && ca != kEmpty) local_box(J.pb, al);
+        m2 = 0u;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            Box<S> bl;
+            shfl_box(b, bl, (unsigned)j);
+            if (!twof || overlap(al, bl)) m2 |= 1u << j;
+        }
+    }
+    if (have && mb != kEmpty && !J.pb.identity) world_box(J.pb, b);
+    fm = cm = 0u;
+    const bool leafa = (ca & kLeaf) && ca != kEmpty;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        Box<S> bj;
+        shfl_box(b, bj, (unsigned)j);
+        cb[j] = __shfl_sync(0xffffffffu, mb, j, 4);
+        const bool ov = ca != kEmpty && cb[j] != kEmpty && ((m2 >> j) & 1u) && overlap(a, bj);
+        const bool leafb = (cb[j] & kLeaf) != 0u;
+        if (ov) {
+            if (leafa && leafb) cm |= 1u << j;
+            else fm |= 1u << j;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Persistent BVH4 x BVH4 traversal: a small warp stack in front of a device
 // work queue (no grid barrier).
 //
@@ -837,13 +954,15 @@ __device__ __forceinline__ void expand_pair(const Bufs& B, const uint4& ent, uns
 //
 // Termination: `work` is the number of node pairs that exist.  Seeds add to it
 // before the seed count completes; an expansion adds (children - expanded
-// pairs) in one atomic, issued before any child is published, so the count
-// never passes through zero while a node pair exists.  Reading seed_done ==
-// all seed tests and then work == 0 proves the traversal is over.  Every wait
-// is bounded; overflow or a spent wait raises the abort flag.
+// pairs) in one atomic, issued after its candidate slots are reserved and
+// before any child is published, so the count never passes through zero
+// while a node pair exists, and once it is zero the candidate count is final.
+// Reading seed_done == all seed tests and then work == 0 proves the traversal
+// is over.  Every wait is bounded; overflow or a spent wait raises the abort
+// flag.
 // ---------------------------------------------------------------------------
 constexpr unsigned kIdleSpins = 1u << 22;     // consecutive idle polls of one warp (~1 s)
-constexpr unsigned kWarpStack = 32;           // node pairs a warp keeps for its next iteration
+constexpr unsigned kWarpStack = 32;           // stack capacity of a warp (both expansion forms)
 constexpr int kTravThreads = 256;
 constexpr int kTravWarps = kTravThreads / 32;
 
@@ -975,9 +1094,15 @@ __device__ __forceinline__ void filter_candidates(const Bufs& B, bool have, cons
     }
 }
 
-template <bool F64>
+// QUAD selects the expansion form: one node pair per lane (32 per warp
+// iteration, the form for work-bound launches) or one per quad (8 per
+// iteration with a quarter of the dependent chain, the form for launches bound
+// by the latency of the traversal's levels).  The host picks it per workload.
+template <bool F64, bool QUAD>
 __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
 {
+    constexpr unsigned kSlots = QUAD ? 8u : 32u;  // node-queue slots per ticket: one per work unit
+    constexpr unsigned kStack = QUAD ? 8u : 32u;  // node pairs kept for the next iteration
     __shared__ uint4 stk[kTravWarps][kWarpStack];
     Counters* C = B.cnt;
     const unsigned lane = threadIdx.x & 31;
@@ -995,13 +1120,18 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
     for (;;) {
         ++iter;
         if (!ticket && sn == 0u) {
-            nbase = take_ticket(&C->q_head);
-            npend = 0xffffffffu;
+            unsigned b0 = 0;
+            if (lane == 0) b0 = atomicAdd(&C->q_head, kSlots);
+            nbase = __shfl_sync(0xffffffffu, b0, 0);
+            npend = kSlots == 32u ? 0xffffffffu : (1u << kSlots) - 1u;
             ticket = true;
         }
-        const unsigned ns = nbase + lane;
-        const unsigned i = cbase + lane;
-        const bool nslot = ticket && ((npend >> lane) & 1u) && ns < B.cap_queue;
+        const unsigned unit = QUAD ? (lane >> 2) : lane;  // work unit: a quad or a lane
+        const unsigned sub = QUAD ? (lane & 3u) : 0u;
+        const unsigned ubit = QUAD ? 4u * unit : unit;     // the unit's first lane
+        const unsigned ns = nbase + unit;  // one queue slot per unit
+        const unsigned i = cbase + lane;   // one candidate slot per lane
+        const bool nslot = ticket && ((npend >> unit) & 1u) && ns < B.cap_queue;
         const bool cslot = ((cpend >> lane) & 1u) && i < B.cap_cand;
         // everything this pass polls, issued together.  The abort flag is one
         // line that every warp reads, so it is read every 8th pass only; its
@@ -1010,15 +1140,15 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
         if (lane == 0 && (iter & 7u) == 0u) ab = ld_vol(&C->abort_);
         const unsigned ntag = nslot ? ld_vol(B.qflag + ns) : 0u;
         const unsigned ctag = cslot ? ld_vol(B.cflag + i) : 0u;
-        const bool from_queue = nslot && ntag == B.tag;
-        const unsigned qmask = __ballot_sync(0xffffffffu, from_queue);
-        if (sn != 0u || qmask != 0u) {
+        const bool from_queue = nslot && ntag == B.tag;  // the same in every lane of a unit
+        const unsigned qball = __ballot_sync(0xffffffffu, from_queue && sub == 0u);  // a unit's first lane: ready
+        if (sn != 0u || qball != 0u) {
             idle = 0;
             backoff = 32;
             // ready queue slots first (queued work is what idle warps wait
-            // for), the other lanes pop the stack
-            const unsigned take = min(sn, 32u - (unsigned)__popc(qmask));
-            const unsigned rank = (unsigned)__popc(~qmask & ((1u << lane) - 1u));
+            // for), the other units pop the stack
+            const unsigned take = min(sn, kSlots - (unsigned)__popc(qball));
+            const unsigned rank = unit - (unsigned)__popc(qball & ((1u << ubit) - 1u));
             const bool from_stack = !from_queue && rank < take;
             uint4 ent = make_uint4(0u, kEmpty, kEmpty, 0u);
             if (from_stack) {
@@ -1030,12 +1160,16 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
             sn -= take;
             __syncwarp();  // popped entries are read before the pushes below reuse their slots
             const bool have = from_stack || from_queue;
-            unsigned fm = 0, cm = 0;
-            uint32_t ca[4], cb[4];
-            if (have) {
+            if (have && sub == 0u) {
                 visited++;
                 maxlev = max(maxlev, ent.w);
-                expand_pair<F64>(B, ent, fm, cm, ca, cb);
+            }
+            unsigned fm = 0, cm = 0;
+            uint32_t ca[4], cb[4];
+            if constexpr (QUAD) {
+                expand_quad<F64>(B, ent, have, sub, fm, cm, ca[0], cb);
+            } else {
+                if (have) expand_pair<F64>(B, ent, fm, cm, ca, cb);
             }
             // children: node pairs onto the stack (up to keep), the rest to the
             // queue; candidates to the global candidate list
@@ -1052,14 +1186,18 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
             }
             const unsigned kf = __shfl_sync(0xffffffffu, incf, 31);
             const unsigned kc = __shfl_sync(0xffffffffu, incc, 31);
-            const unsigned done = __popc(__ballot_sync(0xffffffffu, have));
-            const unsigned keep = min(kf, kWarpStack - sn);
+            const unsigned done = __popc(__ballot_sync(0xffffffffu, have && sub == 0u));
+            const unsigned keep = min(kf, kStack - sn);
             unsigned qb = 0, cg = 0;
             if (lane == 31) {
-                // node pairs made minus expanded, before any child is published
-                if (kf != done) atomicAdd(&C->work, kf - done);
-                if (kf > keep) qb = atomicAdd(&C->q_tail, kf - keep);
                 if (kc) cg = atomicAdd(&C->cand, kc);
+                if (kf > keep) qb = atomicAdd(&C->q_tail, kf - keep);
+                // then node pairs made minus expanded, before any child is
+                // published: work reaches zero only after the candidate slots
+                // of the last expansion are reserved, so a warp that sees
+                // work == 0 reads the final candidate count
+                fence_acq_rel();
+                if (kf != done) atomicAdd(&C->work, kf - done);
             }
             qb = __shfl_sync(0xffffffffu, qb, 31);
             cg = __shfl_sync(0xffffffffu, cg, 31);
@@ -1069,7 +1207,7 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
                 unsigned g = f0, h = c0;
                 for (unsigned mm = fm | cm; mm != 0u; mm &= mm - 1u) {
                     const unsigned q = (unsigned)__ffs(mm) - 1u;
-                    const uint32_t ra = sel4(ca, q >> 2), rb = sel4(cb, q & 3u);
+                    const uint32_t ra = QUAD ? ca[0] : sel4(ca, q >> 2), rb = sel4(cb, QUAD ? q : (q & 3u));
                     if ((fm >> q) & 1u) {
                         const uint4 e = make_uint4(ent.x, ra, rb, ent.w + 1u);
                         if (g < keep) {
@@ -1110,7 +1248,13 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
             __syncwarp();  // stack pushes visible to the whole warp
             sn += keep;
             if (ticket) {
-                npend &= ~qmask;
+                unsigned qm = qball;
+                if constexpr (QUAD) {
+                    qm = 0;
+#pragma unroll
+                    for (int q = 0; q < 8; q++) qm |= ((qball >> (4 * q)) & 1u) << q;
+                }
+                npend &= ~qm;
                 if (npend == 0u) ticket = false;
             }
             if (__any_sync(0xffffffffu, ab != 0u)) break;
@@ -1146,6 +1290,7 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
                 const unsigned sd = ld_vol(&C->seed_done);
                 fence_acq_rel();
                 const unsigned w = ld_vol(&C->work);
+                fence_acq_rel();
                 over = sd == seed_total && w == 0u;
                 ncand = min(ld_vol(&C->cand), B.cap_cand);
             }
@@ -1751,23 +1896,32 @@ cudaError_t query_launch(int device, LaunchCfg* cfg)
     cudaDeviceProp prop;
     GI_TRY(cudaGetDeviceProperties(&prop, device));
     cfg->sms = prop.multiProcessorCount;
-    int b32 = 0, b64 = 0;
-    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b32, k_traverse<false>, 256, 0));
-    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b64, k_traverse<true>, 256, 0));
-    cfg->trav_blocks = (b32 < 1 ? 1 : b32) * cfg->sms;
-    cfg->trav_blocks64 = (b64 < 1 ? 1 : b64) * cfg->sms;
-    cfg->trav_threads = 256;
+    int n[2][2] = {};
+    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n[0][0], k_traverse<false, false>, kTravThreads, 0));
+    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n[0][1], k_traverse<false, true>, kTravThreads, 0));
+    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n[1][0], k_traverse<true, false>, kTravThreads, 0));
+    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n[1][1], k_traverse<true, true>, kTravThreads, 0));
+    for (int a = 0; a < 2; a++)
+        for (int q = 0; q < 2; q++) cfg->trav_per_sm[a][q] = n[a][q] < 1 ? 1 : n[a][q];
+    cfg->trav_threads = kTravThreads;
     return cudaSuccess;
 }
 
 // The persistent traversal needs no co-residency (nothing waits on a block
-// that has not started); the grid is the resident block count so that every
-// warp is live from the start.
-cudaError_t launch_traverse(const Bufs& b, const LaunchCfg& cfg, int precision, cudaStream_t st)
+// that has not started); the grid is at most the resident block count so
+// that every warp is live from the start.
+cudaError_t launch_traverse(const Bufs& b, const LaunchCfg& cfg, int precision, TravShape shape, cudaStream_t st)
 {
     note_launches(1);
-    if (precision == 1) k_traverse<true><<<cfg.trav_blocks64, kTravThreads, 0, st>>>(b);
-    else k_traverse<false><<<cfg.trav_blocks, kTravThreads, 0, st>>>(b);
+    const int f64 = precision == 1 ? 1 : 0, q = shape.quad ? 1 : 0;
+    const int grid = (shape.one_per_sm ? 1 : cfg.trav_per_sm[f64][q]) * cfg.sms;
+    if (f64) {
+        if (q) k_traverse<true, true><<<grid, kTravThreads, 0, st>>>(b);
+        else k_traverse<true, false><<<grid, kTravThreads, 0, st>>>(b);
+    } else {
+        if (q) k_traverse<false, true><<<grid, kTravThreads, 0, st>>>(b);
+        else k_traverse<false, false><<<grid, kTravThreads, 0, st>>>(b);
+    }
     return cudaGetLastError();
 }
 

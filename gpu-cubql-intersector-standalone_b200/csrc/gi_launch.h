@@ -45,14 +45,28 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaMemPool_t pool, cudaStream_
 // Intersect launch configuration.
 struct LaunchCfg {
     int sms = 0;
-    int trav_blocks = 0;    // co-resident blocks for the cooperative traversal (FP32 boxes)
-    int trav_blocks64 = 0;  // the same for FP64 boxes
+    int trav_per_sm[2][2] = {};  // resident traversal blocks per SM, [FP64][quad form]
     int trav_threads = 256;
 };
+
+// Traversal shapes the tuner chooses from: expansion form (one node pair per
+// lane or per quad) x blocks per SM (all resident, or one).
+struct TravShape {
+    bool quad = false;
+    bool one_per_sm = false;
+};
+constexpr int kTravShapes = 4;
+inline TravShape trav_shape(int k)
+{
+    TravShape t;
+    t.quad = (k & 2) != 0;
+    t.one_per_sm = (k & 1) != 0;
+    return t;
+}
 cudaError_t query_launch(int device, LaunchCfg* cfg);
 
 // Traversal + first filter stage (persistent, work queue), then the exact stage.
-cudaError_t launch_traverse(const Bufs& b, const LaunchCfg& cfg, int precision, cudaStream_t st);
+cudaError_t launch_traverse(const Bufs& b, const LaunchCfg& cfg, int precision, TravShape shape, cudaStream_t st);
 cudaError_t launch_exact(const Bufs& b, const LaunchCfg& cfg, cudaStream_t st);
 // Segments of every result (count from the device counters):
 // segs[18*i ..] (up to 3 segments), nseg[i].

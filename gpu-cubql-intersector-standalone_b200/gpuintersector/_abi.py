@@ -16,6 +16,12 @@ GI_ERR_NOT_READY = 7
 GI_ERR_NO_DEVICE = 8
 
 GI_FLAG_TINY_BUFFERS = 1
+GI_FLAG_FIXED_SHAPE = 0x100
+
+
+def GI_FLAG_SHAPE(k):
+    return (int(k) & 3) << 9
+
 
 GI_PREC_FP32_CASCADE = 0
 GI_PREC_FP64 = 1
@@ -53,7 +59,7 @@ class Stats(ctypes.Structure):
                 ("filter_decided", ctypes.c_uint64), ("escalated", ctypes.c_uint64),
                 ("exact_signs", ctypes.c_uint64), ("exact_points", ctypes.c_uint64), ("pairs", ctypes.c_uint64),
                 ("segments", ctypes.c_uint64), ("levels", ctypes.c_uint32), ("retries", ctypes.c_uint32),
-                ("launches", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("launches", ctypes.c_uint32), ("traverse_shape", ctypes.c_uint32),
                 ("ms_traverse", ctypes.c_double), ("ms_exact", ctypes.c_double), ("ms_segments", ctypes.c_double),
                 ("ms_sort", ctypes.c_double), ("ms_total", ctypes.c_double)]
 

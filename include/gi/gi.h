@@ -77,6 +77,12 @@ typedef struct gi_server gi_server;
 /* gi_options.flags */
 #define GI_FLAG_TINY_BUFFERS 1u /* start every intersect buffer at 64 entries: exercises the
                                    capacity-overflow / retry path (host-side fault injection) */
+/* The traversal shape (expansion form x blocks per SM) is autotuned per workload
+ * class on the context's own calls.  GI_FLAG_FIXED_SHAPE | GI_FLAG_SHAPE(k),
+ * k in 0..3 (bit 1: one node pair per quad of lanes, bit 0: one block per SM),
+ * fixes it instead (every shape gives the same results). */
+#define GI_FLAG_FIXED_SHAPE 0x100u
+#define GI_FLAG_SHAPE(k) ((((uint32_t)(k)) & 3u) << 9)
 
 typedef struct {
     int32_t device;             /* CUDA device ordinal */
@@ -119,7 +125,7 @@ typedef struct {
     uint32_t levels;                  /* traversal levels */
     uint32_t retries;                 /* capacity retries */
     uint32_t launches;                /* kernels launched by this call */
-    uint32_t reserved;
+    uint32_t traverse_shape;          /* traversal shape used: bit 1 quad form, bit 0 one block per SM */
     double ms_traverse;               /* device time: traversal + first filter */
     double ms_exact;                  /* device time: FP64 / exact stage */
     double ms_segments;               /* device time: segment construction */

@@ -169,6 +169,27 @@ def test_ordering_paths_and_redo(gi, oc):
         B.release()
 
 
+@pytest.mark.parametrize("shape", [0, 1, 2, 3])
+def test_every_traversal_shape(gi, oc, shape):
+    """Each traversal shape the autotuner may pick (expansion per lane or per
+    quad, all resident blocks or one per SM) gives the oracle's pairs and
+    segments, in both precision forms and in a batch."""
+    from gpuintersector import meshgen as mg
+
+    flags = gi._abi.GI_FLAG_FIXED_SHAPE | gi._abi.GI_FLAG_SHAPE(shape)
+    cfg = mg.config1(seed=30 + shape)
+    with gi.Context(0, flags=flags) as c:
+        for prec in (0, 1):
+            r, ref = run_cfg(c, gi, oc, cfg, precision=prec)
+            assert_same(r, ref)
+            assert r.stats["traverse_shape"] == shape
+        A, B = c.upload(cfg["vA"], cfg["tA"]), c.upload(cfg["vB"], cfg["tB"])
+        rs = c.intersect_batch([(A, None, B, gi_pose(gi, cfg["poseB"])), (B, None, A, None)])
+        assert_same(rs[0], ref)
+        A.release()
+        B.release()
+
+
 def test_fp64_form_identical(ctx, gi, oc):
     from gpuintersector import meshgen as mg
 
