@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--level", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--shape", type=int, default=-1,
+                    help="pin the traversal shape (0..3) instead of autotuning it (for profiling runs)")
     return ap.parse_args()
 
 
@@ -218,7 +220,8 @@ def main():
 
     cfg, rng = workload(args.level)
     poses = step_poses(cfg, rng, args.warmup + args.steps)
-    ctx = gi.Context(local)
+    flags = 0 if args.shape < 0 else (gi._abi.GI_FLAG_FIXED_SHAPE | gi._abi.GI_FLAG_SHAPE(args.shape))
+    ctx = gi.Context(local, flags=flags)
     A = ctx.upload(cfg["vA"], cfg["tA"])
     B = ctx.upload(cfg["vB"], cfg["tB"])
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -230,7 +233,7 @@ def main():
     # autotuning: the library times each traversal shape (expansion form x
     # blocks per SM) twice per workload class on its own calls, then keeps the
     # fastest; these calls precede the warm-up and are not timed
-    for k in range(8):
+    for k in range(8 if args.shape < 0 else 0):
         one(poses[0])
         one(poses[0], precision=1)
     for k in range(args.warmup):
@@ -323,7 +326,7 @@ def main():
             args.level, int(cfg["tA"].shape[0])), "tris_per_mesh": int(cfg["tA"].shape[0]),
             "parallelism": "replicas" if world > 1 else "single", "l2": "flushed (256 MB write) before each step",
             "precision": "fp32 filter -> fp64 filter -> exact", "segments": True,
-            "traverse_shape": int(st["traverse_shape"]), "autotuned": True},
+            "traverse_shape": int(st["traverse_shape"]), "autotuned": args.shape < 0},
         "pairs": int(st["pairs"]), "segments": int(st["segments"]), "candidates": int(cand),
         "tri_pair_tests_per_s": tests_per_s,
         "filter_decided_frac": float(st["filter_decided"] / max(1, st["candidates"])),
