@@ -112,9 +112,11 @@ struct gi_result {
 };
 
 // Traversal autotuner: per workload class (precision, number of jobs, total
-// triangles), each traversal shape is timed on the context's own calls (the
-// best of kTries traversals, CUDA events on the context's stream); after that
-// the fastest shape is used.  Every shape gives the same result.
+// triangles in factors of 4), each traversal shape is timed on the context's
+// own calls (the best of kTries traversals, CUDA events on the context's
+// stream); a shape whose first time is over 1.3x the best so far is not tried
+// again.  After that the fastest shape is used.  Every shape gives the same
+// result.
 struct TravTuner {
     static constexpr int kTries = 2;
     struct Entry {
@@ -134,7 +136,7 @@ struct TravTuner {
     {
         const uint32_t jc = njobs <= 1 ? 0u : njobs < 16 ? 1u : njobs < 256 ? 2u : 3u;
         uint32_t lg = 0;
-        while (lg < 40 && (2ull << lg) <= tris) lg++;
+        while (lg < 20 && (4ull << (2 * lg)) <= tris) lg++;
         return (uint32_t)(precision & 1) | (jc << 1) | (lg << 3);
     }
     int pick(uint32_t k)
@@ -155,6 +157,10 @@ struct TravTuner {
         if (e.choice >= 0 || s < 0 || s >= gi::kTravShapes) return;
         e.tries[s]++;
         if (ms < e.best[s]) e.best[s] = ms;
+        float lead = 3.0e38f;
+        for (int q = 0; q < gi::kTravShapes; q++)
+            if (q != s && e.tries[q] > 0) lead = lead < e.best[q] ? lead : e.best[q];
+        if (e.tries[s] == 1 && ms > 1.3f * lead) e.tries[s] = kTries;  // clearly slower: one try is enough
     }
 };
 

@@ -74,31 +74,39 @@ def icosphere(level):
 
 
 def geodesic_sphere(n):
-    """Class-I geodesic sphere of frequency n (each icosahedron face split into n^2 triangles)."""
+    """Class-I geodesic sphere of frequency n: each icosahedron face split into
+    n^2 triangles, points projected to the unit sphere; 20 n^2 triangles,
+    10 n^2 + 2 vertices.  Vectorised: a grid point is sum(w_k * corner_k) / n
+    with the corners taken in increasing index order, so a point shared by two
+    faces is computed bit-identically from both and exact duplicates merge."""
+    n = int(n)
     v0, f0 = _icosahedron()
-    pts = {}
-    verts = []
-    tris = []
-
-    def vid(face, i, j):
-        a, b, c = f0[face]
-        wa, wb, wc = n - i - j, i, j
-        key = tuple(sorted([(int(a), wa), (int(b), wb), (int(c), wc)]))
-        key = tuple(x for x in key if x[1] > 0)
-        if key not in pts:
-            p = sum(v0[k] * w for k, w in key) / n
-            pts[key] = len(verts)
-            verts.append(p / np.linalg.norm(p))
-        return pts[key]
-
-    for face in range(20):
-        for i in range(n):
-            for j in range(n - i):
-                a, b, c = vid(face, i, j), vid(face, i + 1, j), vid(face, i, j + 1)
-                tris.append((a, b, c))
-                if i + j < n - 1:
-                    tris.append((b, vid(face, i + 1, j + 1), c))
-    return np.array(verts, dtype=np.float64), np.array(tris, dtype=np.uint32)
+    i, j = np.meshgrid(np.arange(n + 1), np.arange(n + 1), indexing="ij")
+    keep = (i + j) <= n
+    i, j = i[keep], j[keep]
+    npf = i.size
+    local = -np.ones((n + 1, n + 1), dtype=np.int64)
+    local[i, j] = np.arange(npf)
+    ids = np.repeat(f0[:, None, :], npf, axis=1)                         # (20, npf, 3) corner ids
+    w = np.stack([n - i - j, i, j], axis=-1)[None].repeat(20, axis=0)   # (20, npf, 3) weights
+    order = np.argsort(ids, axis=-1, kind="stable")
+    ids = np.take_along_axis(ids, order, -1)
+    w = np.take_along_axis(w, order, -1).astype(np.float64)
+    p = (w[..., 0:1] * v0[ids[..., 0]] + w[..., 1:2] * v0[ids[..., 1]]) + w[..., 2:3] * v0[ids[..., 2]]
+    p = p.reshape(-1, 3) / n
+    p /= np.linalg.norm(p, axis=1, keepdims=True)
+    verts, inv = np.unique(p, axis=0, return_inverse=True)
+    inv = inv.reshape(20, npf)
+    a_i, a_j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    up = (a_i + a_j) <= n - 1
+    ui, uj = a_i[up], a_j[up]
+    dn = (a_i + a_j) <= n - 2
+    di, dj = a_i[dn], a_j[dn]
+    t_up = np.stack([local[ui, uj], local[ui + 1, uj], local[ui, uj + 1]], axis=1)
+    t_dn = np.stack([local[di + 1, dj], local[di + 1, dj + 1], local[di, dj + 1]], axis=1)
+    tl = np.concatenate([t_up, t_dn])                                      # per-face local triangles
+    tris = (inv[:, tl]).reshape(-1, 3)
+    return verts.astype(np.float64), tris.astype(np.uint32)
 
 
 def displacement_params(rng, k=8):
@@ -185,27 +193,70 @@ def freq_for_tris(T):
     return max(2, int(round((T / 20.0) ** 0.5)))
 
 
-def config4(seed=4, pairs=4096, t_min=1000, t_max=200000, max_freq=None):
-    """Batched pairs; each mesh a displaced geodesic sphere, B posed with an offset
-    in [0.2, 1.5] * radius along a random direction and a random rotation."""
-    rng = np.random.default_rng(seed)
-    jobs = []
+def _freq_grid(t_min, t_max, steps=24):
+    """Geodesic frequencies on a geometric grid covering [t_min, t_max] triangles
+    (20 n^2 each): drawing T log-uniformly and taking the nearest grid frequency
+    keeps the distribution while only `steps` distinct spheres are built."""
+    f = np.unique(np.round(np.geomspace(freq_for_tris(t_min), freq_for_tris(t_max), steps)).astype(int))
+    return f
+
+
+def _draw_tris(rng, t_min, t_max):
+    return float(np.exp(rng.uniform(np.log(t_min), np.log(t_max))))
+
+
+def _sphere_of_size(rng, grid, T):
+    n = int(grid[np.argmin(np.abs(np.log(20.0 * grid.astype(float) ** 2) - np.log(T)))])
+    u, t = geodesic_cached(n)
+    return displace(u, displacement_params(rng)), t
+
+
+def config4_sizes(seed=4, pairs=4096, t_min=1000, t_max=200000):
+    """Triangle counts (drawn, before the frequency grid) of every pair's meshes,
+    without building them: the first two draws of each pair's own generator."""
+    out = []
     for p in range(pairs):
-        ms = []
-        for _ in range(2):
-            T = float(np.exp(rng.uniform(np.log(t_min), np.log(t_max))))
-            n = freq_for_tris(T)
-            if max_freq:
-                n = min(n, max_freq)
-            u, t = geodesic_cached(n)
-            ms.append((displace(u, displacement_params(rng)), t))
+        rng = np.random.default_rng([seed, p])
+        out.append((_draw_tris(rng, t_min, t_max), _draw_tris(rng, t_min, t_max)))
+    return out
+
+
+def config4_iter(seed=4, pairs=4096, t_min=1000, t_max=200000, which=None):
+    """Batched pairs, one at a time (pair p from its own seeded generator, so any
+    subset can be built alone): each mesh a displaced geodesic sphere with T
+    log-uniform in [t_min, t_max]; B posed with an offset of [0.2, 1.5] *
+    radius in a random direction and a random rotation."""
+    grid = _freq_grid(t_min, t_max)
+    for p in (range(pairs) if which is None else which):
+        rng = np.random.default_rng([seed, p])
+        TA, TB = _draw_tris(rng, t_min, t_max), _draw_tris(rng, t_min, t_max)
+        vA, tA = _sphere_of_size(rng, grid, TA)
+        vB, tB = _sphere_of_size(rng, grid, TB)
         d = rng.standard_normal(3)
         d /= np.linalg.norm(d)
         off = rng.uniform(0.2, 1.5) * d
         R = random_rotation(rng)
-        jobs.append(dict(vA=ms[0][0], tA=ms[0][1], vB=ms[1][0], tB=ms[1][1], poseA=None,
-                         poseB=(R, np.zeros(3), off)))
-    return jobs
+        yield dict(vA=vA, tA=tA, vB=vB, tB=tB, poseA=None, poseB=(R, np.zeros(3), off))
+
+
+def config4(seed=4, pairs=4096, t_min=1000, t_max=200000):
+    return list(config4_iter(seed, pairs, t_min, t_max))
+
+
+def config5(seed=5, pairs=64, t_min=10000, t_max=2000000):
+    """Serving set: mesh pairs of displaced geodesic spheres with T log-uniform
+    in [t_min, t_max]; B's base pose an offset of 0.3 along a random direction
+    plus a random rotation."""
+    rng = np.random.default_rng(seed)
+    grid = _freq_grid(t_min, t_max)
+    out = []
+    for p in range(pairs):
+        vA, tA = _sphere_of_size(rng, grid, _draw_tris(rng, t_min, t_max))
+        vB, tB = _sphere_of_size(rng, grid, _draw_tris(rng, t_min, t_max))
+        d = rng.standard_normal(3)
+        d /= np.linalg.norm(d)
+        out.append(dict(vA=vA, tA=tA, vB=vB, tB=tB, poseB=(random_rotation(rng), np.zeros(3), 0.3 * d)))
+    return out
 
 
 def pose_stream(rng, n, max_rot_deg=5.0, max_trans=0.05):
