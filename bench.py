@@ -39,6 +39,9 @@ PKG = os.path.join(ROOT, "gpu-cubql-intersector-standalone_b200")
 sys.path.insert(0, PKG)
 
 METRIC = "ms/intersect at 2×1.3M tris & tri-pair tests/s; pose-update p50/p99 vs FP64 path"
+# DRAM bytes of one k_traverse launch on the level-8 pose workload, from an ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum = 18.27 MB + 0.86 MB)
+TRAVERSE_DRAM_BYTES = 19.13e6
 
 
 def parse():
@@ -495,7 +498,10 @@ def main():
                 "samples_ms": [round(x, 3) for x in e2e_ms], "split": e2e_split},
         "gpu_launches": int(np.sum([s["launches"] for s in stats])),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "k_traverse", "peak_source": peak_src,
+                     "traffic": TRAVERSE_DRAM_BYTES if args.level == 8 else None,
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of "
+                                       "k_traverse on this workload (shape 1)",
+                     "kernel": "k_traverse", "peak_source": peak_src,
                      "alg_bytes_per_launch": float(alg_bytes),
                      "note": "output-sensitive traversal: bytes = node pairs x 2 nodes x 128 B + leaf pairs x "
                              "2 x (16 B record + 3 x 24 B vertices) + results x 16 B"},
