@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--level", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--workload", default="pose", choices=["pose", "batch", "serving"],
+    ap.add_argument("--workload", default="pose", choices=["pose", "batch", "serving", "ingest"],
                     help="pose: the headline pose-update stream on two 1.3M-triangle meshes; batch: many "
                          "mesh pairs of uneven size in one call; serving: resident pairs under an HBM "
                          "budget with a Poisson pose stream")
@@ -337,6 +337,60 @@ def run_serving(args, gi, world, rank, dist):
         _json(line)
 
 
+def run_ingest(args, gi, world, rank):
+    """Ingestion upstream of the path: two config-2 meshes (1,310,720 triangles
+    each) written as OFF text, then gi_off_load (host threads, mmap) and
+    gi_scene_load (both files parsed, copied, normalised on the device, both
+    BVHs built)."""
+    import tempfile
+
+    from gpuintersector import meshgen as mg
+
+    cfg = mg.config2(level=args.level)
+    tmp = tempfile.mkdtemp(prefix="gi_ingest_")
+    paths = []
+    for tag in ("A", "B"):
+        v, t = cfg["v" + tag], cfg["t" + tag]
+        path = os.path.join(tmp, tag + ".off")
+        with open(path, "w") as f:
+            f.write("OFF\n%d %d 0\n" % (v.shape[0], t.shape[0]))
+            np.savetxt(f, v, fmt="%.17g")
+            np.savetxt(f, np.column_stack([np.full(t.shape[0], 3), t]), fmt="%d")
+        paths.append(path)
+    nbytes = sum(os.path.getsize(p) for p in paths)
+    load_ms, scene_ms = [], []
+    ncores = os.cpu_count() or 1
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        for p in paths:
+            gi.load_off(p)
+        t1 = time.perf_counter()
+        with gi.Context(int(os.environ.get("LOCAL_RANK", "0"))) as ctx:
+            t2 = time.perf_counter()
+            A, B, sc, ra, rb = ctx.load_scene(paths[0], paths[1], scale_to_unit=True)
+            t3 = time.perf_counter()
+            A.release()
+            B.release()
+        if k >= args.warmup:
+            load_ms.append((t1 - t0) * 1e3)
+            scene_ms.append((t3 - t2) * 1e3)
+    tris = int(cfg["tA"].shape[0] + cfg["tB"].shape[0])
+    line = {
+        "metric": "OFF ingestion: ms to load both config-2 files; ms to load + normalise + build both meshes",
+        "value": float(np.median(scene_ms)), "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": float(np.median(scene_ms)), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (config-2 icospheres written as OFF text, %.1f MB)" % (nbytes / 1e6),
+        "config": {"workload": "2 OFF files, %d triangles" % tris, "host_threads": ncores},
+        "off_load_ms": float(np.median(load_ms)), "off_parse_MB_per_s": nbytes / 1e6 / (np.median(load_ms) * 1e-3),
+        "scene_load_ms": float(np.median(scene_ms)), "scene_tris_per_s": tris / (np.median(scene_ms) * 1e-3),
+    }
+    for p in paths:
+        os.remove(p)
+    os.rmdir(tmp)
+    if rank == 0:
+        _json(line)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -365,6 +419,9 @@ def main():
         if dist:
             dist.barrier()
             dist.destroy_process_group()
+        return
+    if args.workload == "ingest":
+        run_ingest(args, gi, world, rank)
         return
     if args.workload == "serving":
         run_serving(args, gi, world, rank, dist)

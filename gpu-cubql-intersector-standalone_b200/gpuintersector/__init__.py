@@ -16,6 +16,7 @@ If libgi.so is missing or no CUDA device is present the calls raise; nothing
 falls back to a CPU implementation.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -206,8 +207,43 @@ class Context:
                                                  ctypes.c_void_p(d_out_ptr))
         self.check(rc, "gi_classify_pairs_noalloc")
 
+    def load_scene(self, path_a, path_b, scale_to_unit=True):
+        """Both OFF files loaded, the scene normalised on the device and both meshes
+        built: (A, B, scene dict with the centres and scale, report A, report B)."""
+        ha, hb = ctypes.c_void_p(), ctypes.c_void_p()
+        sc = _abi.Scene()
+        ra, rb = _abi.OffReport(), _abi.OffReport()
+        self.check(self._lib.gi_scene_load(self.handle, os.fsencode(path_a), os.fsencode(path_b),
+                                           1 if scale_to_unit else 0, ctypes.byref(ha), ctypes.byref(hb),
+                                           ctypes.byref(sc), ctypes.byref(ra), ctypes.byref(rb)), "gi_scene_load")
+        return Mesh._wrap(self, ha), Mesh._wrap(self, hb), sc.as_dict(), ra.as_dict(), rb.as_dict()
+
     def server(self, max_inflight=256, want_segments=True, precision=GI_PREC_FP32_CASCADE):
         return Server(self, max_inflight, want_segments, precision)
+
+
+def load_off(path, nthreads=0):
+    """OFF file as the reference loads it (fan-triangulated, degenerate and
+    duplicate triangles dropped): (verts (nv,3) float64, tris (nt,3) uint32,
+    face_row (nt,) uint32, report dict).  Host only; needs no device."""
+    L = lib()
+    h = ctypes.c_void_p()
+    rep = _abi.OffReport()
+    rc = L.gi_off_load(os.fsencode(path), nthreads, ctypes.byref(h), ctypes.byref(rep))
+    if rc:
+        raise GIError(rc, "gi_off_load(%s)" % path)
+    try:
+        v = ctypes.POINTER(ctypes.c_double)()
+        t = ctypes.POINTER(ctypes.c_uint32)()
+        fr = ctypes.POINTER(ctypes.c_uint32)()
+        nv, nt = ctypes.c_uint32(), ctypes.c_uint32()
+        L.gi_off_arrays(h, ctypes.byref(v), ctypes.byref(nv), ctypes.byref(t), ctypes.byref(nt), ctypes.byref(fr))
+        verts = (np.ctypeslib.as_array(v, shape=(nv.value, 3)).copy() if nv.value else np.zeros((0, 3)))
+        tris = (np.ctypeslib.as_array(t, shape=(nt.value, 3)).copy() if nt.value else np.zeros((0, 3), np.uint32))
+        rows = (np.ctypeslib.as_array(fr, shape=(nt.value,)).copy() if nt.value else np.zeros(0, np.uint32))
+    finally:
+        L.gi_off_free(h)
+    return verts, tris, rows, rep.as_dict()
 
 
 class Mesh:
@@ -225,12 +261,27 @@ class Mesh:
         ctx.check(rc, "gi_mesh_upload")
         self.handle = h
 
+    @classmethod
+    def _wrap(cls, ctx, handle):
+        m = cls.__new__(cls)
+        m.ctx = ctx
+        m.handle = handle
+        return m
+
     def info(self):
         nv, nt = ctypes.c_uint32(), ctypes.c_uint32()
         nodes, nbytes = ctypes.c_uint64(), ctypes.c_uint64()
         self.ctx._lib.gi_mesh_info(self.handle, ctypes.byref(nv), ctypes.byref(nt), ctypes.byref(nodes),
                                    ctypes.byref(nbytes))
         return dict(nv=nv.value, nt=nt.value, nodes=nodes.value, bytes=nbytes.value)
+
+    def download(self):
+        """The vertices as stored on the device (after any normalisation), (nv, 3) float64."""
+        nv = self.info()["nv"]
+        out = np.empty((nv, 3), dtype=np.float64)
+        self.ctx.check(self.ctx._lib.gi_mesh_download(self.handle, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+                       "gi_mesh_download")
+        return out
 
     def release(self):
         if self.handle and self.ctx.handle:

@@ -34,9 +34,28 @@ EXPORTED = [
     "gi_pose_identity", "gi_pose_from_euler_deg", "gi_pose_apply",
     "gi_intersect_opts_default", "gi_intersect", "gi_intersect_oneshot", "gi_intersect_batch",
     "gi_classify_pairs", "gi_classify_pairs_noalloc",
+    "gi_off_load", "gi_off_arrays", "gi_off_free", "gi_scene_load", "gi_mesh_download",
     "gi_result_pairs", "gi_result_segments", "gi_result_stats", "gi_result_free",
     "gi_server_start", "gi_server_submit", "gi_server_poll", "gi_server_wait", "gi_server_stop",
 ]
+
+
+class OffReport(ctypes.Structure):
+    _fields_ = [("file_vertices", ctypes.c_uint64), ("file_polygons", ctypes.c_uint64),
+                ("extra_fan_triangles", ctypes.c_uint64), ("dropped_degenerate", ctypes.c_uint64),
+                ("dropped_duplicate", ctypes.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Scene(ctypes.Structure):
+    _fields_ = [("center", ctypes.c_double * 3), ("scale", ctypes.c_double), ("max_span", ctypes.c_double),
+                ("center_a", ctypes.c_double * 3), ("center_b", ctypes.c_double * 3)]
+
+    def as_dict(self):
+        return dict(center=list(self.center), scale=self.scale, max_span=self.max_span,
+                    center_a=list(self.center_a), center_b=list(self.center_b))
 
 
 class Options(ctypes.Structure):
@@ -116,6 +135,14 @@ def load(path=None):
                                ctypes.c_int32, vp], st),
         "gi_classify_pairs_noalloc": ([vp, vp, ctypes.POINTER(Pose), vp, ctypes.POINTER(Pose), vp, ctypes.c_uint32,
                                        ctypes.c_int32, vp], st),
+        "gi_off_load": ([ctypes.c_char_p, ctypes.c_uint32, ctypes.POINTER(vp), ctypes.POINTER(OffReport)], st),
+        "gi_off_arrays": ([vp, ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(up),
+                           ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(up)], st),
+        "gi_off_free": ([vp], st),
+        "gi_scene_load": ([vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(vp),
+                           ctypes.POINTER(vp), ctypes.POINTER(Scene), ctypes.POINTER(OffReport),
+                           ctypes.POINTER(OffReport)], st),
+        "gi_mesh_download": ([vp, dp], st),
         "gi_result_pairs": ([vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)), ctypes.POINTER(ctypes.c_uint64)], st),
         "gi_result_segments": ([vp, ctypes.POINTER(dp), ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)),
                                 ctypes.POINTER(ctypes.c_uint64)], st),

@@ -215,6 +215,42 @@ gi_status gi_classify_pairs_noalloc(gi_ctx* ctx, const gi_mesh* A, const gi_pose
                                     const gi_pose* pose_b, const int32_t* d_pairs, uint32_t npairs,
                                     int32_t precision_mode, uint8_t* d_out);
 
+/* ---- ingestion (upstream of the path) -------------------------------------- */
+/* OFF files as the reference loads them (src/CPU/RobustOffLoader.h:120-186,
+ * src/CPU/ParallelCgalOffLoader.h:35-186): polygons fan-triangulated as
+ * (p0, pk, pk+1), triangles with a repeated vertex index dropped, and later
+ * copies of a triangle's vertex set dropped.  Parsed on `nthreads` host threads
+ * (0: all) from a memory-mapped file. */
+typedef struct {
+    uint64_t file_vertices, file_polygons; /* counts in the file */
+    uint64_t extra_fan_triangles;          /* added by fan-triangulating polygons with > 3 corners */
+    uint64_t dropped_degenerate;           /* rows with < 3 corners, fan triangles with a repeated index */
+    uint64_t dropped_duplicate;            /* triangles repeating an earlier triangle's vertex set */
+} gi_off_report;
+typedef struct gi_off_mesh gi_off_mesh;
+gi_status gi_off_load(const char* path, uint32_t nthreads, gi_off_mesh** out, gi_off_report* report);
+/* host arrays of a loaded file; face_row[i]: the file's face row triangle i came from */
+gi_status gi_off_arrays(const gi_off_mesh* m, const double** verts_xyz, uint32_t* nv, const uint32_t** tris,
+                        uint32_t* nt, const uint32_t** face_row);
+gi_status gi_off_free(gi_off_mesh* m);
+
+/* Scene normalisation (apps/mainApplication.cpp:166-187, 637-680): the box of
+ * both meshes is centred and, with scale_to_unit, scaled so that its largest
+ * side spans 2: x' = (x - center) * scale in FP64, no fused multiply-add. */
+typedef struct {
+    double center[3];   /* centre of the scene box, subtracted from every vertex */
+    double scale;       /* 2 / max_span with scale_to_unit, else 1 */
+    double max_span;    /* largest side of the scene box before scaling */
+    double center_a[3]; /* box centres of the normalised meshes: the rotation centres of their poses */
+    double center_b[3];
+} gi_scene;
+/* Loads two OFF files, normalises them on the device and builds both meshes
+ * (the reference's load command). */
+gi_status gi_scene_load(gi_ctx* ctx, const char* path_a, const char* path_b, int32_t scale_to_unit, gi_mesh** A,
+                        gi_mesh** B, gi_scene* scene, gi_off_report* report_a, gi_off_report* report_b);
+/* The mesh's vertices (3 doubles each, as stored on the device) into verts_xyz_out. */
+gi_status gi_mesh_download(const gi_mesh* mesh, double* verts_xyz_out);
+
 /* ---- results -------------------------------------------------------------- */
 /* pairs_ab: 2 int32 per pair (faceA, faceB); pointer valid until gi_result_free. */
 gi_status gi_result_pairs(const gi_result* r, const int32_t** pairs_ab, uint64_t* n);
