@@ -246,6 +246,9 @@ def run_batch(args, gi, world, rank, dist):
             dev.append(rs[0].stats["ms_total"])
     st = rs[0].stats
     found = int(sum(len(r.pairs) for r in rs))
+    t0 = time.perf_counter()
+    ncurves = sum(len(r.curves()[1]) for r in rs)
+    curves_ms = (time.perf_counter() - t0) * 1e3
     total = float(np.sum(dev))
     if dist:
         t = torch.tensor([total], device="cuda", dtype=torch.float64)
@@ -267,6 +270,7 @@ def run_batch(args, gi, world, rank, dist):
         "stage_ms": {"traverse_filter": st["ms_traverse"], "exact": st["ms_exact"], "segments": st["ms_segments"],
                      "ordering": st["ms_sort"]},
         "wall_ms_p50": float(np.percentile(wall, 50)), "upload_build_s": upload_s, "clocks": clk.summary(),
+        "curve_assembly": {"ms": curves_ms, "curves": ncurves, "what": "gi_curves_build per pair, host"},
     }
     if rank == 0:
         _json(line)
@@ -513,6 +517,10 @@ def main():
     d2h = int(last_e2e.pairs.nbytes + last_e2e.segments.nbytes + last_e2e.seg_pair.nbytes)
 
     st = stats[-1]
+    # curve assembly (downstream of the path) on the last step's result
+    t0 = time.perf_counter()
+    cv_verts, cv = r.curves()
+    curves_ms = (time.perf_counter() - t0) * 1e3
     cand = np.mean([s["candidates"] for s in stats])
     tests_per_s = float(np.sum([s["candidates"] for s in stats]) / (np.sum(trav_ms) / 1e3))
     # roofline of the dominant kernel (traversal + first filter)
@@ -548,6 +556,8 @@ def main():
                      "ordering": float(np.mean([s["ms_sort"] for s in stats]))},
         "pose_update": {"p50_ms": float(np.percentile(wall_ms, 50)), "p99_ms": float(np.percentile(wall_ms, 99)),
                         "what": "gi_intersect wall clock, resident meshes, results on host"},
+        "curve_assembly": {"ms": curves_ms, "curves": len(cv), "closed": int(sum(1 for _, c in cv if c)),
+                           "vertices": int(cv_verts.shape[0]), "what": "gi_curves_build on the host, last step"},
         "fp64_form": {"value": float(np.mean(fp64_ms)), "unit": "ms",
                       "speedup_fp32_cascade": float(np.mean(fp64_ms) / max(1e-9, np.mean(dev_ms)))},
         "e2e": {"value": float(np.mean(e2e_ms)), "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

@@ -246,6 +246,39 @@ def load_off(path, nthreads=0):
     return verts, tris, rows, rep.as_dict()
 
 
+def curves(segments, seg_pair, npairs, drop_coplanar_interior=True):
+    """Intersection curves from a result's segments (gi_curves_build): returns
+    (vertices (k, 3) float64, list of (vertex index array, closed flag))."""
+    L = lib()
+    seg = np.ascontiguousarray(segments, dtype=np.float64).reshape(-1, 6)
+    sp = np.ascontiguousarray(seg_pair, dtype=np.int32).reshape(-1)
+    h = ctypes.c_void_p()
+    rc = L.gi_curves_build(seg.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                           sp.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), seg.shape[0], int(npairs),
+                           1 if drop_coplanar_interior else 0, ctypes.byref(h))
+    if rc:
+        raise GIError(rc, "gi_curves_build")
+    try:
+        vp = ctypes.POINTER(ctypes.c_double)()
+        nv = ctypes.c_uint64()
+        L.gi_curves_vertices(h, ctypes.byref(vp), ctypes.byref(nv))
+        verts = np.ctypeslib.as_array(vp, shape=(nv.value, 3)).copy() if nv.value else np.zeros((0, 3))
+        off = ctypes.POINTER(ctypes.c_uint64)()
+        idx = ctypes.POINTER(ctypes.c_uint32)()
+        cl = ctypes.POINTER(ctypes.c_uint8)()
+        nc = ctypes.c_uint64()
+        L.gi_curves_polylines(h, ctypes.byref(off), ctypes.byref(idx), ctypes.byref(cl), ctypes.byref(nc))
+        out = []
+        if nc.value:
+            o = np.ctypeslib.as_array(off, shape=(nc.value + 1,)).copy()
+            ii = np.ctypeslib.as_array(idx, shape=(int(o[-1]),)).copy() if o[-1] else np.zeros(0, np.uint32)
+            cc = np.ctypeslib.as_array(cl, shape=(nc.value,)).copy()
+            out = [(ii[o[k]:o[k + 1]], bool(cc[k])) for k in range(nc.value)]
+    finally:
+        L.gi_curves_free(h)
+    return verts, out
+
+
 class Mesh:
     def __init__(self, ctx, verts, tris, device_ptrs=None):
         self.ctx = ctx
@@ -353,10 +386,15 @@ class Result:
             a = np.asarray(_View(owner, ctypes.cast(ptr, ctypes.c_void_p).value, shape, dtype))
             return a if zero_copy else a.copy()
 
+        self.npairs = npairs
         self.pairs = arr(p, (npairs, 2), np.int32, npairs)
         self.segments = arr(sp, (nsegs, 6), np.float64, nsegs)
         self.seg_pair = arr(spp, (nsegs,), np.int32, nsegs)
         del owner  # freed here if every array was copied or empty
+
+    def curves(self, drop_coplanar_interior=True):
+        """The segments chained into polylines (see curves())."""
+        return curves(self.segments, self.seg_pair, self.npairs, drop_coplanar_interior)
 
 
 class Server:

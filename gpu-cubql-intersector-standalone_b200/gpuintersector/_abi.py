@@ -35,6 +35,7 @@ EXPORTED = [
     "gi_intersect_opts_default", "gi_intersect", "gi_intersect_oneshot", "gi_intersect_batch",
     "gi_classify_pairs", "gi_classify_pairs_noalloc",
     "gi_off_load", "gi_off_arrays", "gi_off_free", "gi_scene_load", "gi_mesh_download",
+    "gi_curves_build", "gi_result_curves", "gi_curves_vertices", "gi_curves_polylines", "gi_curves_free",
     "gi_result_pairs", "gi_result_segments", "gi_result_stats", "gi_result_free",
     "gi_server_start", "gi_server_submit", "gi_server_poll", "gi_server_wait", "gi_server_stop",
 ]
@@ -143,6 +144,13 @@ def load(path=None):
                            ctypes.POINTER(vp), ctypes.POINTER(Scene), ctypes.POINTER(OffReport),
                            ctypes.POINTER(OffReport)], st),
         "gi_mesh_download": ([vp, dp], st),
+        "gi_curves_build": ([dp, ctypes.POINTER(ctypes.c_int32), ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int32,
+                             ctypes.POINTER(vp)], st),
+        "gi_result_curves": ([vp, ctypes.c_int32, ctypes.POINTER(vp)], st),
+        "gi_curves_vertices": ([vp, ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_uint64)], st),
+        "gi_curves_polylines": ([vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_uint64)), ctypes.POINTER(up),
+                                 ctypes.POINTER(ctypes.POINTER(ctypes.c_uint8)), ctypes.POINTER(ctypes.c_uint64)], st),
+        "gi_curves_free": ([vp], st),
         "gi_result_pairs": ([vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)), ctypes.POINTER(ctypes.c_uint64)], st),
         "gi_result_segments": ([vp, ctypes.POINTER(dp), ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)),
                                 ctypes.POINTER(ctypes.c_uint64)], st),

@@ -251,6 +251,26 @@ gi_status gi_scene_load(gi_ctx* ctx, const char* path_a, const char* path_b, int
 /* The mesh's vertices (3 doubles each, as stored on the device) into verts_xyz_out. */
 gi_status gi_mesh_download(const gi_mesh* mesh, double* verts_xyz_out);
 
+/* ---- intersection curves (downstream of the path) ------------------------- */
+/* The segments of a result chained into polylines (the reference stops at the
+ * segment soup of src/CPU/MeshIntersectionCurves.cpp:27-91).  Endpoints are
+ * matched by exact equality (they are exact points rounded correctly, so a
+ * crossing on a shared mesh edge is bit-identical from both sides); equal
+ * edges are merged; zero-length segments become one-vertex curves; chains
+ * run through vertices of degree 2 and a chain back to its start is closed.
+ * With drop_coplanar_interior, an edge contributed two or more times and only
+ * by coplanar overlap triangles (pairs with three segments) is dropped, so a
+ * coplanar region is kept as its boundary.  Host code; needs no device. */
+typedef struct gi_curves gi_curves;
+gi_status gi_curves_build(const double* seg6, const int32_t* seg_pair, uint64_t nsegs, uint64_t npairs,
+                          int32_t drop_coplanar_interior, gi_curves** out);
+gi_status gi_result_curves(const gi_result* r, int32_t drop_coplanar_interior, gi_curves** out);
+gi_status gi_curves_vertices(const gi_curves* c, const double** xyz, uint64_t* n);
+/* curve k: vertex ids verts[offsets[k] .. offsets[k+1]), closed[k] = 1 if it closes */
+gi_status gi_curves_polylines(const gi_curves* c, const uint64_t** offsets, const uint32_t** verts,
+                              const uint8_t** closed, uint64_t* ncurves);
+gi_status gi_curves_free(gi_curves* c);
+
 /* ---- results -------------------------------------------------------------- */
 /* pairs_ab: 2 int32 per pair (faceA, faceB); pointer valid until gi_result_free. */
 gi_status gi_result_pairs(const gi_result* r, const int32_t** pairs_ab, uint64_t* n);
