@@ -36,6 +36,7 @@ EXPORTED = [
     "gi_classify_pairs", "gi_classify_pairs_noalloc",
     "gi_off_load", "gi_off_arrays", "gi_off_free", "gi_scene_load", "gi_mesh_download",
     "gi_curves_build", "gi_result_curves", "gi_curves_vertices", "gi_curves_polylines", "gi_curves_free",
+    "gi_records_write_csv", "gi_pairs_diff",
     "gi_result_pairs", "gi_result_segments", "gi_result_stats", "gi_result_free",
     "gi_server_start", "gi_server_submit", "gi_server_poll", "gi_server_wait", "gi_server_stop",
 ]
@@ -48,6 +49,11 @@ class OffReport(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class RecordMesh(ctypes.Structure):
+    _fields_ = [("verts_xyz", ctypes.POINTER(ctypes.c_double)), ("nv", ctypes.c_uint32),
+                ("tris", ctypes.POINTER(ctypes.c_uint32)), ("nt", ctypes.c_uint32)]
 
 
 class Scene(ctypes.Structure):
@@ -151,6 +157,13 @@ def load(path=None):
         "gi_curves_polylines": ([vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_uint64)), ctypes.POINTER(up),
                                  ctypes.POINTER(ctypes.POINTER(ctypes.c_uint8)), ctypes.POINTER(ctypes.c_uint64)], st),
         "gi_curves_free": ([vp], st),
+        "gi_records_write_csv": ([ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_char_p,
+                                  ctypes.POINTER(RecordMesh), ctypes.POINTER(RecordMesh),
+                                  ctypes.POINTER(ctypes.c_int32), ctypes.c_uint64, ctypes.c_uint32], st),
+        "gi_pairs_diff": ([ctypes.POINTER(ctypes.c_int32), ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32),
+                           ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_uint64),
+                           ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_uint64),
+                           ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_uint64)], st),
         "gi_result_pairs": ([vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)), ctypes.POINTER(ctypes.c_uint64)], st),
         "gi_result_segments": ([vp, ctypes.POINTER(dp), ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)),
                                 ctypes.POINTER(ctypes.c_uint64)], st),

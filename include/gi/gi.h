@@ -271,6 +271,34 @@ gi_status gi_curves_polylines(const gi_curves* c, const uint64_t** offsets, cons
                               const uint8_t** closed, uint64_t* ncurves);
 gi_status gi_curves_free(gi_curves* c);
 
+/* ---- run records: CSV export and run diffs (tooling around the path) ------ */
+/* The reference's IntersectionHistory (src/CPU/IntersectionHistory.h:12-232)
+ * keeps per intersecting pair a record of the face ids, the six vertex indices
+ * and the eighteen posed coordinates, exports a run to CSV (exportRunToCsv,
+ * :114-160) and diffs two runs by (faceA, faceB) (exportDiff, :162-232).  Here
+ * a run is its pair list plus the posed meshes (gi_pose_apply of the inputs).
+ * Host code; needs no device. */
+typedef struct {
+    const double* verts_xyz; /* posed vertices, 3 doubles each */
+    uint32_t nv;
+    const uint32_t* tris;    /* 3 vertex indices per triangle */
+    uint32_t nt;
+} gi_record_mesh;
+/* One row per pair in the given order: [category,]FaceA,FaceB,VA0_Idx..VB2_Idx,
+ * A_V0_X..B_V2_Z with every double as %.17g (the reference's setprecision(17)).
+ * header: write the header line first (with a DiffCategory column when
+ * category is given).  append: append to the file.  nthreads: 0 = all.  Every
+ * pair and vertex index is checked before anything is written
+ * (GI_ERR_INVALID_ARG). */
+gi_status gi_records_write_csv(const char* path, int32_t append, int32_t header, const char* category,
+                               const gi_record_mesh* A, const gi_record_mesh* B, const int32_t* pairs_ab, uint64_t n,
+                               uint32_t nthreads);
+/* Set diff of two pair lists by (faceA, faceB), duplicates merged.  Outputs are
+ * sorted by (faceA, faceB) in int order (the reference's std::set order) and
+ * need room for n1, n2 and min(n1, n2) pairs. */
+gi_status gi_pairs_diff(const int32_t* pairs1, uint64_t n1, const int32_t* pairs2, uint64_t n2, int32_t* only1,
+                        uint64_t* n_only1, int32_t* only2, uint64_t* n_only2, int32_t* both, uint64_t* n_both);
+
 /* ---- results -------------------------------------------------------------- */
 /* pairs_ab: 2 int32 per pair (faceA, faceB); pointer valid until gi_result_free. */
 gi_status gi_result_pairs(const gi_result* r, const int32_t** pairs_ab, uint64_t* n);
