@@ -94,6 +94,21 @@ def pose_apply(pose, verts):
     return out
 
 
+def sweep_poses(seed, steps, max_rot_deg=15.0, max_trans=0.5, base_rot_b=(0.0, 0.0, 0.0),
+                base_trans_b=(0.0, 0.0, 0.0)):
+    """B's Euler angles (degrees) and translations, (steps, 3) each, of the
+    seeded pose sweep (gi_sweep_poses: the reference's TestSuite draws)."""
+    rot = np.empty((steps, 3))
+    tr = np.empty((steps, 3))
+    br = np.ascontiguousarray(base_rot_b, dtype=np.float64)
+    bt = np.ascontiguousarray(base_trans_b, dtype=np.float64)
+    rc = lib().gi_sweep_poses(int(seed), int(steps), float(max_rot_deg), float(max_trans), _dp(br), _dp(bt),
+                              _dp(rot), _dp(tr))
+    if rc:
+        raise GIError(rc, "gi_sweep_poses")
+    return rot, tr
+
+
 # ---------------------------------------------------------------- handles
 class Context:
     """Owns one CUDA stream and the scratch buffers of the intersector."""

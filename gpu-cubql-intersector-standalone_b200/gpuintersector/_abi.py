@@ -36,7 +36,7 @@ EXPORTED = [
     "gi_classify_pairs", "gi_classify_pairs_noalloc",
     "gi_off_load", "gi_off_arrays", "gi_off_free", "gi_scene_load", "gi_mesh_download",
     "gi_curves_build", "gi_result_curves", "gi_curves_vertices", "gi_curves_polylines", "gi_curves_free",
-    "gi_records_write_csv", "gi_pairs_diff",
+    "gi_records_write_csv", "gi_pairs_diff", "gi_sweep_poses",
     "gi_result_pairs", "gi_result_segments", "gi_result_stats", "gi_result_free",
     "gi_server_start", "gi_server_submit", "gi_server_poll", "gi_server_wait", "gi_server_stop",
 ]
@@ -160,6 +160,7 @@ def load(path=None):
         "gi_records_write_csv": ([ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_char_p,
                                   ctypes.POINTER(RecordMesh), ctypes.POINTER(RecordMesh),
                                   ctypes.POINTER(ctypes.c_int32), ctypes.c_uint64, ctypes.c_uint32], st),
+        "gi_sweep_poses": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double, dp, dp, dp, dp], st),
         "gi_pairs_diff": ([ctypes.POINTER(ctypes.c_int32), ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32),
                            ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_uint64),
                            ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_uint64),

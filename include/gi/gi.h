@@ -299,6 +299,18 @@ gi_status gi_records_write_csv(const char* path, int32_t append, int32_t header,
 gi_status gi_pairs_diff(const int32_t* pairs1, uint64_t n1, const int32_t* pairs2, uint64_t n2, int32_t* only1,
                         uint64_t* n_only1, int32_t* only2, uint64_t* n_only2, int32_t* both, uint64_t* n_both);
 
+/* ---- pose sweep (verification harness around the path) -------------------- */
+/* The pose sequence of the reference's seeded sweep (TestSuite::runSuite,
+ * src/CPU/TestSuite.cpp:455-505): per step, B's Euler angles (degrees) and
+ * translation are its base plus uniform draws in [-max_rot_deg, max_rot_deg]
+ * and [-max_trans, max_trans] from std::mt19937(seed), drawn z, y, x for the
+ * rotation and then z, y, x for the translation (the order a GCC build of the
+ * reference evaluates them in).  A stays at its base pose.  Null bases are
+ * zero.  Outputs: 3 doubles per step each.  Host code; needs no device. */
+gi_status gi_sweep_poses(uint32_t seed, uint32_t nsteps, double max_rot_deg, double max_trans,
+                         const double base_rot_b[3], const double base_trans_b[3], double* rot_b_out,
+                         double* trans_b_out);
+
 /* ---- results -------------------------------------------------------------- */
 /* pairs_ab: 2 int32 per pair (faceA, faceB); pointer valid until gi_result_free. */
 gi_status gi_result_pairs(const gi_result* r, const int32_t** pairs_ab, uint64_t* n);
