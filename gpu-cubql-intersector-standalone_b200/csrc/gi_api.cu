@@ -91,6 +91,7 @@ extern "C" gi_status gi_create(const gi_options* opts, gi_ctx** out)
     }
     cudaSetDevice(c->device);
     cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking);
     if (e == cudaSuccess) {
         // the context's own stream-ordered pool: memory freed by one call (a
         // released mesh, a grown buffer) is reused by the next without being
@@ -122,6 +123,7 @@ extern "C" gi_status gi_destroy(gi_ctx* c)
     if (!c) return GI_ERR_INVALID_ARG;
     cudaSetDevice(c->device);
     if (c->st) cudaStreamSynchronize(c->st);
+    if (c->st2) cudaStreamSynchronize(c->st2);
     if (c->d_cnt) cudaFree(c->d_cnt);
     if (c->d_jobs) cudaFree(c->d_jobs);
     void* pooled[] = {c->queue, c->qflag,     c->cand,         c->cflag,   c->res,
@@ -136,6 +138,7 @@ extern "C" gi_status gi_destroy(gi_ctx* c)
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->st) cudaStreamDestroy(c->st);
+    if (c->st2) cudaStreamDestroy(c->st2);
     delete c;
     return GI_OK;
 }
@@ -143,39 +146,69 @@ extern "C" gi_status gi_destroy(gi_ctx* c)
 // ---------------------------------------------------------------------------
 // Meshes
 // ---------------------------------------------------------------------------
-static void mesh_free(gi_ctx* c, gi_mesh* m);
+static void mesh_free(gi_ctx* c, gi_mesh* m, cudaStream_t st);
 
-static gi_status mesh_finish(gi_ctx* c, gi_mesh* m, gi_mesh** out)
+// Mesh uploads run on a given stream and report errors to a given sink, so
+// that the two meshes of a one-shot call can be built from two host threads.
+struct UploadSink {
+    gi_ctx* c;
+    std::string* msg;  // nullptr: the context's last error
+    gi_status fail(gi_status s, const char* what, cudaError_t e = cudaSuccess) const
+    {
+        if (!msg) return set_err(c, s, what, e);
+        char buf[512];
+        if (e != cudaSuccess)
+            snprintf(buf, sizeof buf, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+        else
+            snprintf(buf, sizeof buf, "%s", what);
+        *msg = buf;
+        return s;
+    }
+    gi_status cuda(cudaError_t e, const char* what) const
+    {
+        return fail(e == cudaErrorMemoryAllocation ? GI_ERR_OOM : GI_ERR_CUDA, what, e);
+    }
+};
+
+#define CKS(sink, x, what)                          \
+    do {                                            \
+        cudaError_t e_ = (x);                       \
+        if (e_ != cudaSuccess) return (sink).cuda(e_, (what)); \
+    } while (0)
+
+static gi_status mesh_finish(gi_ctx* c, gi_mesh* m, gi_mesh** out, cudaStream_t st, const UploadSink& sk)
 {
     unsigned* d_err = nullptr;
-    CK(c, pool_alloc(&d_err, sizeof(unsigned), c->pool, c->st), "alloc");
-    CK(c, cudaMemsetAsync(d_err, 0, sizeof(unsigned), c->st), "memset");
-    CK(c, launch_validate(m->b.verts, m->b.nv, m->b.tris, m->b.nt, d_err, c->st), "validate");
+    CKS(sk, pool_alloc(&d_err, sizeof(unsigned), c->pool, st), "alloc");
+    CKS(sk, cudaMemsetAsync(d_err, 0, sizeof(unsigned), st), "memset");
+    CKS(sk, launch_validate(m->b.verts, m->b.nv, m->b.tris, m->b.nt, d_err, st), "validate");
     unsigned herr = 0;
-    CK(c, cudaMemcpyAsync(&herr, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st), "copy");
-    CK(c, cudaStreamSynchronize(c->st), "sync");
-    cudaFreeAsync(d_err, c->st);
+    CKS(sk, cudaMemcpyAsync(&herr, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "copy");
+    CKS(sk, cudaStreamSynchronize(st), "sync");
+    cudaFreeAsync(d_err, st);
     if (herr) {
-        mesh_free(c, m);
-        return set_err(c, (herr & 1u) ? GI_ERR_INVALID_ARG : GI_ERR_RANGE,
+        mesh_free(c, m, st);
+        return sk.fail((herr & 1u) ? GI_ERR_INVALID_ARG : GI_ERR_RANGE,
                        (herr & 1u) ? "triangle index out of range" : "vertex coordinate outside the supported domain");
     }
-    cudaError_t e = build_bvh(m->b, false, c->pool, c->st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    cudaError_t e = build_bvh(m->b, false, c->pool, st);
+    // on an error the stream may still hold kernels that use the mesh: drain it before freeing
+    cudaError_t es = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = es;
     if (e != cudaSuccess) {
-        mesh_free(c, m);
-        return set_err(c, e == cudaErrorMemoryAllocation ? GI_ERR_OOM : GI_ERR_CUDA, "BVH build", e);
+        mesh_free(c, m, st);
+        return sk.fail(e == cudaErrorMemoryAllocation ? GI_ERR_OOM : GI_ERR_CUDA, "BVH build", e);
     }
     c->mesh_bytes += m->b.bytes;
     if (c->budget && c->mesh_bytes > c->budget) {
-        mesh_free(c, m);
-        return set_err(c, GI_ERR_OOM, "HBM budget exceeded by mesh upload");
+        mesh_free(c, m, st);
+        return sk.fail(GI_ERR_OOM, "HBM budget exceeded by mesh upload");
     }
     *out = m;
     return GI_OK;
 }
 
-static gi_status mesh_alloc(gi_ctx* c, uint32_t nv, uint32_t nt, gi_mesh** pm)
+static gi_status mesh_alloc(gi_ctx* c, uint32_t nv, uint32_t nt, gi_mesh** pm, cudaStream_t st, const UploadSink& sk)
 {
     gi_mesh* m = new (std::nothrow) gi_mesh();
     if (!m) return GI_ERR_OOM;
@@ -185,18 +218,37 @@ static gi_status mesh_alloc(gi_ctx* c, uint32_t nv, uint32_t nt, gi_mesh** pm)
     size_t vb = sizeof(double) * 3 * (size_t)(nv ? nv : 1), tb = sizeof(uint32_t) * 3 * (size_t)(nt ? nt : 1);
     if (c->budget && c->mesh_bytes + vb + tb > c->budget) {
         delete m;
-        return set_err(c, GI_ERR_OOM, "HBM budget exceeded by mesh upload");
+        return sk.fail(GI_ERR_OOM, "HBM budget exceeded by mesh upload");
     }
-    cudaError_t e = pool_alloc(&m->b.verts, vb, c->pool, c->st);
-    if (e == cudaSuccess) e = pool_alloc(&m->b.tris, tb, c->pool, c->st);
+    cudaError_t e = pool_alloc(&m->b.verts, vb, c->pool, st);
+    if (e == cudaSuccess) e = pool_alloc(&m->b.tris, tb, c->pool, st);
     if (e != cudaSuccess) {
-        if (m->b.verts) cudaFreeAsync(m->b.verts, c->st);
+        if (m->b.verts) cudaFreeAsync(m->b.verts, st);
         delete m;
-        return set_err(c, GI_ERR_OOM, "mesh allocation", e);
+        return sk.fail(GI_ERR_OOM, "mesh allocation", e);
     }
     m->b.bytes = vb + tb;
     *pm = m;
     return GI_OK;
+}
+
+// Host arrays -> device mesh with its BVH, on stream st (the caller holds c->mu).
+static gi_status mesh_upload_on(gi_ctx* c, const double* verts, uint32_t nv, const uint32_t* tris, uint32_t nt,
+                                gi_mesh** out, cudaStream_t st, const UploadSink& sk)
+{
+    gi_mesh* m = nullptr;
+    gi_status s = mesh_alloc(c, nv, nt, &m, st, sk);
+    if (s != GI_OK) return s;
+    cudaError_t e = cudaSuccess;
+    if (nv) e = cudaMemcpyAsync(m->b.verts, verts, sizeof(double) * 3 * (size_t)nv, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && nt)
+        e = cudaMemcpyAsync(m->b.tris, tris, sizeof(uint32_t) * 3 * (size_t)nt, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) {
+        cudaStreamSynchronize(st);
+        mesh_free(c, m, st);
+        return sk.cuda(e, "upload mesh");
+    }
+    return mesh_finish(c, m, out, st, sk);
 }
 
 extern "C" gi_status gi_mesh_upload(gi_ctx* c, const double* verts, uint32_t nv, const uint32_t* tris, uint32_t nt,
@@ -205,14 +257,7 @@ extern "C" gi_status gi_mesh_upload(gi_ctx* c, const double* verts, uint32_t nv,
     if (!c || !out || (nv && !verts) || (nt && !tris) || nt > 0x7fffffffu) return GI_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
-    gi_mesh* m = nullptr;
-    gi_status s = mesh_alloc(c, nv, nt, &m);
-    if (s != GI_OK) return s;
-    if (nv) CK(c, cudaMemcpyAsync(m->b.verts, verts, sizeof(double) * 3 * (size_t)nv, cudaMemcpyHostToDevice, c->st),
-               "upload vertices");
-    if (nt) CK(c, cudaMemcpyAsync(m->b.tris, tris, sizeof(uint32_t) * 3 * (size_t)nt, cudaMemcpyHostToDevice, c->st),
-               "upload triangles");
-    return mesh_finish(c, m, out);
+    return mesh_upload_on(c, verts, nv, tris, nt, out, c->st, UploadSink{c, nullptr});
 }
 
 extern "C" gi_status gi_mesh_upload_device(gi_ctx* c, const double* d_verts, uint32_t nv, const uint32_t* d_tris,
@@ -222,24 +267,25 @@ extern "C" gi_status gi_mesh_upload_device(gi_ctx* c, const double* d_verts, uin
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
     gi_mesh* m = nullptr;
-    gi_status s = mesh_alloc(c, nv, nt, &m);
+    const UploadSink sk{c, nullptr};
+    gi_status s = mesh_alloc(c, nv, nt, &m, c->st, sk);
     if (s != GI_OK) return s;
     if (nv) CK(c, cudaMemcpyAsync(m->b.verts, d_verts, sizeof(double) * 3 * (size_t)nv, cudaMemcpyDeviceToDevice,
                                   c->st), "copy vertices");
     if (nt) CK(c, cudaMemcpyAsync(m->b.tris, d_tris, sizeof(uint32_t) * 3 * (size_t)nt, cudaMemcpyDeviceToDevice,
                                   c->st), "copy triangles");
-    return mesh_finish(c, m, out);
+    return mesh_finish(c, m, out, c->st, sk);
 }
 
-// Frees a mesh's buffers in stream order (the caller holds c->mu).
-static void mesh_free(gi_ctx* c, gi_mesh* m)
+// Frees a mesh's buffers in order on stream st (the caller holds c->mu).
+static void mesh_free(gi_ctx* c, gi_mesh* m, cudaStream_t st)
 {
     cudaSetDevice(c->device);
-    // stream-ordered: work already queued on the context's stream still sees the mesh
+    // stream-ordered: work already queued on st still sees the mesh
     void* p[] = {m->b.verts,     m->b.tris,    m->b.leafTri, m->b.leafBox, m->b.nodes,
                  m->b.leafBox64, m->b.nodes64, m->b.cutRef,  m->b.cutBox,  m->b.cutBox64};
     for (void* q : p)
-        if (q) cudaFreeAsync(q, c->st);
+        if (q) cudaFreeAsync(q, st);
     if (m->b.bytes <= c->mesh_bytes) c->mesh_bytes -= m->b.bytes;
     delete m;
 }
@@ -248,7 +294,7 @@ extern "C" gi_status gi_mesh_release(gi_ctx* c, gi_mesh* m)
 {
     if (!c || !m || m->ctx != c) return GI_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
-    mesh_free(c, m);
+    mesh_free(c, m, c->st);
     return GI_OK;
 }
 
@@ -790,14 +836,34 @@ extern "C" gi_status gi_intersect_oneshot(gi_ctx* c, const double* vA, uint32_t 
                                           uint32_t ntB, const gi_pose* pb, const gi_intersect_opts* opts,
                                           gi_result** out)
 {
-    if (!c || !out) return GI_ERR_INVALID_ARG;
+    if (!c || !out || (nvA && !vA) || (ntA && !tA) || (nvB && !vB) || (ntB && !tB) || ntA > 0x7fffffffu ||
+        ntB > 0x7fffffffu)
+        return GI_ERR_INVALID_ARG;
     gi_mesh *A = nullptr, *B = nullptr;
-    gi_status s = gi_mesh_upload(c, vA, nvA, tA, ntA, &A);
-    if (s != GI_OK) return s;
-    s = gi_mesh_upload(c, vB, nvB, tB, ntB, &B);
-    if (s != GI_OK) {
-        gi_mesh_release(c, A);
-        return s;
+    gi_status s;
+    {
+        // B is copied and built on the second stream by a helper thread while A
+        // is on the context's stream: B's copy overlaps A's build and the two
+        // builds overlap each other
+        std::lock_guard<std::mutex> lk(c->mu);
+        cudaSetDevice(c->device);
+        gi_status sb = GI_OK;
+        std::string msg_b;
+        std::thread tb([&] {
+            cudaSetDevice(c->device);
+            sb = mesh_upload_on(c, vB, nvB, tB, ntB, &B, c->st2, UploadSink{c, &msg_b});
+        });
+        s = mesh_upload_on(c, vA, nvA, tA, ntA, &A, c->st, UploadSink{c, nullptr});
+        tb.join();
+        if (s == GI_OK && sb != GI_OK) {
+            s = sb;
+            c->last_error = msg_b;
+        }
+        if (s != GI_OK) {
+            if (A) mesh_free(c, A, c->st);
+            if (B) mesh_free(c, B, c->st);
+            return s;
+        }
     }
     s = gi_intersect(c, A, pa, B, pb, opts, out);
     gi_mesh_release(c, A);

@@ -167,6 +167,7 @@ struct TravTuner {
 struct gi_ctx {
     int device = 0;
     cudaStream_t st = nullptr;
+    cudaStream_t st2 = nullptr;  // second mesh of a one-shot call builds here, concurrently with the first
     cudaMemPool_t pool = nullptr;  // stream-ordered allocations of this context
     gi::LaunchCfg cfg;
     uint64_t budget = 0;

@@ -65,8 +65,11 @@ __device__ __forceinline__ float ord2f(unsigned u)
 // FP32 boxes rounded outward (so every exact triangle lies inside its box) and
 // centroid bounds.  The reference rounds to nearest (src/common/utils.cu:639),
 // which can drop true pairs; outward rounding keeps the candidate set a superset.
-__global__ void k_tri_boxes(const double* __restrict__ V, const uint32_t* __restrict__ T, uint32_t nt,
-                            float* __restrict__ box, double* __restrict__ box64, unsigned* __restrict__ cb)
+constexpr int kTriBoxThreads = 256;
+__global__ void __launch_bounds__(kTriBoxThreads) k_tri_boxes(const double* __restrict__ V,
+                                                              const uint32_t* __restrict__ T, uint32_t nt,
+                                                              float* __restrict__ box, double* __restrict__ box64,
+                                                              unsigned* __restrict__ cb)
 {
     float cmin[3] = {INFINITY, INFINITY, INFINITY}, cmax[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
@@ -86,17 +89,28 @@ __global__ void k_tri_boxes(const double* __restrict__ V, const uint32_t* __rest
             cmax[k] = fmaxf(cmax[k], cc);
         }
     }
+    // block reduction, then one set of atomics per block: per-warp atomics on
+    // the same six words serialised in L2 and dominated the kernel
+    __shared__ float red[kTriBoxThreads / 32][6];
     for (int k = 0; k < 3; k++) {
         for (int o = 16; o > 0; o >>= 1) {
             cmin[k] = fminf(cmin[k], __shfl_xor_sync(0xffffffffu, cmin[k], o));
             cmax[k] = fmaxf(cmax[k], __shfl_xor_sync(0xffffffffu, cmax[k], o));
         }
     }
-    if ((threadIdx.x & 31) == 0) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0)
         for (int k = 0; k < 3; k++) {
-            atomicMin(&cb[k], f2ord(cmin[k]));
-            atomicMax(&cb[3 + k], f2ord(cmax[k]));
+            red[w][k] = cmin[k];
+            red[w][3 + k] = cmax[k];
         }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int k = threadIdx.x;
+        float v = red[0][k];
+        for (int q = 1; q < kTriBoxThreads / 32; q++) v = k < 3 ? fminf(v, red[q][k]) : fmaxf(v, red[q][k]);
+        if (k < 3) atomicMin(&cb[k], f2ord(v));
+        else atomicMax(&cb[k], f2ord(v));
     }
 }
 
@@ -188,6 +202,13 @@ __device__ __forceinline__ double ldcg_s<double>(const double* p)
     return __ldcg(p);
 }
 
+__device__ __forceinline__ unsigned arrive_acq_rel(unsigned* f)
+{
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(f) : "memory");
+    return old;
+}
+
 // Bottom-up refit: the second thread to arrive at a node merges both children.
 template <class S>
 __global__ void k_refit(int n, const uint2* __restrict__ child, const int* __restrict__ parent,
@@ -197,9 +218,9 @@ __global__ void k_refit(int n, const uint2* __restrict__ child, const int* __res
     if (p >= n) return;
     int node = parent[n - 1 + p];
     for (int guard = 0; node >= 0 && guard < n; guard++) {
-        __threadfence();
-        if (atomicAdd(&flags[node], 1u) == 0u) return;
-        __threadfence();
+        // release: this thread's box stores (the previous level) before the
+        // arrival; acquire: the sibling's box stores after it
+        if (arrive_acq_rel(&flags[node]) == 0u) return;
         uint2 c = child[node];
         S b[6];
         for (int side = 0; side < 2; side++) {
@@ -212,7 +233,6 @@ __global__ void k_refit(int n, const uint2* __restrict__ child, const int* __res
             }
         }
         for (int k = 0; k < 6; k++) nodeBox[6 * (size_t)node + k] = b[k];
-        __threadfence();
         node = parent[node];
     }
 }
@@ -357,7 +377,8 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaMemPool_t pool, cudaStream_
     unsigned* flags = nullptr;
     uint32_t *even = nullptr, *widx = nullptr;
     void* nodeBox = nullptr;
-    size_t cw = radix_counts_words(n);
+    constexpr int kMortonDigit = 10;  // 30-bit keys: three passes
+    size_t cw = radix_counts_words<kMortonDigit>(n);
     size_t sw = scan_temp_words(cw > n ? cw : n);
     GI_TRY(pool_alloc(&box, sizeof(float) * 6 * n, pool, st));
     if (fp64) GI_TRY(pool_alloc(&box64, sizeof(double) * 6 * n, pool, st));
@@ -372,9 +393,10 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaMemPool_t pool, cudaStream_
     GI_TRY(cudaMemcpyAsync(cb, cbinit, sizeof(cbinit), cudaMemcpyHostToDevice, st));
     int tb = 256;
     int gb = (int)((n + tb - 1) / tb);
-    k_tri_boxes<<<gb < 4096 ? gb : 4096, tb, 0, st>>>(m.verts, m.tris, n, box, box64, cb);
+    // a few blocks per SM, each looping: the centroid bounds take one set of atomics per block
+    k_tri_boxes<<<gb < 1184 ? gb : 1184, kTriBoxThreads, 0, st>>>(m.verts, m.tris, n, box, box64, cb);
     k_morton<<<gb, tb, 0, st>>>(box, n, cb, k0, v0);
-    radix_sort<uint32_t>(k0, v0, k1, v1, n, 30, counts, stemp, st);
+    radix_sort<uint32_t, kMortonDigit>(k0, v0, k1, v1, n, 30, counts, stemp, st);
     // leaves in sorted order
     if (!fp64) {
         GI_TRY(pool_alloc(&m.leafBox, sizeof(float) * 6 * n, pool, st));
