@@ -1,4 +1,4 @@
-// gi_sort.cuh -- device scan and LSD radix sort (8-bit digits, stable).
+// gi_sort.cuh -- device scan and LSD radix sort (8- or 10-bit digits, stable).
 //
 // Used by the BVH build (30-bit Morton keys, replaces the reference's CUB
 // DeviceRadixSort in include/third-party/cubql/level_cut_builder.h:345-347)
@@ -110,34 +110,36 @@ constexpr int kRsItems = 16;
 constexpr int kRsTile = kRsThreads * kRsItems;  // 4096
 constexpr int kRsWarps = kRsThreads / 32;
 
-template <class K>
+template <class K, int BITS>
 __global__ void __launch_bounds__(kRsThreads) k_rs_hist(const K* __restrict__ keys, uint32_t n, int shift,
                                                         uint32_t* __restrict__ counts, uint32_t ntiles)
 {
-    __shared__ uint32_t h[256];
-    h[threadIdx.x] = 0;
+    constexpr uint32_t kDig = 1u << BITS;
+    __shared__ uint32_t h[kDig];
+    for (uint32_t d = threadIdx.x; d < kDig; d += kRsThreads) h[d] = 0;
     __syncthreads();
     uint32_t base = blockIdx.x * kRsTile;
 #pragma unroll 4
     for (int k = 0; k < kRsItems; k++) {
         uint32_t i = base + k * kRsThreads + threadIdx.x;
-        if (i < n) atomicAdd(&h[(uint32_t)(keys[i] >> shift) & 255u], 1u);
+        if (i < n) atomicAdd(&h[(uint32_t)(keys[i] >> shift) & (kDig - 1u)], 1u);
     }
     __syncthreads();
-    counts[threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+    for (uint32_t d = threadIdx.x; d < kDig; d += kRsThreads) counts[d * ntiles + blockIdx.x] = h[d];
 }
 
-template <class K>
+template <class K, int BITS>
 __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                            K* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t n,
                                                            int shift, const uint32_t* __restrict__ offsets,
                                                            uint32_t ntiles)
 {
-    __shared__ uint32_t wc[kRsWarps][256];
-    __shared__ uint32_t tile_off[256];
+    constexpr uint32_t kDig = 1u << BITS;
+    __shared__ uint32_t wc[kRsWarps][kDig];
+    __shared__ uint32_t tile_off[kDig];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int d = lane; d < 256; d += 32) wc[w][d] = 0;
-    tile_off[threadIdx.x] = offsets[threadIdx.x * ntiles + blockIdx.x];
+    for (uint32_t d = lane; d < kDig; d += 32) wc[w][d] = 0;
+    for (uint32_t d = threadIdx.x; d < kDig; d += kRsThreads) tile_off[d] = offsets[d * ntiles + blockIdx.x];
     __syncwarp();
     const uint32_t seg = blockIdx.x * kRsTile + w * 32 * kRsItems;
     K key[kRsItems];
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K* __restrict__
         bool ok = i < n;
         key[c] = ok ? kin[i] : (K)0;
         val[c] = ok ? vin[i] : 0u;
-        uint32_t d = ok ? ((uint32_t)(key[c] >> shift) & 255u) : 256u;
+        uint32_t d = ok ? ((uint32_t)(key[c] >> shift) & (kDig - 1u)) : kDig;
         dig[c] = d;
         unsigned peers = __match_any_sync(0xffffffffu, d);
         uint32_t r = 0;
@@ -163,8 +165,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K* __restrict__
     }
     __syncthreads();
     // per digit: exclusive prefix over warps
-    {
-        uint32_t d = threadIdx.x;
+    for (uint32_t d = threadIdx.x; d < kDig; d += kRsThreads) {
         uint32_t run = 0;
         for (int q = 0; q < kRsWarps; q++) {
             uint32_t t = wc[q][d];
@@ -176,7 +177,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K* __restrict__
 #pragma unroll
     for (int c = 0; c < kRsItems; c++) {
         uint32_t d = dig[c];
-        if (d < 256u) {
+        if (d < kDig) {
             uint32_t pos = tile_off[d] + wc[w][d] + rank[c];
             kout[pos] = key[c];
             vout[pos] = val[c];
@@ -184,23 +185,24 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K* __restrict__
     }
 }
 
-// Sorts (keys, vals) by the low `bits` bits of the key; result ends in (k0, v0).
-// Scratch: k1/v1 the same size, counts 256*ntiles words, scan temp.
-template <class K>
+// Sorts (keys, vals) by the low `bits` bits of the key in passes of BITS-bit
+// digits; result ends in (k0, v0).  Scratch: k1/v1 the same size, counts
+// radix_counts_words<BITS>(n) words, scan temp.
+template <class K, int BITS = 8>
 void radix_sort(K* k0, uint32_t* v0, K* k1, uint32_t* v1, uint32_t n, int bits, uint32_t* counts, uint32_t* temp,
                 cudaStream_t st)
 {
     if (n <= 1) return;
     uint32_t ntiles = (n + kRsTile - 1) / kRsTile;
-    int passes = (bits + 7) / 8;
+    int passes = (bits + BITS - 1) / BITS;
     K* ks = k0;
     uint32_t* vs = v0;
     K* kd = k1;
     uint32_t* vd = v1;
     for (int p = 0; p < passes; p++) {
-        k_rs_hist<K><<<ntiles, kRsThreads, 0, st>>>(ks, n, 8 * p, counts, ntiles);
-        scan_exclusive(counts, counts, 256u * ntiles, temp, st);
-        k_rs_scatter<K><<<ntiles, kRsThreads, 0, st>>>(ks, vs, kd, vd, n, 8 * p, counts, ntiles);
+        k_rs_hist<K, BITS><<<ntiles, kRsThreads, 0, st>>>(ks, n, BITS * p, counts, ntiles);
+        scan_exclusive(counts, counts, (1u << BITS) * ntiles, temp, st);
+        k_rs_scatter<K, BITS><<<ntiles, kRsThreads, 0, st>>>(ks, vs, kd, vd, n, BITS * p, counts, ntiles);
         note_launches(2);
         K* tk = ks;
         ks = kd;
@@ -215,9 +217,10 @@ void radix_sort(K* k0, uint32_t* v0, K* k1, uint32_t* v1, uint32_t n, int bits, 
     }
 }
 
+template <int BITS = 8>
 inline size_t radix_counts_words(uint32_t n)
 {
-    return 256ull * ((n + kRsTile - 1) / kRsTile);
+    return (1ull << BITS) * ((n + kRsTile - 1) / kRsTile);
 }
 
 }  // namespace gi
