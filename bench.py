@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--level", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--workload", default="pose", choices=["pose", "batch", "serving", "ingest"],
                     help="pose: the headline pose-update stream on two 1.3M-triangle meshes; batch: many "
                          "mesh pairs of uneven size in one call; serving: resident pairs under an HBM "
@@ -503,12 +503,12 @@ def main():
     hvA, htA, hvB, htB = (h[1] for h in hold)
     e2e_ms = []
     last_e2e = None
-    for k in range(2 + args.e2e_steps):
+    for k in range(3 + args.e2e_steps):
         R, C, T = poses[args.warmup + (k % args.steps)]
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         last_e2e = ctx.intersect_oneshot(hvA, htA, hvB, htB, None, gi.pose_raw(R, C, T))
-        if k >= 2:  # two untimed calls first
+        if k >= 3:  # three untimed warm-up calls first
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
     # the same call from pageable (ordinary numpy) arrays, for comparison
     pageable_ms = []

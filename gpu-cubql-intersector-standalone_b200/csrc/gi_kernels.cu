@@ -62,31 +62,82 @@ __device__ __forceinline__ float ord2f(unsigned u)
     return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
 }
 
+// Boxes are 6 consecutive values (lo xyz, hi xyz): 24 B for float (8-byte
+// aligned), 48 B for double (16-byte aligned), moved as three 2-vectors.
+template <class S>
+struct Vec2Of;
+template <>
+struct Vec2Of<float> {
+    using T = float2;
+};
+template <>
+struct Vec2Of<double> {
+    using T = double2;
+};
+template <class S>
+__device__ __forceinline__ void load_box_cg(const S* p, S b[6])
+{
+    using V = typename Vec2Of<S>::T;
+    const V* q = reinterpret_cast<const V*>(p);
+    const V a = __ldcg(q), c = __ldcg(q + 1), d = __ldcg(q + 2);
+    b[0] = a.x, b[1] = a.y, b[2] = c.x, b[3] = c.y, b[4] = d.x, b[5] = d.y;
+}
+template <class S>
+__device__ __forceinline__ void store_box(S* p, const S b[6])
+{
+    using V = typename Vec2Of<S>::T;
+    V* q = reinterpret_cast<V*>(p);
+    q[0] = V{b[0], b[1]};
+    q[1] = V{b[2], b[3]};
+    q[2] = V{b[4], b[5]};
+}
+
 // FP32 boxes rounded outward (so every exact triangle lies inside its box) and
 // centroid bounds.  The reference rounds to nearest (src/common/utils.cu:639),
 // which can drop true pairs; outward rounding keeps the candidate set a superset.
 constexpr int kTriBoxThreads = 256;
-__global__ void __launch_bounds__(kTriBoxThreads) k_tri_boxes(const double* __restrict__ V,
+__global__ void __launch_bounds__(kTriBoxThreads, 4) k_tri_boxes(const double* __restrict__ V,
                                                               const uint32_t* __restrict__ T, uint32_t nt,
                                                               float* __restrict__ box, double* __restrict__ box64,
                                                               unsigned* __restrict__ cb)
 {
     float cmin[3] = {INFINITY, INFINITY, INFINITY}, cmax[3] = {-INFINITY, -INFINITY, -INFINITY};
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
-        uint32_t i0 = T[3 * (size_t)t], i1 = T[3 * (size_t)t + 1], i2 = T[3 * (size_t)t + 2];
-        for (int k = 0; k < 3; k++) {
-            double a = V[3 * (size_t)i0 + k], b = V[3 * (size_t)i1 + k], c = V[3 * (size_t)i2 + k];
-            double lo = fmin(a, fmin(b, c)), hi = fmax(a, fmax(b, c));
-            float flo = __double2float_rd(lo), fhi = __double2float_ru(hi);
-            box[6 * (size_t)t + k] = flo;
-            box[6 * (size_t)t + 3 + k] = fhi;
-            if (box64) {
-                box64[6 * (size_t)t + k] = lo;
-                box64[6 * (size_t)t + 3 + k] = hi;
+    // two triangles per iteration, all their loads issued before any use
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += 2 * stride) {
+        const uint32_t tt[2] = {t, t + stride < nt ? t + stride : t};
+        uint32_t ix[2][3];
+        double v[2][9];
+#pragma unroll
+        for (int q = 0; q < 2; q++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) ix[q][j] = T[3 * (size_t)tt[q] + j];
+#pragma unroll
+        for (int q = 0; q < 2; q++)
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+#pragma unroll
+                for (int k = 0; k < 3; k++) v[q][3 * j + k] = V[3 * (size_t)ix[q][j] + k];
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            if (q == 1 && tt[1] == t) break;
+            const size_t o = 6 * (size_t)tt[q];
+            float fb[6];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const double a = v[q][k], b = v[q][3 + k], c = v[q][6 + k];
+                const double lo = fmin(a, fmin(b, c)), hi = fmax(a, fmax(b, c));
+                fb[k] = __double2float_rd(lo);
+                fb[3 + k] = __double2float_ru(hi);
+                if (box64) {
+                    box64[o + k] = lo;
+                    box64[o + 3 + k] = hi;
+                }
+                const float cc = 0.5f * fb[k] + 0.5f * fb[3 + k];
+                cmin[k] = fminf(cmin[k], cc);
+                cmax[k] = fmaxf(cmax[k], cc);
             }
-            float cc = 0.5f * flo + 0.5f * fhi;
-            cmin[k] = fminf(cmin[k], cc);
-            cmax[k] = fmaxf(cmax[k], cc);
+            store_box(box + o, fb);
         }
     }
     // block reduction, then one set of atomics per block: per-warp atomics on
@@ -185,7 +236,9 @@ __global__ void k_leaves(const uint32_t* __restrict__ vals, uint32_t n, const ui
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     uint32_t tri = vals[p];
-    for (int k = 0; k < 6; k++) leafBox[6 * (size_t)p + k] = boxOrig[6 * (size_t)tri + k];
+    S b[6];
+    load_box_cg(boxOrig + 6 * (size_t)tri, b);
+    store_box(leafBox + 6 * (size_t)p, b);
     if (leafTri) leafTri[p] = make_uint4(T[3 * (size_t)tri], T[3 * (size_t)tri + 1], T[3 * (size_t)tri + 2], tri);
 }
 
@@ -210,30 +263,47 @@ __device__ __forceinline__ unsigned arrive_acq_rel(unsigned* f)
 }
 
 // Bottom-up refit: the second thread to arrive at a node merges both children.
+// A thread keeps its own subtree's box in registers and reads only the
+// sibling's; the tree links of the next level do not depend on other threads
+// and are loaded while the sibling's box is in flight, so a level costs the
+// arrival atomic and one box load.
 template <class S>
 __global__ void k_refit(int n, const uint2* __restrict__ child, const int* __restrict__ parent,
                         const S* __restrict__ leafBox, S* nodeBox, unsigned* flags)
 {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
+    S b[6];
+    load_box_cg(leafBox + 6 * (size_t)p, b);
+    uint32_t self = kLeaf | (uint32_t)p;
     int node = parent[n - 1 + p];
-    for (int guard = 0; node >= 0 && guard < n; guard++) {
+    if (node < 0) return;
+    uint2 c = child[node];
+    int up = parent[node];
+    for (int guard = 0; guard < n; guard++) {
         // release: this thread's box stores (the previous level) before the
         // arrival; acquire: the sibling's box stores after it
         if (arrive_acq_rel(&flags[node]) == 0u) return;
-        uint2 c = child[node];
-        S b[6];
-        for (int side = 0; side < 2; side++) {
-            uint32_t r = side ? c.y : c.x;
-            const S* src = (r & kLeaf) ? leafBox + 6 * (size_t)(r & ~kLeaf) : nodeBox + 6 * (size_t)r;
-            for (int k = 0; k < 6; k++) {
-                S v = ldcg_s<S>(src + k);
-                if (side == 0) b[k] = v;
-                else b[k] = (k < 3) ? (v < b[k] ? v : b[k]) : (v > b[k] ? v : b[k]);
-            }
+        uint2 cn = make_uint2(0u, 0u);
+        int upn = -1;
+        if (up >= 0) {
+            cn = child[up];
+            upn = parent[up];
         }
-        for (int k = 0; k < 6; k++) nodeBox[6 * (size_t)node + k] = b[k];
-        node = parent[node];
+        const uint32_t sib = c.x == self ? c.y : c.x;
+        const S* src = (sib & kLeaf) ? leafBox + 6 * (size_t)(sib & ~kLeaf) : nodeBox + 6 * (size_t)sib;
+        S o[6];
+        load_box_cg(src, o);
+        for (int k = 0; k < 3; k++) {
+            b[k] = o[k] < b[k] ? o[k] : b[k];
+            b[3 + k] = o[3 + k] > b[3 + k] ? o[3 + k] : b[3 + k];
+        }
+        store_box(nodeBox + 6 * (size_t)node, b);
+        if (up < 0) return;
+        self = (uint32_t)node;
+        node = up;
+        c = cn;
+        up = upn;
     }
 }
 
@@ -393,8 +463,9 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaMemPool_t pool, cudaStream_
     GI_TRY(cudaMemcpyAsync(cb, cbinit, sizeof(cbinit), cudaMemcpyHostToDevice, st));
     int tb = 256;
     int gb = (int)((n + tb - 1) / tb);
-    // a few blocks per SM, each looping: the centroid bounds take one set of atomics per block
-    k_tri_boxes<<<gb < 1184 ? gb : 1184, kTriBoxThreads, 0, st>>>(m.verts, m.tris, n, box, box64, cb);
+    // four resident blocks per SM, each looping: the centroid bounds take one set of atomics per block
+    const int gboxes = (int)((n + 2 * kTriBoxThreads - 1) / (2 * kTriBoxThreads));
+    k_tri_boxes<<<gboxes < 592 ? gboxes : 592, kTriBoxThreads, 0, st>>>(m.verts, m.tris, n, box, box64, cb);
     k_morton<<<gb, tb, 0, st>>>(box, n, cb, k0, v0);
     radix_sort<uint32_t, kMortonDigit>(k0, v0, k1, v1, n, 30, counts, stemp, st);
     // leaves in sorted order
