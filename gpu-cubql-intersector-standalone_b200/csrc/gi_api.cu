@@ -124,6 +124,8 @@ extern "C" gi_status gi_destroy(gi_ctx* c)
     cudaSetDevice(c->device);
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->st2) cudaStreamSynchronize(c->st2);
+    for (auto& sg : c->stage) sg.release();
+    c->copy_pool.reset();
     if (c->d_cnt) cudaFree(c->d_cnt);
     if (c->d_jobs) cudaFree(c->d_jobs);
     void* pooled[] = {c->queue, c->qflag,     c->cand,         c->cflag,   c->res,
@@ -232,6 +234,45 @@ static gi_status mesh_alloc(gi_ctx* c, uint32_t nv, uint32_t nt, gi_mesh** pm, c
     return GI_OK;
 }
 
+// Host -> device copy on stream st.  Pinned sources go straight to the DMA
+// engine.  A large pageable source would be staged by the driver on the
+// calling thread at about a third of the link rate; instead the context's
+// copy helpers fill one pinned chunk while the DMA of the previous one runs.
+// Returns when the source may be reused (like a pageable cudaMemcpyAsync).
+static cudaError_t h2d(gi_ctx* c, void* dst, const void* src, size_t bytes, cudaStream_t st)
+{
+    if (bytes < 2 * Staging::kChunk) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, src) != cudaSuccess) {
+        cudaGetLastError();  // an unknown pointer is ordinary host memory
+        a.type = cudaMemoryTypeUnregistered;
+    }
+    if (a.type != cudaMemoryTypeUnregistered)
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+    Staging& sg = c->stage[st == c->st2 ? 1 : 0];
+    cudaError_t e = sg.init();
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+    }
+    std::call_once(c->copy_pool_once, [c] {
+        const unsigned hw = std::thread::hardware_concurrency();
+        c->copy_pool.reset(new CopyPool(hw >= 16 ? 7u : hw >= 4 ? hw / 2 - 1 : 0u));
+    });
+    size_t k = 0;
+    for (size_t off = 0; off < bytes; off += Staging::kChunk, k++) {
+        const int slot = (int)(k & 1);
+        const size_t n = bytes - off < Staging::kChunk ? bytes - off : Staging::kChunk;
+        e = cudaEventSynchronize(sg.ev[slot]);  // the slot's previous DMA is done
+        if (e != cudaSuccess) return e;
+        c->copy_pool->copy(sg.buf[slot], static_cast<const char*>(src) + off, n);
+        e = cudaMemcpyAsync(static_cast<char*>(dst) + off, sg.buf[slot], n, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaEventRecord(sg.ev[slot], st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 // Host arrays -> device mesh with its BVH, on stream st (the caller holds c->mu).
 static gi_status mesh_upload_on(gi_ctx* c, const double* verts, uint32_t nv, const uint32_t* tris, uint32_t nt,
                                 gi_mesh** out, cudaStream_t st, const UploadSink& sk)
@@ -240,9 +281,8 @@ static gi_status mesh_upload_on(gi_ctx* c, const double* verts, uint32_t nv, con
     gi_status s = mesh_alloc(c, nv, nt, &m, st, sk);
     if (s != GI_OK) return s;
     cudaError_t e = cudaSuccess;
-    if (nv) e = cudaMemcpyAsync(m->b.verts, verts, sizeof(double) * 3 * (size_t)nv, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && nt)
-        e = cudaMemcpyAsync(m->b.tris, tris, sizeof(uint32_t) * 3 * (size_t)nt, cudaMemcpyHostToDevice, st);
+    if (nv) e = h2d(c, m->b.verts, verts, sizeof(double) * 3 * (size_t)nv, st);
+    if (e == cudaSuccess && nt) e = h2d(c, m->b.tris, tris, sizeof(uint32_t) * 3 * (size_t)nt, st);
     if (e != cudaSuccess) {
         cudaStreamSynchronize(st);
         mesh_free(c, m, st);

@@ -2,11 +2,15 @@
 // (shared by the translation units that implement the C ABI).
 #pragma once
 #include <atomic>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
-#include <cstdio>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "gi/gi.h"
@@ -26,6 +30,140 @@ struct gi_mesh {
 // from its context's pool; the results of that call point into it (no further
 // copy) and the block goes back to the pool when the last of them is freed,
 // even after the context itself is gone.
+// Host threads that split large memcpys into parts; the calling thread works
+// on its own job too.  Several callers may copy at once (the two meshes of a
+// one-shot call): each job is queued, helpers take its parts in turn.
+class CopyPool {
+public:
+    explicit CopyPool(unsigned helpers)
+    {
+        for (unsigned i = 0; i < helpers; i++) th_.emplace_back([this] { work(); });
+    }
+    ~CopyPool()
+    {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : th_) t.join();
+    }
+    CopyPool(const CopyPool&) = delete;
+    CopyPool& operator=(const CopyPool&) = delete;
+
+    void copy(void* dst, const void* src, size_t bytes)
+    {
+        constexpr size_t kPart = (size_t)1 << 20;
+        Job j{static_cast<char*>(dst), static_cast<const char*>(src), bytes, kPart, (unsigned)((bytes + kPart - 1) / kPart)};
+        if (j.parts <= 1 || th_.empty()) {
+            std::memcpy(dst, src, bytes);
+            return;
+        }
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            q_.push_back(&j);
+        }
+        cv_.notify_all();
+        // the caller takes parts as well
+        for (;;) {
+            unsigned part;
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                if (j.next >= j.parts) break;
+                part = claim(&j);
+            }
+            run(&j, part);
+            std::lock_guard<std::mutex> lk(mu_);
+            j.done++;
+        }
+        std::unique_lock<std::mutex> lk(mu_);
+        done_.wait(lk, [&] { return j.done == j.parts; });
+    }
+
+private:
+    struct Job {
+        char* dst;
+        const char* src;
+        size_t bytes, part_bytes;
+        unsigned parts;
+        unsigned next = 0, done = 0;  // guarded by mu_
+    };
+    // takes the next part of j (mu_ held); the job leaves the queue with its last part
+    unsigned claim(Job* j)
+    {
+        const unsigned part = j->next++;
+        if (j->next == j->parts)
+            for (auto it = q_.begin(); it != q_.end(); ++it)
+                if (*it == j) {
+                    q_.erase(it);
+                    break;
+                }
+        return part;
+    }
+    static void run(Job* j, unsigned part)
+    {
+        const size_t off = (size_t)part * j->part_bytes;
+        const size_t n = j->bytes - off < j->part_bytes ? j->bytes - off : j->part_bytes;
+        std::memcpy(j->dst + off, j->src + off, n);
+    }
+    void work()
+    {
+        for (;;) {
+            Job* j;
+            unsigned part;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return stop_ || !q_.empty(); });
+                if (stop_) return;
+                j = q_.front();
+                part = claim(j);
+            }
+            run(j, part);
+            {
+                // the job is not touched after this: its owner returns once done == parts
+                std::lock_guard<std::mutex> lk(mu_);
+                j->done++;
+            }
+            done_.notify_all();
+        }
+    }
+    std::mutex mu_;
+    std::condition_variable cv_, done_;
+    std::deque<Job*> q_;
+    std::vector<std::thread> th_;
+    bool stop_ = false;
+};
+
+// Pinned chunks through which pageable host arrays are copied to the device:
+// helpers fill one chunk while the DMA of the other runs.
+struct Staging {
+    static constexpr size_t kChunk = (size_t)4 << 20;
+    void* buf[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    bool ready = false;
+    cudaError_t init()
+    {
+        if (ready) return cudaSuccess;
+        for (int i = 0; i < 2; i++) {
+            cudaError_t e = cudaMallocHost(&buf[i], kChunk);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+            if (e != cudaSuccess) return e;
+        }
+        ready = true;
+        return cudaSuccess;
+    }
+    void release()
+    {
+        for (int i = 0; i < 2; i++) {
+            if (ev[i]) cudaEventSynchronize(ev[i]), cudaEventDestroy(ev[i]);
+            if (buf[i]) cudaFreeHost(buf[i]);
+            ev[i] = nullptr;
+            buf[i] = nullptr;
+        }
+        ready = false;
+    }
+};
+
 struct PinnedPool;
 struct PinnedBuf {
     void* p = nullptr;
@@ -168,6 +306,9 @@ struct gi_ctx {
     int device = 0;
     cudaStream_t st = nullptr;
     cudaStream_t st2 = nullptr;  // second mesh of a one-shot call builds here, concurrently with the first
+    std::unique_ptr<CopyPool> copy_pool;  // created with the first staged upload
+    std::once_flag copy_pool_once;
+    Staging stage[2];                     // per upload stream (st, st2)
     cudaMemPool_t pool = nullptr;  // stream-ordered allocations of this context
     gi::LaunchCfg cfg;
     uint64_t budget = 0;
