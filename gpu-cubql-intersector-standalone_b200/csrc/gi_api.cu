@@ -663,16 +663,31 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         CK(c, cudaEventRecord(c->ev[1], c->st), "event");
         CK(c, launch_exact(b, c->cfg, c->st), "exact stage");
         CK(c, cudaEventRecord(c->ev[2], c->st), "event");
-        if (want_segs) CK(c, launch_segments(b, c->segs, c->nseg, c->cfg, c->st), "segments");
-        CK(c, cudaEventRecord(c->ev[3], c->st), "event");
-        if (small_order)
-            CK(c, launch_order_small(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
-                                     c->segpair_out, want_segs, c->st),
+        if (small_order && want_segs && sort) {
+            // the segments are built on the second stream while the ordering
+            // ranks the results; only the placing launch waits for them
+            CK(c, cudaStreamWaitEvent(c->st2, c->ev[2], 0), "event");
+            CK(c, launch_segments(b, c->segs, c->nseg, c->cfg, c->st2), "segments");
+            CK(c, cudaEventRecord(c->ev[3], c->st2), "event");
+            CK(c, launch_order_small_phases(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
+                                            c->segpair_out, want_segs, kOrderRank, c->st),
                "ordering");
-        else
-            CK(c, launch_order_gather(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
-                                      c->segpair_out, want_segs, c->cfg, c->st),
+            CK(c, cudaStreamWaitEvent(c->st, c->ev[3], 0), "event");
+            CK(c, launch_order_small_phases(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
+                                            c->segpair_out, want_segs, kOrderPlace, c->st),
                "ordering");
+        } else {
+            if (want_segs) CK(c, launch_segments(b, c->segs, c->nseg, c->cfg, c->st), "segments");
+            CK(c, cudaEventRecord(c->ev[3], c->st), "event");
+            if (small_order)
+                CK(c, launch_order_small(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
+                                         c->segpair_out, want_segs, c->st),
+                   "ordering");
+            else
+                CK(c, launch_order_gather(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
+                                          c->segpair_out, want_segs, c->cfg, c->st),
+                   "ordering");
+        }
         CK(c, cudaEventRecord(c->ev[4], c->st), "event");
         // speculative copy at the previous call's size
         uint32_t pp = std::min<uint32_t>(cap, (uint32_t)std::min<uint64_t>(c->pred_pairs + c->pred_pairs / 4 + 1024,

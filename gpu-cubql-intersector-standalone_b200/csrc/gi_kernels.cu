@@ -1805,6 +1805,10 @@ cudaError_t launch_order_gather(const Bufs& b, const OrderBufs& O, bool sort, co
 // blocks are co-resident, and every barrier wait is bounded all the same.
 // ---------------------------------------------------------------------------
 constexpr int kOrderSmallThreads = kOrderSmallRun;  // one key per thread
+// lower-bound steps over a run: 2^(steps-1) < kOrderSmallRun + 1 <= 2^steps
+constexpr int kOrderSearchSteps = 11;
+static_assert((1 << (kOrderSearchSteps - 1)) < kOrderSmallRun + 1 && kOrderSmallRun + 1 <= (1 << kOrderSearchSteps),
+              "search steps must cover a run");
 constexpr size_t kOrderSmallDyn = sizeof(unsigned long long) * kOrderSmallMax;  // all runs, phase 2
 
 // Arrive at grid barrier `k` (1-based) of the launch; waits bounded.  On a spent
@@ -1833,7 +1837,7 @@ __device__ __forceinline__ void grid_barrier(unsigned* ctr, unsigned k, unsigned
 __global__ void __launch_bounds__(kOrderSmallThreads, 1)
     k_order_small(Bufs B, OrderBufs O, const double* __restrict__ segs, const uint32_t* __restrict__ nseg,
                   int32_t* pairs_out, uint32_t* job_out, double* segs_out, int32_t* segpair_out, int want_segments,
-                  int sorted)
+                  int sorted, unsigned phases, unsigned bar0)
 {
     extern __shared__ unsigned long long allk[];  // every sorted run (phase 2)
     __shared__ unsigned long long sk[kOrderSmallRun];
@@ -1853,8 +1857,8 @@ __global__ void __launch_bounds__(kOrderSmallThreads, 1)
     const unsigned base = t * kOrderSmallRun;
     const unsigned len = t < nruns ? min((unsigned)kOrderSmallRun, n - base) : 0u;
     uint32_t* perm = O.vals[1];
-    unsigned bar = 0;
-    if (sorted) {
+    unsigned bar = bar0;  // grid barriers already passed by an earlier launch of this call
+    if (sorted && (phases & kOrderRank)) {
         // ---- phase 1: sort this block's run (padding keys sort last) ----
         unsigned long long key = tid < len ? order_key(__ldcg(B.res + base + tid), O) : ~0ull;
         uint32_t val = tid < len ? base + tid : 0xffffffffu;
@@ -1911,7 +1915,7 @@ __global__ void __launch_bounds__(kOrderSmallThreads, 1)
                 }
 #pragma unroll
                 for (int r = 0; r < 4; r++) pos -= lo[r];  // counts are relative to each run's start
-                for (int step = 0; step < 10; step++) {  // 2^9 < kOrderSmallRun + 1 <= 2^10
+                for (int step = 0; step < kOrderSearchSteps; step++) {
 #pragma unroll
                     for (int r = 0; r < 4; r++) {
                         if (lo[r] < hi[r]) {
@@ -1928,6 +1932,7 @@ __global__ void __launch_bounds__(kOrderSmallThreads, 1)
         }
         grid_barrier(&C->obar, ++bar, &C->err, &s_ok);
     }
+    if (!(phases & kOrderPlace)) return;
     // ---- phase 3: gather pairs, place segments (one sorted position per thread) ----
     const unsigned k = base + tid;
     const bool ok = tid < len;
@@ -1965,6 +1970,17 @@ cudaError_t launch_order_small(const Bufs& b, const OrderBufs& O, bool sort, con
                                const uint32_t* nseg, int32_t* pairs_out, uint32_t* job_out, double* segs_out,
                                int32_t* segpair_out, bool want_segments, cudaStream_t st)
 {
+    return launch_order_small_phases(b, O, sort, segs, nseg, pairs_out, job_out, segs_out, segpair_out,
+                                     want_segments, kOrderRank | kOrderPlace, st);
+}
+
+cudaError_t launch_order_small_phases(const Bufs& b, const OrderBufs& O, bool sort, const double* segs,
+                                      const uint32_t* nseg, int32_t* pairs_out, uint32_t* job_out, double* segs_out,
+                                      int32_t* segpair_out, bool want_segments, unsigned phases, cudaStream_t st)
+{
+    if (!sort) phases &= ~kOrderRank;  // nothing to rank: results keep their order
+    if (!phases) return cudaSuccess;
+    const size_t dyn = (phases & kOrderRank) ? kOrderSmallDyn : 0;
     cudaError_t e = cudaFuncSetAttribute((const void*)k_order_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)kOrderSmallDyn);
     if (e != cudaSuccess) return e;
@@ -1973,9 +1989,12 @@ cudaError_t launch_order_small(const Bufs& b, const OrderBufs& O, bool sort, con
     const double* a_segs = segs;
     const uint32_t* a_nseg = nseg;
     int ws = want_segments ? 1 : 0, so = sort ? 1 : 0;
-    void* args[] = {&bb, &oo, &a_segs, &a_nseg, &pairs_out, &job_out, &segs_out, &segpair_out, &ws, &so};
+    // the ranking phases pass two grid barriers; a placing launch that follows
+    // a ranking launch of the same call counts its barrier after them
+    unsigned ph = phases, b0 = (sort && !(phases & kOrderRank)) ? 2u : 0u;
+    void* args[] = {&bb, &oo, &a_segs, &a_nseg, &pairs_out, &job_out, &segs_out, &segpair_out, &ws, &so, &ph, &b0};
     e = cudaLaunchCooperativeKernel((const void*)k_order_small, dim3(kOrderSmallBlocks), dim3(kOrderSmallThreads),
-                                    args, kOrderSmallDyn, st);
+                                    args, dyn, st);
     note_launches(1);
     return e;
 }

@@ -97,12 +97,20 @@ cudaError_t launch_order_gather(const Bufs& b, const OrderBufs& O, bool sort, co
 // each sorting a run of kOrderSmallRun keys, for up to kOrderSmallMax results.
 // If the call produced more, the kernel only sets Counters::order_redo and the
 // caller reruns with launch_order_gather.  Keys must fit in 63 bits.
-constexpr int kOrderSmallRun = 512;
-constexpr int kOrderSmallBlocks = 48;
+constexpr int kOrderSmallRun = 1024;
+constexpr int kOrderSmallBlocks = 24;
 constexpr uint32_t kOrderSmallMax = (uint32_t)kOrderSmallRun * kOrderSmallBlocks;
 cudaError_t launch_order_small(const Bufs& b, const OrderBufs& O, bool sort, const double* segs,
                                const uint32_t* nseg, int32_t* pairs_out, uint32_t* job_out, double* segs_out,
                                int32_t* segpair_out, bool want_segments, cudaStream_t st);
+// The same in two launches: kOrderRank (sort the runs, rank every key) needs
+// only the final result list; kOrderPlace (gather the pairs, place the
+// segments) needs the segments too, so the ranking can run while the segments
+// are built on another stream.
+constexpr unsigned kOrderRank = 1u, kOrderPlace = 2u;
+cudaError_t launch_order_small_phases(const Bufs& b, const OrderBufs& O, bool sort, const double* segs,
+                                      const uint32_t* nseg, int32_t* pairs_out, uint32_t* job_out, double* segs_out,
+                                      int32_t* segpair_out, bool want_segments, unsigned phases, cudaStream_t st);
 // Number of kernels launched by the launchers of this library (monotonic).
 unsigned long long launch_count();
 void note_launches(unsigned n);

@@ -129,7 +129,8 @@ typedef struct {
     double ms_traverse;               /* device time: traversal + first filter */
     double ms_exact;                  /* device time: FP64 / exact stage */
     double ms_segments;               /* device time: segment construction */
-    double ms_sort;                   /* device time: output ordering */
+    double ms_sort;                   /* device time: output ordering (the part after segment construction
+                                         ends; ranking overlaps the segments) */
     double ms_total;                  /* device time of the whole call */
 } gi_stats;
 
