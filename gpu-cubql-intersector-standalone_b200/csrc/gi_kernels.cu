@@ -1805,10 +1805,6 @@ cudaError_t launch_order_gather(const Bufs& b, const OrderBufs& O, bool sort, co
 // blocks are co-resident, and every barrier wait is bounded all the same.
 // ---------------------------------------------------------------------------
 constexpr int kOrderSmallThreads = kOrderSmallRun;  // one key per thread
-// lower-bound steps over a run: 2^(steps-1) < kOrderSmallRun + 1 <= 2^steps
-constexpr int kOrderSearchSteps = 11;
-static_assert((1 << (kOrderSearchSteps - 1)) < kOrderSmallRun + 1 && kOrderSmallRun + 1 <= (1 << kOrderSearchSteps),
-              "search steps must cover a run");
 constexpr size_t kOrderSmallDyn = sizeof(unsigned long long) * kOrderSmallMax;  // all runs, phase 2
 
 // Arrive at grid barrier `k` (1-based) of the launch; waits bounded.  On a spent
@@ -1902,33 +1898,74 @@ __global__ void __launch_bounds__(kOrderSmallThreads, 1)
         if ((n & 1u) && tid == 0) allk[n - 1u] = __ldcg(O.keys[0] + (n - 1u));
         asm volatile("cp.async.wait_all;\n" ::: "memory");
         __syncthreads();
-        if (tid < len) {
+        // A warp's keys are consecutive in its sorted run, so in another run
+        // their lower bounds lie between those of its first and its last key.
+        // Two lanes per run find that bracket (four runs at once); every lane
+        // then counts the keys below its own inside the bracket, held in the
+        // warp's registers and searched with shuffles, or (a bracket wider
+        // than two chunks) with its own search of the bracket.
+        const unsigned lane = tid & 31u, wbase = tid & ~31u;
+        if (wbase < len) {  // warp-uniform
+            const unsigned wlast = min(len - wbase, 32u) - 1u;  // the warp's last key
+            const unsigned long long kf = __shfl_sync(0xffffffffu, key, 0);
+            const unsigned long long kl = __shfl_sync(0xffffffffu, key, wlast);
             unsigned pos = tid;
             for (unsigned s0 = 0; s0 < nruns; s0 += 4) {
-                unsigned lo[4], hi[4];
-#pragma unroll
-                for (int r = 0; r < 4; r++) {
-                    const unsigned s = s0 + r;
-                    lo[r] = s * kOrderSmallRun;
-                    hi[r] = (s < nruns && s != t) ? lo[r] + min((unsigned)kOrderSmallRun, n - s * kOrderSmallRun)
-                                                  : lo[r];
-                }
-#pragma unroll
-                for (int r = 0; r < 4; r++) pos -= lo[r];  // counts are relative to each run's start
-                for (int step = 0; step < kOrderSearchSteps; step++) {
-#pragma unroll
-                    for (int r = 0; r < 4; r++) {
-                        if (lo[r] < hi[r]) {
-                            const unsigned mid = (lo[r] + hi[r]) >> 1;
-                            if (allk[mid] < key) lo[r] = mid + 1u;
-                            else hi[r] = mid;
-                        }
+                // lanes 2r and 2r + 1: lower bounds of the first and last key in run s0 + r
+                unsigned a = 0, b = 0;
+                if (lane < 8u) {
+                    const unsigned sr = s0 + (lane >> 1);
+                    if (sr < nruns && sr != t) {
+                        a = sr * kOrderSmallRun;
+                        b = a + min((unsigned)kOrderSmallRun, n - a);
+                    }
+                    const unsigned long long q = (lane & 1u) ? kl : kf;
+                    while (a < b) {
+                        const unsigned mid = (a + b) >> 1;
+                        if (allk[mid] < q) a = mid + 1u;
+                        else b = mid;
                     }
                 }
 #pragma unroll
-                for (int r = 0; r < 4; r++) pos += lo[r];
+                for (unsigned r = 0; r < 4u; r++) {
+                    const unsigned sr = s0 + r;
+                    if (sr >= nruns || sr == t) continue;  // warp-uniform
+                    const unsigned L = sr * kOrderSmallRun;
+                    const unsigned lo = __shfl_sync(0xffffffffu, a, 2u * r);
+                    const unsigned hi = __shfl_sync(0xffffffffu, a, 2u * r + 1u);
+                    unsigned c = 0;
+                    if (hi - lo <= 64u) {
+                        for (unsigned w0 = lo; w0 < hi; w0 += 32u) {
+                            const unsigned cnt = min(32u, hi - w0);
+                            const unsigned long long v = lane < cnt ? allk[w0 + lane] : ~0ull;
+                            unsigned first = 0, count = cnt;  // lower bound of key among v[0 .. cnt)
+                            for (int st = 0; st < 6; st++) {  // 2^5 < 32 + 1 <= 2^6
+                                const unsigned half = count >> 1;
+                                const unsigned long long vm = __shfl_sync(0xffffffffu, v, (first + half) & 31u);
+                                if (count > 0u) {
+                                    if (vm < key) {
+                                        first += half + 1u;
+                                        count -= half + 1u;
+                                    } else {
+                                        count = half;
+                                    }
+                                }
+                            }
+                            c += first;
+                        }
+                    } else {
+                        unsigned x = lo, y = hi;
+                        while (x < y) {
+                            const unsigned mid = (x + y) >> 1;
+                            if (allk[mid] < key) x = mid + 1u;
+                            else y = mid;
+                        }
+                        c = x - lo;
+                    }
+                    pos += lo - L + c;
+                }
             }
-            if (pos < n) perm[pos] = val;
+            if (lane <= wlast && pos < n) perm[pos] = val;
         }
         grid_barrier(&C->obar, ++bar, &C->err, &s_ok);
     }
