@@ -174,7 +174,12 @@ struct PinnedBuf {
 struct PinnedPool {
     std::mutex mu;
     std::vector<PinnedBuf*> free_list;
-    static constexpr size_t kKeepFree = 4;  // blocks kept for reuse; more are released
+    size_t free_bytes = 0;
+    // free blocks kept for reuse up to this many bytes; beyond it the smallest
+    // are released.  Pinning and unpinning cost milliseconds and cudaFreeHost
+    // waits for the device, so a serving loop whose round sizes vary must not
+    // release and allocate blocks on every round.
+    static constexpr size_t kKeepFreeBytes = (size_t)512 << 20;
     ~PinnedPool()
     {
         for (PinnedBuf* b : free_list) {
@@ -194,12 +199,15 @@ struct PinnedPool {
             if (best != free_list.size()) {
                 PinnedBuf* b = free_list[best];
                 free_list.erase(free_list.begin() + (long)best);
+                free_bytes -= b->bytes;
                 return b;
             }
         }
         PinnedBuf* b = new (std::nothrow) PinnedBuf();
         if (!b) return nullptr;
-        const size_t want = bytes + bytes / 4 > ((size_t)1 << 20) ? bytes + bytes / 4 : ((size_t)1 << 20);
+        // power-of-two sizes (at least 1 MB): a block serves later results of similar size
+        size_t want = (size_t)1 << 20;
+        while (want < bytes) want <<= 1;
         if (cudaMallocHost(&b->p, want) != cudaSuccess) {
             delete b;
             return nullptr;
@@ -209,21 +217,23 @@ struct PinnedPool {
     }
     void put(PinnedBuf* b)
     {
-        PinnedBuf* drop = nullptr;
+        std::vector<PinnedBuf*> drop;
         {
             std::lock_guard<std::mutex> lk(mu);
             free_list.push_back(b);
-            if (free_list.size() > kKeepFree) {  // release the smallest
+            free_bytes += b->bytes;
+            while (free_bytes > kKeepFreeBytes && free_list.size() > 1) {  // release the smallest
                 size_t k = 0;
                 for (size_t i = 1; i < free_list.size(); i++)
                     if (free_list[i]->bytes < free_list[k]->bytes) k = i;
-                drop = free_list[k];
+                free_bytes -= free_list[k]->bytes;
+                drop.push_back(free_list[k]);
                 free_list.erase(free_list.begin() + (long)k);
             }
         }
-        if (drop) {
-            cudaFreeHost(drop->p);
-            delete drop;
+        for (PinnedBuf* d : drop) {
+            cudaFreeHost(d->p);
+            delete d;
         }
     }
 };
