@@ -488,6 +488,7 @@ MeshDev mesh_dev(const gi_mesh* m)
     d.cutBox = m->b.cutBox;
     d.cutBox64 = m->b.cutBox64;
     d.ncut = m->b.ncut;
+    d.ncut4 = m->b.ncut4;
     d.root = m->b.root;
     d.nv = m->b.nv;
     d.nt = m->b.nt;
@@ -657,6 +658,10 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         b.cnt = c->d_cnt;
         b.precision = prec;
         b.two_frame = nj > 1 ? 1 : 0;
+        // one pair: skip the narrowest level by seeding from the depth-4 cuts
+        // (up to 256 x 256 seed tests); a batch keeps the depth-3 cuts, whose
+        // seed tests grow with the number of jobs
+        b.deep_seed = nj == 1 ? 1 : 0;
         CK(c, cudaMemsetAsync(c->d_cnt, 0, sizeof(Counters), c->st), "counters");
         CK(c, cudaEventRecord(c->ev[0], c->st), "event");
         CK(c, launch_traverse(b, c->cfg, prec, trav_shape(shape), c->st), "traverse");

@@ -59,16 +59,20 @@ struct MeshDev {
     const double* leafBox64;
     const WNode* nodes;
     const WNode64* nodes64;
-    const uint32_t* cutRef;  // depth-3 cut: node / leaf refs whose subtrees cover all leaves
+    // cuts: node / leaf refs whose subtrees cover all leaves, the depth-3 cut in
+    // entries [0, kCutMax) and the depth-4 cut in [kCutMax, kCutMax + kCut4Max)
+    const uint32_t* cutRef;
     const float* cutBox;     // their boxes (6 floats each)
-    const double* cutBox64;  // FP64 boxes of the same cut (FP64 form)
+    const double* cutBox64;  // FP64 boxes of the same cuts (FP64 form)
     uint32_t root;  // wide node index, or kLeaf | leaf position when nt == 1
     uint32_t nv, nt, nnodes;
-    uint32_t ncut;
-    uint32_t pad_;
+    uint32_t ncut;   // entries of the depth-3 cut
+    uint32_t ncut4;  // entries of the depth-4 cut
 };
 
-constexpr int kCutMax = 64;  // 4^3
+constexpr int kCutMax = 64;    // 4^3
+constexpr int kCut4Max = 256;  // 4^4
+constexpr int kCutCap = kCutMax + kCut4Max;
 
 struct JobDev {
     MeshDev A, B;
@@ -128,6 +132,7 @@ struct Bufs {
     unsigned tag;     // nonzero, different for every call on the context
     int precision;    // 0 FP32 cascade, 1 FP64
     int two_frame;    // also test child boxes in B's own frame (fewer pairs, more work per pair)
+    int deep_seed;    // seed from the depth-4 cuts (single-pair calls) instead of the depth-3 cuts
 };
 
 }  // namespace gi

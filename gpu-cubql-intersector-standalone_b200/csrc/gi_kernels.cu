@@ -361,58 +361,82 @@ __global__ void k_collapse(int n, const uint2* __restrict__ child, const uint32_
     nodes[widx[i]] = out;
 }
 
-// Depth-3 cut of the wide BVH: the root expanded three times (leaves met on the
-// way are kept), with each entry's box from its parent's child slot.  At most
-// 4^3 = 64 entries; the traversal starts from all pairs of the two cuts.
+// Cuts of the wide BVH: the root expanded three and four times (leaves met on
+// the way are kept), each entry's box from its parent's child slot.  One block
+// expands a level at a time, an entry per thread, the children placed by a
+// block scan, so entries keep the order of a sequential expansion.  Output:
+// the depth-3 cut (at most 4^3 entries) at [0, kCutMax), the depth-4 cut (at
+// most 4^4) at [kCutMax, kCutCap); ncut[0], ncut[1] their sizes.  The
+// traversal starts from all pairs of two meshes' cuts.
+constexpr int kCutThreads = kCut4Max;
 template <class S, class NodeT>
-__global__ void k_cut(const NodeT* __restrict__ nodes, const S* __restrict__ leafBox, uint32_t root,
-                      uint32_t* __restrict__ cutRef, S* __restrict__ cutBox, uint32_t* __restrict__ ncut)
+__global__ void __launch_bounds__(kCutThreads) k_cut(const NodeT* __restrict__ nodes, const S* __restrict__ leafBox,
+                                                     uint32_t root, uint32_t* __restrict__ cutRef,
+                                                     S* __restrict__ cutBox, uint32_t* __restrict__ ncut)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    uint32_t r[kCutMax], r2[kCutMax];
-    S b[kCutMax][6], b2[kCutMax][6];
-    int n = 0;
+    __shared__ uint32_t r[2][kCut4Max];
+    __shared__ S b[2][kCut4Max][6];
+    __shared__ uint32_t sw[33];
+    const unsigned tid = threadIdx.x;
     if (root & kLeaf) {
-        r[0] = root;
-        for (int k = 0; k < 6; k++) b[0][k] = leafBox[6 * (size_t)(root & ~kLeaf) + k];
-        n = 1;
-    } else {
-        r[0] = root;
-        n = 1;
-        for (int depth = 0; depth < 3; depth++) {
-            int m = 0;
-            for (int e = 0; e < n; e++) {
-                if (r[e] & kLeaf) {
-                    r2[m] = r[e];
-                    for (int k = 0; k < 6; k++) b2[m][k] = b[e][k];
-                    m++;
-                    continue;
-                }
-                const NodeT& nd = nodes[r[e]];
+        if (tid == 0) {
+            for (int c = 0; c < 2; c++) {
+                const unsigned o = c ? kCutMax : 0u;
+                cutRef[o] = root;
+                for (int k = 0; k < 6; k++) cutBox[6 * o + k] = leafBox[6 * (size_t)(root & ~kLeaf) + k];
+            }
+            ncut[0] = ncut[1] = 1u;
+        }
+        return;
+    }
+    if (tid == 0) r[0][0] = root;  // the root's own box is never used: it is expanded first
+    __syncthreads();
+    unsigned n = 1, cur = 0;
+    for (int depth = 1; depth <= 4; depth++) {
+        // n <= 4^(depth-1) <= kCutThreads: one entry per thread
+        const uint32_t ref = tid < n ? r[cur][tid] : kLeaf;
+        const bool node = tid < n && !(ref & kLeaf);
+        unsigned cnt = 0;
+        if (tid < n) {
+            if (!node) cnt = 1;
+            else
+                for (int c = 0; c < 4; c++) cnt += nodes[ref].child[c] != kEmpty;
+        }
+        unsigned tot;
+        const unsigned ex = block_exclusive_scan(cnt, sw, &tot);
+        const unsigned nx = cur ^ 1u;
+        if (tid < n) {
+            if (!node) {
+                r[nx][ex] = ref;
+                for (int k = 0; k < 6; k++) b[nx][ex][k] = b[cur][tid][k];
+            } else {
+                const NodeT& nd = nodes[ref];
+                unsigned m = ex;
                 for (int c = 0; c < 4; c++) {
                     if (nd.child[c] == kEmpty) continue;
-                    r2[m] = nd.child[c];
-                    b2[m][0] = nd.lox[c];
-                    b2[m][1] = nd.loy[c];
-                    b2[m][2] = nd.loz[c];
-                    b2[m][3] = nd.hix[c];
-                    b2[m][4] = nd.hiy[c];
-                    b2[m][5] = nd.hiz[c];
+                    r[nx][m] = nd.child[c];
+                    b[nx][m][0] = nd.lox[c];
+                    b[nx][m][1] = nd.loy[c];
+                    b[nx][m][2] = nd.loz[c];
+                    b[nx][m][3] = nd.hix[c];
+                    b[nx][m][4] = nd.hiy[c];
+                    b[nx][m][5] = nd.hiz[c];
                     m++;
                 }
             }
-            n = m;
-            for (int e = 0; e < n; e++) {
-                r[e] = r2[e];
-                for (int k = 0; k < 6; k++) b[e][k] = b2[e][k];
+        }
+        __syncthreads();
+        n = tot;
+        cur = nx;
+        if (depth >= 3) {
+            const unsigned o = depth == 3 ? 0u : (unsigned)kCutMax;
+            for (unsigned e = tid; e < n; e += kCutThreads) {
+                cutRef[o + e] = r[cur][e];
+                for (int k = 0; k < 6; k++) cutBox[6 * (o + e) + k] = b[cur][e][k];
             }
+            if (tid == 0) ncut[depth - 3] = n;
         }
     }
-    for (int e = 0; e < n; e++) {
-        cutRef[e] = r[e];
-        for (int k = 0; k < 6; k++) cutBox[6 * e + k] = b[e][k];
-    }
-    *ncut = (uint32_t)n;
 }
 
 cudaError_t launch_validate(const double* verts, uint32_t nv, const uint32_t* tris, uint32_t nt, unsigned* d_err,
@@ -514,23 +538,25 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaMemPool_t pool, cudaStream_
         m.nnodes = nw;
         m.root = 0;
     }
-    // depth-3 cut (refs shared by both precisions; boxes per precision)
+    // depth-3 and depth-4 cuts (refs shared by both precisions; boxes per precision)
     {
         uint32_t* d_n = nullptr;
-        GI_TRY(pool_alloc(&d_n, sizeof(uint32_t), pool, st));
-        if (!m.cutRef) GI_TRY(pool_alloc(&m.cutRef, sizeof(uint32_t) * kCutMax, pool, st));
+        GI_TRY(pool_alloc(&d_n, sizeof(uint32_t) * 2, pool, st));
+        if (!m.cutRef) GI_TRY(pool_alloc(&m.cutRef, sizeof(uint32_t) * kCutCap, pool, st));
         if (!fp64) {
-            GI_TRY(pool_alloc(&m.cutBox, sizeof(float) * 6 * kCutMax, pool, st));
-            k_cut<float, WNode><<<1, 32, 0, st>>>(m.nodes, m.leafBox, m.root, m.cutRef, m.cutBox, d_n);
+            GI_TRY(pool_alloc(&m.cutBox, sizeof(float) * 6 * kCutCap, pool, st));
+            k_cut<float, WNode><<<1, kCutThreads, 0, st>>>(m.nodes, m.leafBox, m.root, m.cutRef, m.cutBox, d_n);
         } else {
-            GI_TRY(pool_alloc(&m.cutBox64, sizeof(double) * 6 * kCutMax, pool, st));
-            k_cut<double, WNode64><<<1, 32, 0, st>>>(m.nodes64, m.leafBox64, m.root, m.cutRef, m.cutBox64, d_n);
+            GI_TRY(pool_alloc(&m.cutBox64, sizeof(double) * 6 * kCutCap, pool, st));
+            k_cut<double, WNode64><<<1, kCutThreads, 0, st>>>(m.nodes64, m.leafBox64, m.root, m.cutRef,
+                                                               m.cutBox64, d_n);
         }
-        uint32_t hn = 0;
-        GI_TRY(cudaMemcpyAsync(&hn, d_n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        uint32_t hn[2] = {0, 0};
+        GI_TRY(cudaMemcpyAsync(hn, d_n, sizeof(uint32_t) * 2, cudaMemcpyDeviceToHost, st));
         GI_TRY(cudaStreamSynchronize(st));
         cudaFreeAsync(d_n, st);
-        m.ncut = hn;
+        m.ncut = hn[0];
+        m.ncut4 = hn[1];
     }
     GI_TRY(cudaGetLastError());
     cudaFreeAsync(box, st);
@@ -1078,7 +1104,13 @@ __device__ __forceinline__ unsigned take_ticket(unsigned* head)
     return __shfl_sync(0xffffffffu, b, 0);
 }
 
-// Seeds the queue: pair (i, j) of the depth-3 cut entries of every job.  Warps
+// Seed tests per job: every pair of the two meshes' cut entries.
+__device__ __forceinline__ unsigned seed_tests_per_job(const Bufs& B)
+{
+    return B.deep_seed ? (unsigned)kCut4Max * kCut4Max : (unsigned)kCutMax * kCutMax;
+}
+
+// Seeds the queue: pair (i, j) of the depth-3 (or depth-4) cut entries of every job.  Warps
 // claim chunks of 32 seed tests with one atomic, so only warps that run do the
 // work (nothing waits for a block that never becomes resident); seed_done
 // counts finished tests after their node pairs are counted in `work`.
@@ -1088,7 +1120,8 @@ __device__ __forceinline__ void seed_cut_pairs(const Bufs& B, unsigned total)
     using S = typename Prec<F64>::S;
     Counters* C = B.cnt;
     const unsigned lane = threadIdx.x & 31;
-    const unsigned per_job = (unsigned)kCutMax * kCutMax;
+    const unsigned per_job = seed_tests_per_job(B);
+    const unsigned coff = B.deep_seed ? (unsigned)kCutMax : 0u;  // the cut's first entry
     for (;;) {
         unsigned base = 0;
         if (lane == 0) base = atomicAdd(&C->seed_head, 32u);
@@ -1101,9 +1134,10 @@ __device__ __forceinline__ void seed_cut_pairs(const Bufs& B, unsigned total)
             job = g / per_job;
             const unsigned t = g % per_job;
             const JobDev& J = B.jobs[job];
-            const unsigned nA = (J.A.nt && J.B.nt) ? J.A.ncut : 0u, nB = J.B.ncut;
+            const unsigned nA = (J.A.nt && J.B.nt) ? (B.deep_seed ? J.A.ncut4 : J.A.ncut) : 0u;
+            const unsigned nB = B.deep_seed ? J.B.ncut4 : J.B.ncut;
             if (t < nA * nB) {
-                const unsigned i = t / nB, j = t % nB;
+                const unsigned i = coff + t / nB, j = coff + t % nB;
                 const S* ba_ = F64 ? (const S*)J.A.cutBox64 : (const S*)J.A.cutBox;
                 const S* bb_ = F64 ? (const S*)J.B.cutBox64 : (const S*)J.B.cutBox;
                 Box<S> ba, bb;
@@ -1200,7 +1234,7 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
     Counters* C = B.cnt;
     const unsigned lane = threadIdx.x & 31;
     uint4* S = stk[threadIdx.x >> 5];
-    const unsigned seed_total = B.njobs * (unsigned)(kCutMax * kCutMax);
+    const unsigned seed_total = B.njobs * seed_tests_per_job(B);
     seed_cut_pairs<F64>(B, seed_total);
     unsigned long long visited = 0, decided = 0, tested = 0;
     unsigned maxlev = 0, idle = 0, backoff = 32;

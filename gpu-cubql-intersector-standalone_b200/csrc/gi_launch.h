@@ -19,7 +19,7 @@ struct MeshBuffers {
     uint32_t* cutRef = nullptr;
     float* cutBox = nullptr;
     double* cutBox64 = nullptr;
-    uint32_t nv = 0, nt = 0, nnodes = 0, root = 0, ncut = 0;
+    uint32_t nv = 0, nt = 0, nnodes = 0, root = 0, ncut = 0, ncut4 = 0;
     size_t bytes = 0;
 };
 
