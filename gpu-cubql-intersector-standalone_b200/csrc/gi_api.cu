@@ -235,7 +235,7 @@ static gi_status mesh_alloc(gi_ctx* c, uint32_t nv, uint32_t nt, gi_mesh** pm, c
 }
 
 // Host -> device copy on stream st.  Pinned sources go straight to the DMA
-// engine.  A large pageable source would be staged by the driver on the
+// engine.  A large pageable source would be staged by the CUDA driver on the
 // calling thread at about a third of the link rate; instead the context's
 // copy helpers fill one pinned chunk while the DMA of the previous one runs.
 // Returns when the source may be reused (like a pageable cudaMemcpyAsync).

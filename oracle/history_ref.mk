@@ -1,5 +1,5 @@
 # Builds oracle/_ref/history_ref: the reference's header-only IntersectionHistory
-# (src/CPU/IntersectionHistory.h) compiled where it lies, with the driver
+# (src/CPU/IntersectionHistory.h) compiled where it lies, with the program
 # history_ref_main.cpp.  Test infrastructure; needs the reference tree (REF) and
 # CUDA's vector_types.h.  Usage: make -f history_ref.mk REF=<reference root>
 REF ?= /root/reference

@@ -1,4 +1,4 @@
-// Test infrastructure: a driver around the reference's own IntersectionHistory
+// Test infrastructure: a small program around the reference's own IntersectionHistory
 // (src/CPU/IntersectionHistory.h, header-only), compiled from the reference
 // sources by history_ref.mk into oracle/_ref/history_ref.  It reads runs as
 // record files and writes the reference's CSVs, against which the library's

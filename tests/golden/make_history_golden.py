@@ -70,7 +70,7 @@ def digest(path):
 
 def main():
     if not os.path.exists(REF_BIN):
-        sys.exit("build the reference driver first: make -f oracle/history_ref.mk")
+        sys.exit("build the reference program first: make -f oracle/history_ref.mk")
     out = {}
     with tempfile.TemporaryDirectory() as td:
         bins = {}

@@ -2,7 +2,7 @@
 device), pinned to the reference's own IntersectionHistory
 (src/CPU/IntersectionHistory.h): byte-exact digests of the CSVs it wrote
 (tests/golden/history.json, made by tests/golden/make_history_golden.py) and,
-where the reference driver is built (oracle/_ref/history_ref), live comparisons
+where the reference program is built (oracle/_ref/history_ref), live comparisons
 on seeded runs."""
 import csv
 import hashlib
@@ -154,7 +154,7 @@ def test_pairs_diff_properties():
         assert b.tolist() == [list(x) for x in sorted(s1 & s2)]
 
 
-@pytest.mark.skipif(not os.path.exists(REF_BIN), reason="reference history driver not built here")
+@pytest.mark.skipif(not os.path.exists(REF_BIN), reason="reference history program not built here")
 def test_live_reference_on_seeded_runs(oc, tmp_path):
     import make_history_golden as mhg
     from gpuintersector.history import IntersectionHistory, PosedMesh
