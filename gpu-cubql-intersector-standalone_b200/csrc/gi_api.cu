@@ -808,7 +808,9 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         r->pairs = hpairs + 2 * (size_t)a;
         r->npairs = e - a;
         size_t s0 = sp;
-        while (sp < nsegs && (uint32_t)hsegpair[sp] < e) sp++;
+        if (nj == 1) sp = nsegs;  // one job: all segments are its own
+        else
+            while (sp < nsegs && (uint32_t)hsegpair[sp] < e) sp++;
         r->segs = hsegs + 6 * s0;
         r->seg_pair = hsegpair + s0;
         r->nsegs = sp - s0;

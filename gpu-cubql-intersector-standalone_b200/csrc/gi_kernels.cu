@@ -2052,9 +2052,18 @@ cudaError_t launch_order_small_phases(const Bufs& b, const OrderBufs& O, bool so
     if (!sort) phases &= ~kOrderRank;  // nothing to rank: results keep their order
     if (!phases) return cudaSuccess;
     const size_t dyn = (phases & kOrderRank) ? kOrderSmallDyn : 0;
-    cudaError_t e = cudaFuncSetAttribute((const void*)k_order_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kOrderSmallDyn);
+    // the shared-memory opt-in is a per-device function attribute: set it once per device
+    static std::atomic<uint64_t> attr_done{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
+    const uint64_t bit = dev < 64 ? (1ull << dev) : 0ull;
+    if (!bit || !(attr_done.load(std::memory_order_acquire) & bit)) {
+        e = cudaFuncSetAttribute((const void*)k_order_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kOrderSmallDyn);
+        if (e != cudaSuccess) return e;
+        attr_done.fetch_or(bit, std::memory_order_acq_rel);
+    }
     Bufs bb = b;
     OrderBufs oo = O;
     const double* a_segs = segs;
