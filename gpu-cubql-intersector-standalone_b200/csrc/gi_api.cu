@@ -591,7 +591,7 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
             if (b) c->pinned->put(b);
         }
     } guard{c, buf};
-    // ordering path: one cooperative launch when the previous call's count says
+    // ordering path: the small cooperative one when the previous call's count says
     // the result will be small (the kernel refuses, and this loop reruns on the
     // radix path, if it is not)
     bool small_order = ba + bb + bj <= 63 && c->pred_pairs <= kOrderSmallMax - kOrderSmallMax / 4;

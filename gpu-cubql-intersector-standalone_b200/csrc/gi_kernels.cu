@@ -1060,7 +1060,8 @@ __device__ __forceinline__ void expand_quad(const Bufs& B, const uint4& ent, boo
 // queue; leaf pairs (candidates) always go to the global candidate list, so
 // the first filter stage runs on warps that have no node pair at hand.  The
 // launch first seeds the queue: every overlapping pair of the two meshes'
-// depth-3 cut entries becomes a node pair (a leaf pair, a candidate).
+// cut entries (depth 4 for a single pair, depth 3 for a batch) becomes a node
+// pair (a leaf pair, a candidate).
 //
 // Slot protocol (queue and candidate list): producers reserve slots with one
 // atomic per warp, write the entries and, after a release fence, store the
@@ -1824,7 +1825,9 @@ cudaError_t launch_order_gather(const Bufs& b, const OrderBufs& O, bool sort, co
 }
 
 // ---------------------------------------------------------------------------
-// Small-count ordering (up to kOrderSmallMax results) in one cooperative launch.
+// Small-count ordering (up to kOrderSmallMax results) in cooperative launches:
+// one, or a rank launch and a place launch when the segments are built on
+// another stream in between.
 //
 // At a few thousand to a few tens of thousands of results the radix passes
 // above are bound by launch and look-back latency, not by bytes.  Here each of

@@ -93,7 +93,7 @@ OrderBufs make_order_bufs(void* scratch, uint32_t cap, int bits_a, int bits_b, i
 cudaError_t launch_order_gather(const Bufs& b, const OrderBufs& O, bool sort, const double* segs,
                                 const uint32_t* nseg, int32_t* pairs_out, uint32_t* job_out, double* segs_out,
                                 int32_t* segpair_out, bool want_segments, const LaunchCfg& cfg, cudaStream_t st);
-// Small-count ordering: one cooperative launch of kOrderSmallBlocks blocks,
+// Small-count ordering: a cooperative launch of kOrderSmallBlocks blocks,
 // each sorting a run of kOrderSmallRun keys, for up to kOrderSmallMax results.
 // If the call produced more, the kernel only sets Counters::order_redo and the
 // caller reruns with launch_order_gather.  Keys must fit in 63 bits.
