@@ -21,7 +21,6 @@
 //    one-vertex curves, and branch vertices (degree >= 3) end chains.
 #include <algorithm>
 #include <cstring>
-#include <unordered_map>
 #include <vector>
 
 #include "gi_host.h"
@@ -39,13 +38,53 @@ struct PtKey {
     uint64_t b[3];
     bool operator==(const PtKey& o) const { return b[0] == o.b[0] && b[1] == o.b[1] && b[2] == o.b[2]; }
 };
-struct PtHash {
-    size_t operator()(const PtKey& k) const
+
+// splitmix64 finaliser: every input bit reaches the low bits the tables index with
+inline uint64_t mix64(uint64_t x)
+{
+    x ^= x >> 30;
+    x *= 0xbf58476d1ce4e5b9ull;
+    x ^= x >> 27;
+    x *= 0x94d049bb133111ebull;
+    x ^= x >> 31;
+    return x;
+}
+inline uint64_t hash_pt(const PtKey& k)
+{
+    return mix64(k.b[0] ^ mix64(k.b[1] ^ mix64(k.b[2])));
+}
+
+// Open-addressing hash table (linear probing, power-of-two capacity of at
+// least twice the number of keys it will hold): one flat allocation instead of
+// a node per entry.
+template <class K, class V>
+struct FlatMap {
+    std::vector<K> keys;
+    std::vector<V> vals;
+    std::vector<uint8_t> used;
+    size_t mask = 0;
+    explicit FlatMap(size_t max_keys)
     {
-        uint64_t h = k.b[0] * 0x9E3779B97F4A7C15ull;
-        h ^= (k.b[1] + 0x632BE59BD9B4E019ull + (h << 6) + (h >> 2));
-        h ^= (k.b[2] + 0x85157AF5ull + (h << 6) + (h >> 2));
-        return (size_t)h;
+        size_t cap = 16;
+        while (cap < 2 * max_keys + 1) cap <<= 1;
+        keys.resize(cap);
+        vals.resize(cap);
+        used.assign(cap, 0);
+        mask = cap - 1;
+    }
+    // the value of k, inserted as v when absent; second: inserted
+    template <class Hash>
+    std::pair<V*, bool> emplace(const K& k, const V& v, Hash hash)
+    {
+        size_t h = (size_t)hash(k) & mask;
+        while (used[h]) {
+            if (keys[h] == k) return {&vals[h], false};
+            h = (h + 1) & mask;
+        }
+        used[h] = 1;
+        keys[h] = k;
+        vals[h] = v;
+        return {&vals[h], true};
     }
 };
 
@@ -78,37 +117,58 @@ extern "C" gi_status gi_curves_build(const double* seg6, const int32_t* seg_pair
     std::vector<uint32_t> per_pair(r->npairs, 0);
     for (uint64_t s = 0; s < ns; s++)
         if (r->seg_pair[s] >= 0 && (uint64_t)r->seg_pair[s] < r->npairs) per_pair[r->seg_pair[s]]++;
-    std::unordered_map<PtKey, uint32_t, PtHash> vid;
-    vid.reserve(2 * ns + 16);
+    // vertex table: 8-byte slots (hash tag, vertex id + 1) over keys stored once in vertex order
+    size_t vcap = 16;
+    while (vcap < 4 * ns + 1) vcap <<= 1;
+    std::vector<uint64_t> vslot(vcap, 0);
+    std::vector<PtKey> vkeys;
+    vkeys.reserve(2 * ns);
+    cv->verts.reserve(6 * ns);
     auto vertex = [&](const double* p) {
-        auto it = vid.emplace(key_of(p), (uint32_t)(cv->verts.size() / 3));
-        if (it.second) cv->verts.insert(cv->verts.end(), p, p + 3);
-        return it.first->second;
+        const PtKey k = key_of(p);
+        const uint64_t h = hash_pt(k);
+        const uint32_t tag = (uint32_t)(h >> 32);
+        size_t i = (size_t)h & (vcap - 1);
+        for (;;) {
+            const uint64_t e = vslot[i];
+            if (e == 0) break;
+            const uint32_t id = (uint32_t)e - 1u;
+            if ((uint32_t)(e >> 32) == tag && vkeys[id] == k) return id;
+            i = (i + 1) & (vcap - 1);
+        }
+        const uint32_t id = (uint32_t)vkeys.size();
+        vslot[i] = ((uint64_t)tag << 32) | (uint64_t)(id + 1u);
+        vkeys.push_back(k);
+        cv->verts.insert(cv->verts.end(), p, p + 3);
+        return id;
     };
     struct EdgeInfo {
         uint32_t coplanar = 0, other = 0;
     };
-    std::unordered_map<uint64_t, EdgeInfo> edges;
-    edges.reserve(ns + 16);
+    FlatMap<uint64_t, EdgeInfo> edges(ns);
+    std::vector<uint64_t> edge_keys;  // distinct edges in first-seen order
+    edge_keys.reserve(ns);
     for (uint64_t s = 0; s < ns; s++) {
         const double* a = r->segs + 6 * s;
         const uint32_t u = vertex(a), v = vertex(a + 3);
         if (u == v) continue;  // touching point: an isolated vertex unless an edge reaches it
         const uint64_t k = u < v ? ((uint64_t)u << 32) | v : ((uint64_t)v << 32) | u;
         const bool cop = r->seg_pair[s] >= 0 && (uint64_t)r->seg_pair[s] < r->npairs && per_pair[r->seg_pair[s]] == 3;
-        EdgeInfo& e = edges[k];
+        auto it = edges.emplace(k, EdgeInfo{}, mix64);
+        if (it.second) edge_keys.push_back(k);
+        EdgeInfo& e = *it.first;
         if (cop) e.coplanar++;
         else e.other++;
     }
     const uint32_t nv = (uint32_t)(cv->verts.size() / 3);
     std::vector<std::pair<uint32_t, uint32_t>> el;
-    el.reserve(edges.size());
-    for (auto& kv : edges) {
-        const EdgeInfo& e = kv.second;
+    el.reserve(edge_keys.size());
+    for (uint64_t k : edge_keys) {
+        const EdgeInfo& e = *edges.emplace(k, EdgeInfo{}, mix64).first;
         if (drop_coplanar_interior && e.other == 0 && e.coplanar >= 2) continue;
-        el.emplace_back((uint32_t)(kv.first >> 32), (uint32_t)(kv.first & 0xffffffffu));
+        el.emplace_back((uint32_t)(k >> 32), (uint32_t)(k & 0xffffffffu));
     }
-    std::sort(el.begin(), el.end());  // deterministic curve order
+    // edges in first-seen order: the curve order follows the segment order (deterministic)
     // adjacency (CSR)
     std::vector<uint32_t> deg(nv + 1, 0);
     for (auto& e : el) {
