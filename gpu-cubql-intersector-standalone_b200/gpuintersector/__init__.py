@@ -379,8 +379,30 @@ class Result:
 
     ZERO_COPY_BYTES = 4 << 20
 
+    __slots__ = ("_owner", "_stats", "_npairs", "_pairs", "_segments", "_seg_pair")
+
     def __init__(self, handle):
+        # the device work and the copy to the host are done when the library
+        # returns the handle; the Python views and the stats dict are built on
+        # first use, so a batch of thousands of results returns at once
+        self._owner = _ResultOwner(handle)
+        self._stats = None
+        self._pairs = None
+
+    @property
+    def stats(self):
+        if self._stats is None:
+            st = _abi.Stats()
+            lib().gi_result_stats(self._owner.handle, ctypes.byref(st))
+            self._stats = st.as_dict()
+        return self._stats
+
+    def _load(self):
+        if self._pairs is not None:
+            return
+        self.stats  # kept: the handle may be released below
         L = lib()
+        handle = self._owner.handle
         p = ctypes.POINTER(ctypes.c_int32)()
         n = ctypes.c_uint64()
         L.gi_result_pairs(handle, ctypes.byref(p), ctypes.byref(n))
@@ -388,11 +410,8 @@ class Result:
         spp = ctypes.POINTER(ctypes.c_int32)()
         m = ctypes.c_uint64()
         L.gi_result_segments(handle, ctypes.byref(sp), ctypes.byref(spp), ctypes.byref(m))
-        st = _abi.Stats()
-        L.gi_result_stats(handle, ctypes.byref(st))
-        self.stats = st.as_dict()
         npairs, nsegs = n.value, m.value
-        owner = _ResultOwner(handle)
+        owner = self._owner
         zero_copy = 8 * npairs + 52 * nsegs <= self.ZERO_COPY_BYTES
 
         def arr(ptr, shape, dtype, count):
@@ -401,11 +420,32 @@ class Result:
             a = np.asarray(_View(owner, ctypes.cast(ptr, ctypes.c_void_p).value, shape, dtype))
             return a if zero_copy else a.copy()
 
-        self.npairs = npairs
-        self.pairs = arr(p, (npairs, 2), np.int32, npairs)
-        self.segments = arr(sp, (nsegs, 6), np.float64, nsegs)
-        self.seg_pair = arr(spp, (nsegs,), np.int32, nsegs)
-        del owner  # freed here if every array was copied or empty
+        self._npairs = npairs
+        self._segments = arr(sp, (nsegs, 6), np.float64, nsegs)
+        self._seg_pair = arr(spp, (nsegs,), np.int32, nsegs)
+        self._pairs = arr(p, (npairs, 2), np.int32, npairs)
+        self._owner = None  # the views hold it while they need it; freed here if every array was copied or empty
+        del owner
+
+    @property
+    def npairs(self):
+        self._load()
+        return self._npairs
+
+    @property
+    def pairs(self):
+        self._load()
+        return self._pairs
+
+    @property
+    def segments(self):
+        self._load()
+        return self._segments
+
+    @property
+    def seg_pair(self):
+        self._load()
+        return self._seg_pair
 
     def curves(self, drop_coplanar_interior=True):
         """The segments chained into polylines (see curves())."""
