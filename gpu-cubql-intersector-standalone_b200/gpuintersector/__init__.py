@@ -392,6 +392,8 @@ class Result:
     @property
     def stats(self):
         if self._stats is None:
+            if self._owner is None:
+                raise RuntimeError("result handle already released")
             st = _abi.Stats()
             lib().gi_result_stats(self._owner.handle, ctypes.byref(st))
             self._stats = st.as_dict()
@@ -400,7 +402,6 @@ class Result:
     def _load(self):
         if self._pairs is not None:
             return
-        self.stats  # kept: the handle may be released below
         L = lib()
         handle = self._owner.handle
         p = ctypes.POINTER(ctypes.c_int32)()
@@ -413,6 +414,8 @@ class Result:
         npairs, nsegs = n.value, m.value
         owner = self._owner
         zero_copy = 8 * npairs + 52 * nsegs <= self.ZERO_COPY_BYTES
+        if not zero_copy:
+            self.stats  # read now: the handle is released once the arrays are copied
 
         def arr(ptr, shape, dtype, count):
             if count == 0:
@@ -424,7 +427,8 @@ class Result:
         self._segments = arr(sp, (nsegs, 6), np.float64, nsegs)
         self._seg_pair = arr(spp, (nsegs,), np.int32, nsegs)
         self._pairs = arr(p, (npairs, 2), np.int32, npairs)
-        self._owner = None  # the views hold it while they need it; freed here if every array was copied or empty
+        if not zero_copy:
+            self._owner = None  # freed here: every array was copied
         del owner
 
     @property
