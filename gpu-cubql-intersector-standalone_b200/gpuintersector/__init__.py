@@ -23,7 +23,7 @@ import numpy as np
 from . import _abi
 from ._abi import GI_NOALLOC_MAX_PAIRS, GI_PREC_FP32_CASCADE, GI_PREC_FP64
 
-__all__ = ["GIError", "Context", "Mesh", "Result", "pose_identity", "pose_from_euler_deg", "pose_raw",
+__all__ = ["GIError", "Context", "Mesh", "Result", "BatchResult", "pose_identity", "pose_from_euler_deg", "pose_raw",
            "KernelBVHController", "run_grid_forest_intersection_pipeline", "compute_exact_intersection_curves",
            "GI_PREC_FP32_CASCADE", "GI_PREC_FP64", "lib"]
 
@@ -176,16 +176,43 @@ class Context:
         """jobs: list of (A, pose_a, B, pose_b); returns a list of Result."""
         n = len(jobs)
         arr = (_abi.PairJob * n)()
+        ident = pose_identity()
         for i, (A, pa, B, pb) in enumerate(jobs):
             arr[i].A = A.handle
             arr[i].B = B.handle
-            arr[i].pose_a = pa if pa is not None else pose_identity()
-            arr[i].pose_b = pb if pb is not None else pose_identity()
+            arr[i].pose_a = pa if pa is not None else ident
+            arr[i].pose_b = pb if pb is not None else ident
         outs = (ctypes.c_void_p * n)()
         o = self._opts(want_segments, precision, sort_output)
         rc = self._lib.gi_intersect_batch(self.handle, arr, n, ctypes.byref(o), outs)
         self.check(rc, "gi_intersect_batch")
         return [Result(ctypes.c_void_p(outs[i])) for i in range(n)]
+
+    def intersect_batch_flat(self, jobs, want_segments=True, precision=GI_PREC_FP32_CASCADE, sort_output=True):
+        """The batch call of intersect_batch with its results as whole-batch
+        arrays instead of one Result per job (a batch of thousands of jobs
+        does not pay per-job Python objects):
+
+          pairs (N, 2) int32, job (N,) uint32: the job of each pair,
+          offsets (njobs + 1,): job j owns pairs[offsets[j]:offsets[j + 1]],
+          segments (M, 6) float64, seg_pair (M,) int64: index into pairs,
+          stats: the launch-wide statistics of the call.
+
+        pairs and segments are views of the library's pinned result block
+        (all jobs' results lie in it back to back; copies are made otherwise)."""
+        n = len(jobs)
+        arr = (_abi.PairJob * n)()
+        ident = pose_identity()
+        for i, (A, pa, B, pb) in enumerate(jobs):
+            arr[i].A = A.handle
+            arr[i].B = B.handle
+            arr[i].pose_a = pa if pa is not None else ident
+            arr[i].pose_b = pb if pb is not None else ident
+        outs = (ctypes.c_void_p * n)()
+        o = self._opts(want_segments, precision, sort_output)
+        rc = self._lib.gi_intersect_batch(self.handle, arr, n, ctypes.byref(o), outs)
+        self.check(rc, "gi_intersect_batch")
+        return BatchResult([_ResultOwner(ctypes.c_void_p(outs[i])) for i in range(n)])
 
     def intersect_oneshot(self, vA, tA, vB, tB, pose_a=None, pose_b=None, want_segments=True,
                           precision=GI_PREC_FP32_CASCADE, sort_output=True):
@@ -454,6 +481,64 @@ class Result:
     def curves(self, drop_coplanar_interior=True):
         """The segments chained into polylines (see curves())."""
         return curves(self.segments, self.seg_pair, self.npairs, drop_coplanar_interior)
+
+
+class _BatchOwner:
+    """Keeps every result handle of a batch alive while views of their shared block exist."""
+
+    __slots__ = ("owners",)
+
+    def __init__(self, owners):
+        self.owners = owners
+
+
+class BatchResult:
+    """Whole-batch arrays of one gi_intersect_batch call (see Context.intersect_batch_flat)."""
+
+    def __init__(self, owners):
+        L = lib()
+        n = len(owners)
+        p = ctypes.POINTER(ctypes.c_int32)()
+        cnt = ctypes.c_uint64()
+        sp = ctypes.POINTER(ctypes.c_double)()
+        spp = ctypes.POINTER(ctypes.c_int32)()
+        m = ctypes.c_uint64()
+        pa, sa, qa = np.zeros(n, np.uint64), np.zeros(n, np.uint64), np.zeros(n, np.uint64)
+        npairs, nsegs = np.zeros(n, np.int64), np.zeros(n, np.int64)
+        for i, ow in enumerate(owners):
+            L.gi_result_pairs(ow.handle, ctypes.byref(p), ctypes.byref(cnt))
+            L.gi_result_segments(ow.handle, ctypes.byref(sp), ctypes.byref(spp), ctypes.byref(m))
+            pa[i] = ctypes.cast(p, ctypes.c_void_p).value or 0
+            sa[i] = ctypes.cast(sp, ctypes.c_void_p).value or 0
+            qa[i] = ctypes.cast(spp, ctypes.c_void_p).value or 0
+            npairs[i], nsegs[i] = cnt.value, m.value
+        self.offsets = np.concatenate([[0], np.cumsum(npairs)]).astype(np.int64)
+        soff = np.concatenate([[0], np.cumsum(nsegs)]).astype(np.int64)
+        st = _abi.Stats()
+        if n:
+            L.gi_result_stats(owners[0].handle, ctypes.byref(st))
+        self.stats = st.as_dict()
+        holder = _BatchOwner(owners)
+
+        def whole(addr, counts, starts, width, dtype):
+            total = int(starts[-1])
+            item = np.dtype(dtype).itemsize * width
+            nz = np.nonzero(counts)[0]
+            if total == 0:
+                return np.zeros((0, width) if width > 1 else (0,), dtype=dtype)
+            shape = (total, width) if width > 1 else (total,)
+            first = int(nz[0])
+            base = int(addr[first]) - item * int(starts[first])
+            if np.all(addr[nz].astype(np.int64) == base + item * starts[nz]):  # back to back in one block
+                return np.asarray(_View(holder, base + item * int(starts[0]), shape, dtype))
+            parts = [np.asarray(_View(holder, int(addr[i]), (int(counts[i]),) + shape[1:], dtype)) for i in nz]
+            return np.concatenate(parts)
+
+        self.pairs = whole(pa, npairs, self.offsets, 2, np.int32)
+        self.segments = whole(sa, nsegs, soff, 6, np.float64)
+        local = whole(qa, nsegs, soff, 1, np.int32)  # per job, relative to the job's first pair
+        self.seg_pair = local.astype(np.int64) + np.repeat(self.offsets[:-1], nsegs)
+        self.job = np.repeat(np.arange(n, dtype=np.uint32), npairs)
 
 
 class Server:

@@ -277,6 +277,38 @@ def test_batch_equals_individual(ctx, gi, oc):
         m.release()
 
 
+def test_batch_flat_matches_per_job_results(ctx, gi):
+    """intersect_batch_flat: the same pairs, segments and segment grouping as the
+    per-job results, as whole-batch arrays (jobs with no pair included)."""
+    from gpuintersector import meshgen as mg
+
+    jobs = mg.config4(seed=9, pairs=12, t_min=200, t_max=3000)
+    meshes, bjobs = [], []
+    for k, j in enumerate(jobs):
+        A, B = ctx.upload(j["vA"], j["tA"]), ctx.upload(j["vB"], j["tB"])
+        meshes += [A, B]
+        pose = gi_pose(gi, j["poseB"])
+        if k % 5 == 4:  # far apart: a job with no pair
+            R, C, T = j["poseB"]
+            pose = gi.pose_raw(R, C, np.asarray(T) + 50.0)
+        bjobs.append((A, None, B, pose))
+    per = ctx.intersect_batch(bjobs)
+    flat = ctx.intersect_batch_flat(bjobs)
+    assert flat.offsets.shape == (len(jobs) + 1,)
+    assert any(len(r.pairs) == 0 for r in per) and sum(len(r.pairs) for r in per) > 0
+    for k, r in enumerate(per):
+        a, e = flat.offsets[k], flat.offsets[k + 1]
+        assert np.array_equal(flat.pairs[a:e], r.pairs)
+        assert np.all(flat.job[a:e] == k)
+        sel = (flat.seg_pair >= a) & (flat.seg_pair < e)
+        assert np.array_equal(flat.segments[sel], r.segments)
+        assert np.array_equal(flat.seg_pair[sel] - a, r.seg_pair)
+    assert flat.stats["pairs"] == len(per[0].pairs)
+    del per, flat
+    for m in meshes:
+        m.release()
+
+
 def test_oneshot_and_controller_mirror(ctx, gi, oc):
     from gpuintersector import meshgen as mg
 
