@@ -1275,6 +1275,70 @@ int oc_intersect_meshes(const double* vA, uint32_t nvA, const uint32_t* tA, uint
     return 0;
 }
 
+/* Exact test of an explicit pair list on `nthreads` threads: the CPU side of
+ * the reference's pair-list filter (filterYellowPairsTBB,
+ * src/CPU/YellowFilter.h:80-137, CGAL do_intersect over a pair list on TBB
+ * threads).  Vertices are posed once; the list is split into equal slices. */
+typedef struct {
+    const double *wA, *wB;
+    const uint32_t *tA, *tB;
+    const int32_t* pairs;
+    uint8_t* out;
+    uint64_t lo, hi;
+} PairSlice;
+
+static void* pair_slice_main(void* arg)
+{
+    PairSlice* S = (PairSlice*)arg;
+    for (uint64_t i = S->lo; i < S->hi; i++) {
+        const uint32_t* ta = S->tA + 3 * (size_t)S->pairs[2 * i];
+        const uint32_t* tb = S->tB + 3 * (size_t)S->pairs[2 * i + 1];
+        const double* T1[3] = {S->wA + 3 * (size_t)ta[0], S->wA + 3 * (size_t)ta[1], S->wA + 3 * (size_t)ta[2]};
+        const double* T2[3] = {S->wB + 3 * (size_t)tb[0], S->wB + 3 * (size_t)tb[1], S->wB + 3 * (size_t)tb[2]};
+        TTRes r;
+        classify(T1, T2, &r, 0);
+        S->out[i] = r.kind != OC_NONE;
+    }
+    return NULL;
+}
+
+int oc_classify_pairs(const double* vA, uint32_t nvA, const uint32_t* tA, uint32_t ntA, const oc_pose* pA,
+                      const double* vB, uint32_t nvB, const uint32_t* tB, uint32_t ntB, const oc_pose* pB,
+                      const int32_t* pairs, uint64_t n, uint8_t* out, int nthreads)
+{
+    for (uint64_t i = 0; i < n; i++)
+        if (pairs[2 * i] < 0 || (uint32_t)pairs[2 * i] >= ntA || pairs[2 * i + 1] < 0 || (uint32_t)pairs[2 * i + 1] >= ntB)
+            return -1;
+    for (uint64_t i = 0; i < 3 * (uint64_t)ntA; i++)
+        if (tA[i] >= nvA) return -1;
+    for (uint64_t i = 0; i < 3 * (uint64_t)ntB; i++)
+        if (tB[i] >= nvB) return -1;
+    double* wA = (double*)malloc(sizeof(double) * 3 * (size_t)(nvA ? nvA : 1));
+    double* wB = (double*)malloc(sizeof(double) * 3 * (size_t)(nvB ? nvB : 1));
+    oc_transform_vertices(pA, vA, nvA, wA);
+    oc_transform_vertices(pB, vB, nvB, wB);
+    if (nthreads <= 0) nthreads = oc_hw_threads();
+    PairSlice* S = (PairSlice*)calloc((size_t)nthreads, sizeof(PairSlice));
+    pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * (size_t)nthreads);
+    for (int k = 0; k < nthreads; k++) {
+        S[k].wA = wA;
+        S[k].wB = wB;
+        S[k].tA = tA;
+        S[k].tB = tB;
+        S[k].pairs = pairs;
+        S[k].out = out;
+        S[k].lo = n * (uint64_t)k / (uint64_t)nthreads;
+        S[k].hi = n * (uint64_t)(k + 1) / (uint64_t)nthreads;
+        pthread_create(&th[k], NULL, pair_slice_main, &S[k]);
+    }
+    for (int k = 0; k < nthreads; k++) pthread_join(th[k], NULL);
+    free(th);
+    free(S);
+    free(wA);
+    free(wB);
+    return 0;
+}
+
 int oc_intersect_meshes_bruteforce(const double* vA, uint32_t nvA, const uint32_t* tA, uint32_t ntA,
                                    const oc_pose* pA, const double* vB, uint32_t nvB, const uint32_t* tB,
                                    uint32_t ntB, const oc_pose* pB, int32_t** pairs, uint64_t* npairs)

@@ -108,6 +108,13 @@ int oc_intersect_meshes(const double* vA, uint32_t nvA, const uint32_t* tA, uint
                         double** segs, int32_t** seg_pair, uint64_t* nsegs,
                         oc_stats* stats);
 
+/* Exact test of each (a, b) of an explicit pair list (out[i] = 1 iff the posed
+ * triangles A[a] and B[b] share a point) on `nthreads` threads (0 = all).
+ * Returns -1 (nothing written) for an index out of range. */
+int oc_classify_pairs(const double* vA, uint32_t nvA, const uint32_t* tA, uint32_t ntA, const oc_pose* pA,
+                      const double* vB, uint32_t nvB, const uint32_t* tB, uint32_t ntB, const oc_pose* pB,
+                      const int32_t* pairs, uint64_t n, uint8_t* out, int nthreads);
+
 /* Brute-force candidate-free variant for tiny meshes (all pairs, 1 thread). */
 int oc_intersect_meshes_bruteforce(const double* vA, uint32_t nvA, const uint32_t* tA, uint32_t ntA,
                                    const oc_pose* pA,

@@ -68,6 +68,11 @@ def lib():
             dp, ctypes.c_uint32, up, ctypes.c_uint32, ctypes.POINTER(Pose),
             ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)), ctypes.POINTER(ctypes.c_uint64)]
         L.oc_intersect_meshes_bruteforce.restype = ctypes.c_int
+        L.oc_classify_pairs.argtypes = [
+            dp, ctypes.c_uint32, up, ctypes.c_uint32, ctypes.POINTER(Pose),
+            dp, ctypes.c_uint32, up, ctypes.c_uint32, ctypes.POINTER(Pose),
+            ctypes.POINTER(ctypes.c_int32), ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint8), ctypes.c_int]
+        L.oc_classify_pairs.restype = ctypes.c_int
         L.oc_free.argtypes = [ctypes.c_void_p]
         L.oc_hw_threads.restype = ctypes.c_int
         _lib = L
@@ -176,6 +181,23 @@ def intersect_meshes(vA, tA, pA, vB, tB, pB, want_segments=True, nthreads=0, a_l
     if spp:
         L.oc_free(ctypes.cast(spp, ctypes.c_void_p))
     return dict(pairs=pairs, segs=segs, seg_pair=seg_pair, stats=st)
+
+
+def classify_pairs(vA, tA, pA, vB, tB, pB, pairs, nthreads=0):
+    """Exact test of each (a, b) of a pair list on host threads: uint8 per pair."""
+    vA = np.ascontiguousarray(vA, dtype=np.float64).reshape(-1, 3)
+    vB = np.ascontiguousarray(vB, dtype=np.float64).reshape(-1, 3)
+    tA = np.ascontiguousarray(tA, dtype=np.uint32).reshape(-1, 3)
+    tB = np.ascontiguousarray(tB, dtype=np.uint32).reshape(-1, 3)
+    p = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+    out = np.empty(p.shape[0], dtype=np.uint8)
+    rc = lib().oc_classify_pairs(_dp(vA), vA.shape[0], _up(tA), tA.shape[0], ctypes.byref(pA),
+                                 _dp(vB), vB.shape[0], _up(tB), tB.shape[0], ctypes.byref(pB),
+                                 p.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), p.shape[0],
+                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), int(nthreads))
+    if rc != 0:
+        raise ValueError("oc_classify_pairs: index out of range")
+    return out
 
 
 def intersect_meshes_bruteforce(vA, tA, pA, vB, tB, pB):

@@ -141,3 +141,30 @@ def test_empty_and_bad_meshes(oc):
     assert len(r["pairs"]) == 0
     with pytest.raises(RuntimeError):
         oc.intersect_meshes(v, np.array([[0, 1, 5]], np.uint32), ip, v, t, ip)
+
+
+def test_oracle_classify_pairs_list(oc):
+    """oc_classify_pairs (a pair list on host threads) agrees with the per-pair
+    exact test, and rejects an index out of range."""
+    from gpuintersector import meshgen as mg
+
+    cfg = mg.config1(seed=5)
+    R, C, T = cfg["poseB"]
+    pB = oc.pose_raw(R, C, T)
+    ref = oc.intersect_meshes(cfg["vA"], cfg["tA"], oc.pose_identity(), cfg["vB"], cfg["tB"], pB, want_segments=False)
+    hits = ref["pairs"]
+    nt = cfg["tB"].shape[0]
+    d = np.arange(-6, 6)
+    pairs = np.stack([np.repeat(hits[:, 0], d.size), (np.repeat(hits[:, 1], d.size) + np.tile(d, len(hits))) % nt], 1)
+    out = oc.classify_pairs(cfg["vA"], cfg["tA"], oc.pose_identity(), cfg["vB"], cfg["tB"], pB, pairs, nthreads=3)
+    wA = oc.transform(oc.pose_identity(), cfg["vA"])
+    wB = oc.transform(pB, cfg["vB"])
+    sample = range(0, len(pairs), 7)
+    exp = [oc.tri_tri_intersect(wA[cfg["tA"][pairs[i, 0]]], wB[cfg["tB"][pairs[i, 1]]]) for i in sample]
+    assert np.array_equal(out[list(sample)], np.array(exp, dtype=np.uint8))
+    # every known intersecting pair is classified as such; the counts agree with the mesh run
+    assert out[d.size // 2::d.size].all()
+    hit_set = set(map(tuple, hits.tolist()))
+    assert int(out.sum()) == sum(1 for p in map(tuple, pairs.tolist()) if p in hit_set)
+    with pytest.raises(ValueError):
+        oc.classify_pairs(cfg["vA"], cfg["tA"], oc.pose_identity(), cfg["vB"], cfg["tB"], pB, np.array([[0, nt]]))
