@@ -2018,11 +2018,16 @@ __global__ void __launch_bounds__(kOrderSmallThreads, 1)
     const unsigned ex = block_exclusive_scan(cnt, sw, &tot);
     if (tid == 0) O.tile_tot[t] = tot;
     grid_barrier(&C->obar, ++bar, &C->err, &s_ok);
-    if (tid == 0) {
-        unsigned b0 = 0;
-        for (unsigned s = 0; s < t; s++) b0 += __ldcg(O.tile_tot + s);
-        s_base = b0;
-        if (nruns && t == nruns - 1) C->nseg = b0 + tot;
+    if (tid < 32u) {
+        // the preceding blocks' totals, loaded by one warp at once and summed by shuffles
+        static_assert(kOrderSmallBlocks <= 32, "one warp sums the block totals");
+        unsigned v = tid < t ? __ldcg(O.tile_tot + tid) : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (tid == 0) {
+            s_base = v;
+            if (nruns && t == nruns - 1) C->nseg = v + tot;
+        }
     }
     __syncthreads();
     if (!ok) return;
