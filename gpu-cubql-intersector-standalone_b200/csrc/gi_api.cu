@@ -180,26 +180,30 @@ struct UploadSink {
 
 static gi_status mesh_finish(gi_ctx* c, gi_mesh* m, gi_mesh** out, cudaStream_t st, const UploadSink& sk)
 {
+    // The validation result is read back with the build's last synchronisation,
+    // not before it: the build reads vertex indices clamped to the array, so an
+    // invalid mesh costs a wasted build but no out-of-bounds access.
     unsigned* d_err = nullptr;
     CKS(sk, pool_alloc(&d_err, sizeof(unsigned), c->pool, st), "alloc");
     CKS(sk, cudaMemsetAsync(d_err, 0, sizeof(unsigned), st), "memset");
     CKS(sk, launch_validate(m->b.verts, m->b.nv, m->b.tris, m->b.nt, d_err, st), "validate");
+    cudaError_t e = build_bvh(m->b, false, c->pool, st);
     unsigned herr = 0;
-    CKS(sk, cudaMemcpyAsync(&herr, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "copy");
-    CKS(sk, cudaStreamSynchronize(st), "sync");
+    // a pageable destination: the copy returns when the stream has reached it (the build is done)
+    cudaError_t es = cudaMemcpyAsync(&herr, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+    // on an error the stream may still hold kernels that use the mesh: drain it before freeing
+    const cudaError_t es2 = cudaStreamSynchronize(st);
+    if (es == cudaSuccess) es = es2;
+    if (e == cudaSuccess) e = es;
     cudaFreeAsync(d_err, st);
+    if (e != cudaSuccess) {
+        mesh_free(c, m, st);
+        return sk.fail(e == cudaErrorMemoryAllocation ? GI_ERR_OOM : GI_ERR_CUDA, "BVH build", e);
+    }
     if (herr) {
         mesh_free(c, m, st);
         return sk.fail((herr & 1u) ? GI_ERR_INVALID_ARG : GI_ERR_RANGE,
                        (herr & 1u) ? "triangle index out of range" : "vertex coordinate outside the supported domain");
-    }
-    cudaError_t e = build_bvh(m->b, false, c->pool, st);
-    // on an error the stream may still hold kernels that use the mesh: drain it before freeing
-    cudaError_t es = cudaStreamSynchronize(st);
-    if (e == cudaSuccess) e = es;
-    if (e != cudaSuccess) {
-        mesh_free(c, m, st);
-        return sk.fail(e == cudaErrorMemoryAllocation ? GI_ERR_OOM : GI_ERR_CUDA, "BVH build", e);
     }
     c->mesh_bytes += m->b.bytes;
     if (c->budget && c->mesh_bytes > c->budget) {
@@ -212,6 +216,7 @@ static gi_status mesh_finish(gi_ctx* c, gi_mesh* m, gi_mesh** out, cudaStream_t 
 
 static gi_status mesh_alloc(gi_ctx* c, uint32_t nv, uint32_t nt, gi_mesh** pm, cudaStream_t st, const UploadSink& sk)
 {
+    if (nt && !nv) return sk.fail(GI_ERR_INVALID_ARG, "triangle index out of range");  // no vertex to index
     gi_mesh* m = new (std::nothrow) gi_mesh();
     if (!m) return GI_ERR_OOM;
     m->ctx = c;
@@ -322,8 +327,8 @@ static void mesh_free(gi_ctx* c, gi_mesh* m, cudaStream_t st)
 {
     cudaSetDevice(c->device);
     // stream-ordered: work already queued on st still sees the mesh
-    void* p[] = {m->b.verts,     m->b.tris,    m->b.leafTri, m->b.leafBox, m->b.nodes,
-                 m->b.leafBox64, m->b.nodes64, m->b.cutRef,  m->b.cutBox,  m->b.cutBox64};
+    void* p[] = {m->b.verts,   m->b.tris,   m->b.leafTri, m->b.leafBox,  m->b.nodes,   m->b.leafBox64,
+                 m->b.nodes64, m->b.cutRef, m->b.cutBox,  m->b.cutBox64, m->b.ncuts};
     for (void* q : p)
         if (q) cudaFreeAsync(q, st);
     if (m->b.bytes <= c->mesh_bytes) c->mesh_bytes -= m->b.bytes;
@@ -487,8 +492,7 @@ MeshDev mesh_dev(const gi_mesh* m)
     d.cutRef = m->b.cutRef;
     d.cutBox = m->b.cutBox;
     d.cutBox64 = m->b.cutBox64;
-    d.ncut = m->b.ncut;
-    d.ncut4 = m->b.ncut4;
+    d.ncuts = m->b.ncuts;
     d.root = m->b.root;
     d.nv = m->b.nv;
     d.nt = m->b.nt;

@@ -66,8 +66,7 @@ struct MeshDev {
     const double* cutBox64;  // FP64 boxes of the same cuts (FP64 form)
     uint32_t root;  // wide node index, or kLeaf | leaf position when nt == 1
     uint32_t nv, nt, nnodes;
-    uint32_t ncut;   // entries of the depth-3 cut
-    uint32_t ncut4;  // entries of the depth-4 cut
+    const uint32_t* ncuts;  // device: entries of the depth-3 and the depth-4 cut (null for an empty mesh)
 };
 
 constexpr int kCutMax = 64;    // 4^3

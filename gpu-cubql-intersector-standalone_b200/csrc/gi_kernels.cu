@@ -96,7 +96,7 @@ __device__ __forceinline__ void store_box(S* p, const S b[6])
 // centroid bounds.  The reference rounds to nearest (src/common/utils.cu:639),
 // which can drop true pairs; outward rounding keeps the candidate set a superset.
 constexpr int kTriBoxThreads = 256;
-__global__ void __launch_bounds__(kTriBoxThreads, 4) k_tri_boxes(const double* __restrict__ V,
+__global__ void __launch_bounds__(kTriBoxThreads, 4) k_tri_boxes(const double* __restrict__ V, uint32_t nv,
                                                               const uint32_t* __restrict__ T, uint32_t nt,
                                                               float* __restrict__ box, double* __restrict__ box64,
                                                               unsigned* __restrict__ cb)
@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(kTriBoxThreads, 4) k_tri_boxes(const double* _
 #pragma unroll
         for (int q = 0; q < 2; q++)
 #pragma unroll
-            for (int j = 0; j < 3; j++) ix[q][j] = T[3 * (size_t)tt[q] + j];
+            for (int j = 0; j < 3; j++) ix[q][j] = min(T[3 * (size_t)tt[q] + j], nv - 1u);  // validated later
 #pragma unroll
         for (int q = 0; q < 2; q++)
 #pragma unroll
@@ -489,7 +489,7 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaMemPool_t pool, cudaStream_
     int gb = (int)((n + tb - 1) / tb);
     // four resident blocks per SM, each looping: the centroid bounds take one set of atomics per block
     const int gboxes = (int)((n + 2 * kTriBoxThreads - 1) / (2 * kTriBoxThreads));
-    k_tri_boxes<<<gboxes < 592 ? gboxes : 592, kTriBoxThreads, 0, st>>>(m.verts, m.tris, n, box, box64, cb);
+    k_tri_boxes<<<gboxes < 592 ? gboxes : 592, kTriBoxThreads, 0, st>>>(m.verts, m.nv, m.tris, n, box, box64, cb);
     k_morton<<<gb, tb, 0, st>>>(box, n, cb, k0, v0);
     radix_sort<uint32_t, kMortonDigit>(k0, v0, k1, v1, n, 30, counts, stemp, st);
     // leaves in sorted order
@@ -538,10 +538,11 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaMemPool_t pool, cudaStream_
         m.nnodes = nw;
         m.root = 0;
     }
-    // depth-3 and depth-4 cuts (refs shared by both precisions; boxes per precision)
+    // depth-3 and depth-4 cuts (refs and sizes shared by both precisions; boxes per
+    // precision); the sizes stay on the device, where the seeding reads them
     {
-        uint32_t* d_n = nullptr;
-        GI_TRY(pool_alloc(&d_n, sizeof(uint32_t) * 2, pool, st));
+        if (!m.ncuts) GI_TRY(pool_alloc(&m.ncuts, sizeof(uint32_t) * 2, pool, st));
+        uint32_t* d_n = m.ncuts;
         if (!m.cutRef) GI_TRY(pool_alloc(&m.cutRef, sizeof(uint32_t) * kCutCap, pool, st));
         if (!fp64) {
             GI_TRY(pool_alloc(&m.cutBox, sizeof(float) * 6 * kCutCap, pool, st));
@@ -551,12 +552,6 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaMemPool_t pool, cudaStream_
             k_cut<double, WNode64><<<1, kCutThreads, 0, st>>>(m.nodes64, m.leafBox64, m.root, m.cutRef,
                                                                m.cutBox64, d_n);
         }
-        uint32_t hn[2] = {0, 0};
-        GI_TRY(cudaMemcpyAsync(hn, d_n, sizeof(uint32_t) * 2, cudaMemcpyDeviceToHost, st));
-        GI_TRY(cudaStreamSynchronize(st));
-        cudaFreeAsync(d_n, st);
-        m.ncut = hn[0];
-        m.ncut4 = hn[1];
     }
     GI_TRY(cudaGetLastError());
     cudaFreeAsync(box, st);
@@ -1135,8 +1130,9 @@ __device__ __forceinline__ void seed_cut_pairs(const Bufs& B, unsigned total)
             job = g / per_job;
             const unsigned t = g % per_job;
             const JobDev& J = B.jobs[job];
-            const unsigned nA = (J.A.nt && J.B.nt) ? (B.deep_seed ? J.A.ncut4 : J.A.ncut) : 0u;
-            const unsigned nB = B.deep_seed ? J.B.ncut4 : J.B.ncut;
+            const bool both = J.A.nt && J.B.nt;  // an empty mesh has no cut (null sizes)
+            const unsigned nA = both ? __ldg(J.A.ncuts + (B.deep_seed ? 1 : 0)) : 0u;
+            const unsigned nB = both ? __ldg(J.B.ncuts + (B.deep_seed ? 1 : 0)) : 0u;
             if (t < nA * nB) {
                 const unsigned i = coff + t / nB, j = coff + t % nB;
                 const S* ba_ = F64 ? (const S*)J.A.cutBox64 : (const S*)J.A.cutBox;

@@ -17,9 +17,10 @@ struct MeshBuffers {
     double* leafBox64 = nullptr;
     WNode64* nodes64 = nullptr;
     uint32_t* cutRef = nullptr;
+    uint32_t* ncuts = nullptr;  // device: sizes of the depth-3 and depth-4 cuts
     float* cutBox = nullptr;
     double* cutBox64 = nullptr;
-    uint32_t nv = 0, nt = 0, nnodes = 0, root = 0, ncut = 0, ncut4 = 0;
+    uint32_t nv = 0, nt = 0, nnodes = 0, root = 0;
     size_t bytes = 0;
 };
 
