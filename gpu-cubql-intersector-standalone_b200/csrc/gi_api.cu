@@ -187,7 +187,7 @@ static gi_status mesh_finish(gi_ctx* c, gi_mesh* m, gi_mesh** out, cudaStream_t 
     CKS(sk, pool_alloc(&d_err, sizeof(unsigned), c->pool, st), "alloc");
     CKS(sk, cudaMemsetAsync(d_err, 0, sizeof(unsigned), st), "memset");
     CKS(sk, launch_validate(m->b.verts, m->b.nv, m->b.tris, m->b.nt, d_err, st), "validate");
-    cudaError_t e = build_bvh(m->b, false, c->pool, st);
+    cudaError_t e = build_bvh(m->b, false, d_err, c->pool, st);
     unsigned herr = 0;
     // a pageable destination: the copy returns when the stream has reached it (the build is done)
     cudaError_t es = cudaMemcpyAsync(&herr, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
@@ -202,8 +202,9 @@ static gi_status mesh_finish(gi_ctx* c, gi_mesh* m, gi_mesh** out, cudaStream_t 
     }
     if (herr) {
         mesh_free(c, m, st);
-        return sk.fail((herr & 1u) ? GI_ERR_INVALID_ARG : GI_ERR_RANGE,
-                       (herr & 1u) ? "triangle index out of range" : "vertex coordinate outside the supported domain");
+        if (herr & 1u) return sk.fail(GI_ERR_INVALID_ARG, "triangle index out of range");
+        if (herr & 2u) return sk.fail(GI_ERR_RANGE, "vertex coordinate outside the supported domain");
+        return sk.fail(GI_ERR_CUDA, "BVH build: inconsistent wide-node collapse");
     }
     c->mesh_bytes += m->b.bytes;
     if (c->budget && c->mesh_bytes > c->budget) {
@@ -523,9 +524,18 @@ static gi_status ensure_fp64(gi_ctx* c, gi_mesh* m)
         m->has64 = true;
         return GI_OK;
     }
-    cudaError_t e = build_bvh(m->b, true, c->pool, c->st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    unsigned* d_err = nullptr;
+    cudaError_t e = pool_alloc(&d_err, sizeof(unsigned), c->pool, c->st);
+    if (e != cudaSuccess) return set_err(c, GI_ERR_OOM, "FP64 BVH build", e);
+    unsigned herr = 0;
+    e = cudaMemsetAsync(d_err, 0, sizeof(unsigned), c->st);
+    if (e == cudaSuccess) e = build_bvh(m->b, true, d_err, c->pool, c->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st);
+    const cudaError_t es = cudaStreamSynchronize(c->st);
+    if (e == cudaSuccess) e = es;
+    cudaFreeAsync(d_err, c->st);
     if (e != cudaSuccess) return set_err(c, GI_ERR_CUDA, "FP64 BVH build", e);
+    if (herr) return set_err(c, GI_ERR_CUDA, "FP64 BVH build: inconsistent wide-node collapse");
     m->has64 = true;
     return GI_OK;
 }

@@ -4,15 +4,16 @@
 // include/third-party/cubql/level_cut_builder.h:278-364 and forest_builder.h:405-517,
 // which loop on the host with a device sync per tree level):
 //   k_validate -> k_tri_boxes -> k_morton -> radix sort -> k_karras -> k_leaves
-//   -> k_refit (bottom-up, atomic arrival counters) -> k_depth -> scan -> k_collapse
+//   -> k_refit (bottom-up, atomic arrival counters) -> k_state_tables -> k_wide_flags
+//   -> scan -> k_collapse (size-greedy 4-wide nodes)
 // No host round trip between kernels.
 //
 // Intersect (replaces crossCheck.cu, DualTreeStep.cu, rapidDescendKernel.cu and the
 // chunk loop of SingleTreeBatchIntersector.cu:170-455 in the reference):
-//   k_traverse  one cooperative persistent launch: level-synchronous BVH4 x BVH4
-//               traversal (16 child pairs per node pair, one half-warp each),
-//               warp-aggregated appends, bounded software grid barrier between
-//               levels, then the first filter stage over all leaf pairs.
+//   k_traverse  one persistent launch: seeding from the cut pairs, BVH4 x BVH4
+//               traversal through warp stacks and a device work queue (16 child
+//               pairs per node pair; no grid barrier), and the first filter
+//               stage on the leaf pairs, run by warps without node pairs.
 //   k_exact     FP64 filter + exact integer signs for the escalated pairs.
 //   k_segments  intersection sets and correctly rounded endpoints.
 //   ordering    radix sort by (job, a, b) and gathers.
@@ -202,7 +203,9 @@ __device__ __forceinline__ int kdelta(const uint32_t* __restrict__ keys, int n, 
 }
 
 // Karras 2012 radix-tree construction over sorted Morton keys (ties by index).
-__global__ void k_karras(const uint32_t* __restrict__ keys, int n, uint2* __restrict__ child, int* __restrict__ parent)
+// cnt[i]: the number of leaves under internal node i (the length of its range).
+__global__ void k_karras(const uint32_t* __restrict__ keys, int n, uint2* __restrict__ child, int* __restrict__ parent,
+                         uint32_t* __restrict__ cnt)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
@@ -224,6 +227,7 @@ __global__ void k_karras(const uint32_t* __restrict__ keys, int n, uint2* __rest
     uint32_t left = (min(i, j) == gamma) ? (kLeaf | (uint32_t)gamma) : (uint32_t)gamma;
     uint32_t right = (max(i, j) == gamma + 1) ? (kLeaf | (uint32_t)(gamma + 1)) : (uint32_t)(gamma + 1);
     child[i] = make_uint2(left, right);
+    cnt[i] = (uint32_t)(j > i ? j - i : i - j) + 1u;
     parent[(left & kLeaf) ? (n - 1 + (int)(left & ~kLeaf)) : (int)left] = i;
     parent[(right & kLeaf) ? (n - 1 + (int)(right & ~kLeaf)) : (int)right] = i;
     if (i == 0) parent[0] = -1;
@@ -307,42 +311,149 @@ __global__ void k_refit(int n, const uint2* __restrict__ child, const int* __res
     }
 }
 
-__global__ void k_depth(int n, const int* __restrict__ parent, uint32_t* __restrict__ even)
+// ---------------------------------------------------------------------------
+// Collapse of the binary radix tree into the 4-wide BVH, size-greedy.
+//
+// A wide node is made from a binary node r by opening r and then, twice, the
+// part with the most leaves (ties: the leftmost part), as long as that part is
+// an internal node; the parts stay in left-to-right order.  Each binary node is
+// thus either a wide node (state W) or opened in the second (O2) or third (O3)
+// step of its wide ancestor's expansion.  Opening the largest part shrinks
+// the largest subtree of a wide node faster than taking grandchildren by
+// depth parity does on the unbalanced trees that Morton splits give on a
+// surface: on a 1.3 M-triangle sphere the pair tree of two such meshes has a
+// level and a fifth of its node pairs fewer.
+//
+// A node's state follows from its parent's through a 3-entry table that
+// depends only on the leaf counts around it (k_state_tables).  k_wide_flags
+// composes the tables up the parent chain until the composition no longer
+// depends on the state above (about five steps a node), so no top-down pass
+// over the levels is needed.
+constexpr unsigned kStW = 0u, kStO2 = 1u, kStO3 = 2u;
+
+__device__ __forceinline__ uint32_t leaves_under(const uint32_t* __restrict__ cnt, uint32_t ref)
+{
+    return (ref & kLeaf) ? 1u : __ldg(cnt + ref);
+}
+
+// position (0..2) of the first maximum of three counts
+__device__ __forceinline__ unsigned first_max3(uint32_t a, uint32_t b, uint32_t c)
+{
+    unsigned k = 0;
+    uint32_t m = a;
+    if (b > m) {
+        m = b;
+        k = 1;
+    }
+    if (c > m) k = 2;
+    return k;
+}
+
+// tab[y] bits 2s..2s+1: the state of internal node y (y >= 1) when its parent
+// is in state s (s = W, O2; a child of an O3 node is always W).
+__global__ void k_state_tables(int n, const uint2* __restrict__ child, const int* __restrict__ parent,
+                               const uint32_t* __restrict__ cnt, uint8_t* __restrict__ tab)
+{
+    int y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (y < 1 || y >= n - 1) return;
+    const int p = parent[y];
+    const uint2 c = child[p];
+    const bool left = c.x == (uint32_t)y;
+    const uint32_t z = left ? c.y : c.x;
+    const uint32_t ny = cnt[y], nz = leaves_under(cnt, z);
+    // parent in W: step 2 opens the larger child (tie: the left one)
+    unsigned sW;
+    if (left ? ny >= nz : ny > nz) {
+        sW = kStO2;
+    } else {  // the sibling z (internal: nz > ny >= 2) was opened; step 3 over the three parts
+        const uint2 g = child[z];
+        const uint32_t n0 = leaves_under(cnt, g.x), n1 = leaves_under(cnt, g.y);
+        sW = (left ? first_max3(ny, n0, n1) == 0u : first_max3(n0, n1, ny) == 2u) ? kStO3 : kStW;
+    }
+    // parent in O2 (opened by its own parent r): step 3 over p's children and p's sibling
+    unsigned sO2 = kStW;
+    const int r = parent[p];
+    if (r >= 0) {
+        const uint2 cr = child[r];
+        const bool pleft = cr.x == (uint32_t)p;
+        const uint32_t ns = leaves_under(cnt, pleft ? cr.y : cr.x);
+        const uint32_t n0 = leaves_under(cnt, c.x), n1 = leaves_under(cnt, c.y);
+        const unsigned mine = pleft ? (left ? 0u : 1u) : (left ? 1u : 2u);
+        const unsigned k = pleft ? first_max3(n0, n1, ns) : first_max3(ns, n0, n1);
+        sO2 = k == mine ? kStO3 : kStW;
+    }
+    tab[y] = (uint8_t)(sW | (sO2 << 2) | (kStW << 4));
+}
+
+// wide[i] = 1 iff binary node i becomes a wide node.
+__global__ void k_wide_flags(int n, const int* __restrict__ parent, const uint8_t* __restrict__ tab,
+                             uint32_t* __restrict__ wide)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
-    int d = 0, x = i;
-    while (x > 0 && d < n) {
-        x = parent[x];
-        d++;
+    if (i == 0) {
+        wide[0] = 1u;
+        return;
     }
-    even[i] = (d & 1) == 0;
+    unsigned f = tab[i];  // state of i as a function of the state of the node above the chain
+    int x = parent[i];
+    for (int guard = 0; x > 0 && guard < n; guard++) {
+        const unsigned f0 = f & 3u, f1 = (f >> 2) & 3u, f2 = (f >> 4) & 3u;
+        if (f0 == f1 && f1 == f2) break;
+        const unsigned t = __ldg(tab + x);
+        f = ((f >> (2u * (t & 3u))) & 3u) | (((f >> (2u * ((t >> 2) & 3u))) & 3u) << 2) |
+            (((f >> (2u * ((t >> 4) & 3u))) & 3u) << 4);
+        x = parent[x];
+    }
+    wide[i] = (f & 3u) == kStW ? 1u : 0u;  // the root is a wide node
 }
 
+// Writes wide node widx[i] from binary node i: the size-greedy expansion of i
+// (the same choices as k_state_tables).  An internal part that is not a wide
+// node, or whose index is out of range, cannot arise; it is written as an
+// empty slot and flagged in *bad rather than followed.
 template <class S, class NodeT>
-__global__ void k_collapse(int n, const uint2* __restrict__ child, const uint32_t* __restrict__ even,
-                           const uint32_t* __restrict__ widx, const S* __restrict__ leafBox,
-                           const S* __restrict__ nodeBox, NodeT* __restrict__ nodes)
+__global__ void k_collapse(int n, const uint2* __restrict__ child, const uint32_t* __restrict__ cnt,
+                           const uint32_t* __restrict__ wide, const uint32_t* __restrict__ widx, uint32_t nw,
+                           const S* __restrict__ leafBox, const S* __restrict__ nodeBox, NodeT* __restrict__ nodes,
+                           unsigned* __restrict__ bad)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n - 1 || !even[i]) return;
-    uint32_t slot[4];
-    int ns = 0;
-    uint2 c = child[i];
-    uint32_t cc[2] = {c.x, c.y};
-    for (int s = 0; s < 2; s++) {
-        if (cc[s] & kLeaf) {
-            slot[ns++] = cc[s];
-        } else {
-            uint2 g = child[cc[s]];
-            slot[ns++] = g.x;
-            slot[ns++] = g.y;
+    if (i >= n - 1 || !wide[i]) return;
+    const uint32_t wi = widx[i];
+    if (wi >= nw) {
+        atomicOr(bad, 1u);
+        return;
+    }
+    const uint2 c = child[i];
+    uint32_t slot[4] = {c.x, c.y, kEmpty, kEmpty};
+    uint32_t num[4] = {leaves_under(cnt, c.x), leaves_under(cnt, c.y), 0u, 0u};
+    int ns = 2;
+#pragma unroll
+    for (int step = 0; step < 2; step++) {
+        int b = 0;
+        for (int k = 1; k < ns; k++)
+            if (num[k] > num[b]) b = k;
+        if (num[b] < 2u) break;
+        const uint2 g = child[slot[b]];
+        for (int k = ns; k > b + 1; k--) {
+            slot[k] = slot[k - 1];
+            num[k] = num[k - 1];
         }
+        slot[b] = g.x;
+        slot[b + 1] = g.y;
+        num[b] = leaves_under(cnt, g.x);
+        num[b + 1] = leaves_under(cnt, g.y);
+        ns++;
     }
     NodeT out;
     for (int k = 0; k < 4; k++) {
-        if (k < ns) {
-            uint32_t r = slot[k];
+        uint32_t r = k < ns ? slot[k] : kEmpty;
+        if (r != kEmpty && !(r & kLeaf) && (!wide[r] || widx[r] >= nw)) {
+            atomicOr(bad, 1u);
+            r = kEmpty;
+        }
+        if (r != kEmpty) {
             const S* src = (r & kLeaf) ? leafBox + 6 * (size_t)(r & ~kLeaf) : nodeBox + 6 * (size_t)r;
             out.lox[k] = src[0];
             out.loy[k] = src[1];
@@ -358,7 +469,7 @@ __global__ void k_collapse(int n, const uint2* __restrict__ child, const uint32_
         }
     }
     for (int k = 0; k < (int)(sizeof(out.pad) / sizeof(out.pad[0])); k++) out.pad[k] = 0;
-    nodes[widx[i]] = out;
+    nodes[wi] = out;
 }
 
 // Cuts of the wide BVH: the root expanded three and four times (leaves met on
@@ -453,7 +564,7 @@ cudaError_t launch_validate(const double* verts, uint32_t nv, const uint32_t* tr
         if (e_ != cudaSuccess) return e_;        \
     } while (0)
 
-cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaMemPool_t pool, cudaStream_t st)
+cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t pool, cudaStream_t st)
 {
     const uint32_t n = m.nt;
     if (n == 0) {
@@ -469,7 +580,8 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaMemPool_t pool, cudaStream_
     uint2* child = nullptr;
     int* parent = nullptr;
     unsigned* flags = nullptr;
-    uint32_t *even = nullptr, *widx = nullptr;
+    uint32_t *wide = nullptr, *widx = nullptr, *cnt = nullptr;
+    uint8_t* tab = nullptr;
     void* nodeBox = nullptr;
     constexpr int kMortonDigit = 10;  // 30-bit keys: three passes
     size_t cw = radix_counts_words<kMortonDigit>(n);
@@ -508,32 +620,35 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaMemPool_t pool, cudaStream_
         GI_TRY(pool_alloc(&child, sizeof(uint2) * (n - 1), pool, st));
         GI_TRY(pool_alloc(&parent, sizeof(int) * (2 * (size_t)n - 1), pool, st));
         GI_TRY(pool_alloc(&flags, sizeof(unsigned) * (n - 1), pool, st));
-        GI_TRY(pool_alloc(&even, sizeof(uint32_t) * (n - 1), pool, st));
+        GI_TRY(pool_alloc(&wide, sizeof(uint32_t) * (n - 1), pool, st));
+        GI_TRY(pool_alloc(&cnt, sizeof(uint32_t) * (n - 1), pool, st));
+        GI_TRY(pool_alloc(&tab, sizeof(uint8_t) * (n - 1), pool, st));
         GI_TRY(pool_alloc(&widx, sizeof(uint32_t) * (n - 1), pool, st));
         GI_TRY(pool_alloc(&nodeBox, (fp64 ? sizeof(double) : sizeof(float)) * 6 * (n - 1), pool, st));
         GI_TRY(cudaMemsetAsync(flags, 0, sizeof(unsigned) * (n - 1), st));
         int gi_ = (int)((n - 1 + tb - 1) / tb);
-        k_karras<<<gi_, tb, 0, st>>>(k0, (int)n, child, parent);
+        k_karras<<<gi_, tb, 0, st>>>(k0, (int)n, child, parent, cnt);
         if (!fp64)
             k_refit<float><<<gb, tb, 0, st>>>((int)n, child, parent, m.leafBox, (float*)nodeBox, flags);
         else
             k_refit<double><<<gb, tb, 0, st>>>((int)n, child, parent, m.leafBox64, (double*)nodeBox, flags);
-        k_depth<<<gi_, tb, 0, st>>>((int)n, parent, even);
-        scan_exclusive(even, widx, n - 1, stemp, st);
-        // number of wide nodes = widx[n-2] + even[n-2]
+        k_state_tables<<<gi_, tb, 0, st>>>((int)n, child, parent, cnt, tab);
+        k_wide_flags<<<gi_, tb, 0, st>>>((int)n, parent, tab, wide);
+        scan_exclusive(wide, widx, n - 1, stemp, st);
+        // number of wide nodes = widx[n-2] + wide[n-2]
         uint32_t last[2];
         GI_TRY(cudaMemcpyAsync(&last[0], widx + (n - 2), sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        GI_TRY(cudaMemcpyAsync(&last[1], even + (n - 2), sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        GI_TRY(cudaMemcpyAsync(&last[1], wide + (n - 2), sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         GI_TRY(cudaStreamSynchronize(st));
         uint32_t nw = last[0] + last[1];
         if (!fp64) {
             GI_TRY(pool_alloc(&m.nodes, sizeof(WNode) * (size_t)nw, pool, st));
-            k_collapse<float, WNode><<<gi_, tb, 0, st>>>((int)n, child, even, widx, m.leafBox, (float*)nodeBox,
-                                                         m.nodes);
+            k_collapse<float, WNode><<<gi_, tb, 0, st>>>((int)n, child, cnt, wide, widx, nw, m.leafBox,
+                                                         (float*)nodeBox, m.nodes, d_err);
         } else {
             GI_TRY(pool_alloc(&m.nodes64, sizeof(WNode64) * (size_t)nw, pool, st));
-            k_collapse<double, WNode64><<<gi_, tb, 0, st>>>((int)n, child, even, widx, m.leafBox64,
-                                                            (double*)nodeBox, m.nodes64);
+            k_collapse<double, WNode64><<<gi_, tb, 0, st>>>((int)n, child, cnt, wide, widx, nw, m.leafBox64,
+                                                            (double*)nodeBox, m.nodes64, d_err);
         }
         m.nnodes = nw;
         m.root = 0;
@@ -566,7 +681,9 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, cudaMemPool_t pool, cudaStream_
     if (child) cudaFreeAsync(child, st);
     if (parent) cudaFreeAsync(parent, st);
     if (flags) cudaFreeAsync(flags, st);
-    if (even) cudaFreeAsync(even, st);
+    if (wide) cudaFreeAsync(wide, st);
+    if (cnt) cudaFreeAsync(cnt, st);
+    if (tab) cudaFreeAsync(tab, st);
     if (widx) cudaFreeAsync(widx, st);
     if (nodeBox) cudaFreeAsync(nodeBox, st);
     if (!fp64)
