@@ -4,9 +4,9 @@
 // include/third-party/cubql/level_cut_builder.h:278-364 and forest_builder.h:405-517,
 // which loop on the host with a device sync per tree level):
 //   k_validate -> k_tri_boxes -> k_morton -> radix sort -> k_karras -> k_leaves
-//   -> k_refit (bottom-up, atomic arrival counters) -> k_state_tables -> k_wide_flags
-//   -> scan -> k_collapse (size-greedy 4-wide nodes)
-// No host round trip between kernels.
+//   -> k_state_tables -> k_wide_flags -> scan -> k_collapse (size-greedy 4-wide nodes,
+//   topology) -> k_refit_wide (bottom-up over the wide tree, atomic arrival counters)
+// One host round trip, for the wide-node count (the node array's size).
 //
 // Intersect (replaces crossCheck.cu, DualTreeStep.cu, rapidDescendKernel.cu and the
 // chunk loop of SingleTreeBatchIntersector.cu:170-455 in the reference):
@@ -203,9 +203,8 @@ __device__ __forceinline__ int kdelta(const uint32_t* __restrict__ keys, int n, 
 }
 
 // Karras 2012 radix-tree construction over sorted Morton keys (ties by index).
-// cnt[i]: the number of leaves under internal node i (the length of its range).
-__global__ void k_karras(const uint32_t* __restrict__ keys, int n, uint2* __restrict__ child, int* __restrict__ parent,
-                         uint32_t* __restrict__ cnt)
+// child[i] = (left ref, right ref, leaves under left, leaves under right).
+__global__ void k_karras(const uint32_t* __restrict__ keys, int n, uint4* __restrict__ child, int* __restrict__ parent)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
@@ -226,8 +225,8 @@ __global__ void k_karras(const uint32_t* __restrict__ keys, int n, uint2* __rest
     int gamma = i + s * d + min(d, 0);
     uint32_t left = (min(i, j) == gamma) ? (kLeaf | (uint32_t)gamma) : (uint32_t)gamma;
     uint32_t right = (max(i, j) == gamma + 1) ? (kLeaf | (uint32_t)(gamma + 1)) : (uint32_t)(gamma + 1);
-    child[i] = make_uint2(left, right);
-    cnt[i] = (uint32_t)(j > i ? j - i : i - j) + 1u;
+    const int lo = min(i, j), hi = max(i, j);
+    child[i] = make_uint4(left, right, (uint32_t)(gamma - lo + 1), (uint32_t)(hi - gamma));
     parent[(left & kLeaf) ? (n - 1 + (int)(left & ~kLeaf)) : (int)left] = i;
     parent[(right & kLeaf) ? (n - 1 + (int)(right & ~kLeaf)) : (int)right] = i;
     if (i == 0) parent[0] = -1;
@@ -266,51 +265,6 @@ __device__ __forceinline__ unsigned arrive_acq_rel(unsigned* f)
     return old;
 }
 
-// Bottom-up refit: the second thread to arrive at a node merges both children.
-// A thread keeps its own subtree's box in registers and reads only the
-// sibling's; the tree links of the next level do not depend on other threads
-// and are loaded while the sibling's box is in flight, so a level costs the
-// arrival atomic and one box load.
-template <class S>
-__global__ void k_refit(int n, const uint2* __restrict__ child, const int* __restrict__ parent,
-                        const S* __restrict__ leafBox, S* nodeBox, unsigned* flags)
-{
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    S b[6];
-    load_box_cg(leafBox + 6 * (size_t)p, b);
-    uint32_t self = kLeaf | (uint32_t)p;
-    int node = parent[n - 1 + p];
-    if (node < 0) return;
-    uint2 c = child[node];
-    int up = parent[node];
-    for (int guard = 0; guard < n; guard++) {
-        // release: this thread's box stores (the previous level) before the
-        // arrival; acquire: the sibling's box stores after it
-        if (arrive_acq_rel(&flags[node]) == 0u) return;
-        uint2 cn = make_uint2(0u, 0u);
-        int upn = -1;
-        if (up >= 0) {
-            cn = child[up];
-            upn = parent[up];
-        }
-        const uint32_t sib = c.x == self ? c.y : c.x;
-        const S* src = (sib & kLeaf) ? leafBox + 6 * (size_t)(sib & ~kLeaf) : nodeBox + 6 * (size_t)sib;
-        S o[6];
-        load_box_cg(src, o);
-        for (int k = 0; k < 3; k++) {
-            b[k] = o[k] < b[k] ? o[k] : b[k];
-            b[3 + k] = o[3 + k] > b[3 + k] ? o[3 + k] : b[3 + k];
-        }
-        store_box(nodeBox + 6 * (size_t)node, b);
-        if (up < 0) return;
-        self = (uint32_t)node;
-        node = up;
-        c = cn;
-        up = upn;
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Collapse of the binary radix tree into the 4-wide BVH, size-greedy.
 //
@@ -330,11 +284,7 @@ __global__ void k_refit(int n, const uint2* __restrict__ child, const int* __res
 // depends on the state above (about five steps a node), so no top-down pass
 // over the levels is needed.
 constexpr unsigned kStW = 0u, kStO2 = 1u, kStO3 = 2u;
-
-__device__ __forceinline__ uint32_t leaves_under(const uint32_t* __restrict__ cnt, uint32_t ref)
-{
-    return (ref & kLeaf) ? 1u : __ldg(cnt + ref);
-}
+constexpr unsigned kErrBuild = 4u;  // error word bit: an inconsistent wide tree (not expected)
 
 // position (0..2) of the first maximum of three counts
 __device__ __forceinline__ unsigned first_max3(uint32_t a, uint32_t b, uint32_t c)
@@ -351,33 +301,33 @@ __device__ __forceinline__ unsigned first_max3(uint32_t a, uint32_t b, uint32_t 
 
 // tab[y] bits 2s..2s+1: the state of internal node y (y >= 1) when its parent
 // is in state s (s = W, O2; a child of an O3 node is always W).
-__global__ void k_state_tables(int n, const uint2* __restrict__ child, const int* __restrict__ parent,
-                               const uint32_t* __restrict__ cnt, uint8_t* __restrict__ tab)
+__global__ void k_state_tables(int n, const uint4* __restrict__ child, const int* __restrict__ parent,
+                               uint8_t* __restrict__ tab)
 {
     int y = blockIdx.x * blockDim.x + threadIdx.x;
     if (y < 1 || y >= n - 1) return;
     const int p = parent[y];
-    const uint2 c = child[p];
+    const uint4 c = child[p];
     const bool left = c.x == (uint32_t)y;
     const uint32_t z = left ? c.y : c.x;
-    const uint32_t ny = cnt[y], nz = leaves_under(cnt, z);
+    const uint32_t ny = left ? c.z : c.w, nz = left ? c.w : c.z;
     // parent in W: step 2 opens the larger child (tie: the left one)
     unsigned sW;
     if (left ? ny >= nz : ny > nz) {
         sW = kStO2;
     } else {  // the sibling z (internal: nz > ny >= 2) was opened; step 3 over the three parts
-        const uint2 g = child[z];
-        const uint32_t n0 = leaves_under(cnt, g.x), n1 = leaves_under(cnt, g.y);
+        const uint4 g = child[z];
+        const uint32_t n0 = g.z, n1 = g.w;
         sW = (left ? first_max3(ny, n0, n1) == 0u : first_max3(n0, n1, ny) == 2u) ? kStO3 : kStW;
     }
     // parent in O2 (opened by its own parent r): step 3 over p's children and p's sibling
     unsigned sO2 = kStW;
     const int r = parent[p];
     if (r >= 0) {
-        const uint2 cr = child[r];
+        const uint4 cr = child[r];
         const bool pleft = cr.x == (uint32_t)p;
-        const uint32_t ns = leaves_under(cnt, pleft ? cr.y : cr.x);
-        const uint32_t n0 = leaves_under(cnt, c.x), n1 = leaves_under(cnt, c.y);
+        const uint32_t ns = pleft ? cr.w : cr.z;
+        const uint32_t n0 = c.z, n1 = c.w;
         const unsigned mine = pleft ? (left ? 0u : 1u) : (left ? 1u : 2u);
         const unsigned k = pleft ? first_max3(n0, n1, ns) : first_max3(ns, n0, n1);
         sO2 = k == mine ? kStO3 : kStW;
@@ -409,25 +359,29 @@ __global__ void k_wide_flags(int n, const int* __restrict__ parent, const uint8_
 }
 
 // Writes wide node widx[i] from binary node i: the size-greedy expansion of i
-// (the same choices as k_state_tables).  An internal part that is not a wide
-// node, or whose index is out of range, cannot arise; it is written as an
-// empty slot and flagged in *bad rather than followed.
+// (the same choices as k_state_tables).  Topology only: the child refs, and
+// for each child the (wide node, slot) it sits in (leafUp for leaves, nodeUp
+// for wide nodes; the root's is kEmpty) and the node's child count, from
+// which k_refit_wide fills the slot boxes.  An internal part that is not a
+// wide node, or whose index is out of range, cannot arise; it is written as
+// an empty slot and flagged in *bad rather than followed.
 template <class S, class NodeT>
-__global__ void k_collapse(int n, const uint2* __restrict__ child, const uint32_t* __restrict__ cnt,
-                           const uint32_t* __restrict__ wide, const uint32_t* __restrict__ widx, uint32_t nw,
-                           const S* __restrict__ leafBox, const S* __restrict__ nodeBox, NodeT* __restrict__ nodes,
+__global__ void k_collapse(int n, const uint4* __restrict__ child, const uint32_t* __restrict__ wide,
+                           const uint32_t* __restrict__ widx, uint32_t nw, NodeT* __restrict__ nodes,
+                           uint2* __restrict__ leafUp, uint2* __restrict__ nodeUp, uint32_t* __restrict__ nkids,
                            unsigned* __restrict__ bad)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1 || !wide[i]) return;
     const uint32_t wi = widx[i];
     if (wi >= nw) {
-        atomicOr(bad, 1u);
+        atomicOr(bad, kErrBuild);
         return;
     }
-    const uint2 c = child[i];
+    if (wi == 0u) nodeUp[0] = make_uint2(kEmpty, 0u);
+    const uint4 c = child[i];
     uint32_t slot[4] = {c.x, c.y, kEmpty, kEmpty};
-    uint32_t num[4] = {leaves_under(cnt, c.x), leaves_under(cnt, c.y), 0u, 0u};
+    uint32_t num[4] = {c.z, c.w, 0u, 0u};
     int ns = 2;
 #pragma unroll
     for (int step = 0; step < 2; step++) {
@@ -435,41 +389,106 @@ __global__ void k_collapse(int n, const uint2* __restrict__ child, const uint32_
         for (int k = 1; k < ns; k++)
             if (num[k] > num[b]) b = k;
         if (num[b] < 2u) break;
-        const uint2 g = child[slot[b]];
+        const uint4 g = child[slot[b]];
         for (int k = ns; k > b + 1; k--) {
             slot[k] = slot[k - 1];
             num[k] = num[k - 1];
         }
         slot[b] = g.x;
         slot[b + 1] = g.y;
-        num[b] = leaves_under(cnt, g.x);
-        num[b + 1] = leaves_under(cnt, g.y);
+        num[b] = g.z;
+        num[b + 1] = g.w;
         ns++;
     }
     NodeT out;
+    uint32_t kids = 0;
     for (int k = 0; k < 4; k++) {
         uint32_t r = k < ns ? slot[k] : kEmpty;
         if (r != kEmpty && !(r & kLeaf) && (!wide[r] || widx[r] >= nw)) {
-            atomicOr(bad, 1u);
+            atomicOr(bad, kErrBuild);
             r = kEmpty;
         }
-        if (r != kEmpty) {
-            const S* src = (r & kLeaf) ? leafBox + 6 * (size_t)(r & ~kLeaf) : nodeBox + 6 * (size_t)r;
-            out.lox[k] = src[0];
-            out.loy[k] = src[1];
-            out.loz[k] = src[2];
-            out.hix[k] = src[3];
-            out.hiy[k] = src[4];
-            out.hiz[k] = src[5];
-            out.child[k] = (r & kLeaf) ? r : widx[r];
-        } else {
-            out.lox[k] = out.loy[k] = out.loz[k] = (S)INFINITY;
-            out.hix[k] = out.hiy[k] = out.hiz[k] = (S)-INFINITY;
+        out.lox[k] = out.loy[k] = out.loz[k] = (S)INFINITY;
+        out.hix[k] = out.hiy[k] = out.hiz[k] = (S)-INFINITY;
+        if (r == kEmpty) {
             out.child[k] = kEmpty;
+            continue;
+        }
+        kids++;
+        if (r & kLeaf) {
+            out.child[k] = r;
+            leafUp[r & ~kLeaf] = make_uint2(wi, (uint32_t)k);
+        } else {
+            const uint32_t cw = widx[r];
+            out.child[k] = cw;
+            nodeUp[cw] = make_uint2(wi, (uint32_t)k);
         }
     }
     for (int k = 0; k < (int)(sizeof(out.pad) / sizeof(out.pad[0])); k++) out.pad[k] = 0;
+    nkids[wi] = kids;
     nodes[wi] = out;
+}
+
+// The six child-box fields of a wide node, read through L2 (other threads of
+// the same launch wrote them): the union of its slots (empty slots hold
+// +inf / -inf and change nothing).
+__device__ __forceinline__ void node_union_cg(const WNode* nd, float b[6])
+{
+    const float4* q = reinterpret_cast<const float4*>(nd);
+#pragma unroll
+    for (int f = 0; f < 6; f++) {
+        const float4 v = __ldcg(q + f);
+        b[f] = f < 3 ? fminf(fminf(v.x, v.y), fminf(v.z, v.w)) : fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w));
+    }
+}
+__device__ __forceinline__ void node_union_cg(const WNode64* nd, double b[6])
+{
+    const double2* q = reinterpret_cast<const double2*>(nd);
+#pragma unroll
+    for (int f = 0; f < 6; f++) {
+        const double2 v = __ldcg(q + 2 * f), w = __ldcg(q + 2 * f + 1);
+        b[f] = f < 3 ? fmin(fmin(v.x, v.y), fmin(w.x, w.y)) : fmax(fmax(v.x, v.y), fmax(w.x, w.y));
+    }
+}
+
+// Bottom-up refit of the wide tree, one thread per leaf: a thread stores its
+// box into its slot of the node above and arrives there; the thread that
+// arrives last (after the node's other children) takes the union of the
+// node's slots and climbs on.  The links of the node above are loaded while
+// the arrival is in flight, so a level costs the slot stores, the arrival
+// atomic and one read of the node's six box fields; the wide tree has about
+// half the levels of the binary one.
+template <class S, class NodeT>
+__global__ void k_refit_wide(uint32_t n, uint32_t nw, const uint2* __restrict__ leafUp,
+                             const uint2* __restrict__ nodeUp, const uint32_t* __restrict__ nkids,
+                             const S* __restrict__ leafBox, NodeT* nodes, unsigned* arrive, unsigned* bad)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    S b[6];
+    load_box_cg(leafBox + 6 * (size_t)p, b);
+    uint2 up = leafUp[p];
+    for (uint32_t guard = 0; guard < n; guard++) {
+        const uint32_t w = up.x, k = up.y & 3u;
+        if (w >= nw) {
+            atomicOr(bad, kErrBuild);
+            return;
+        }
+        NodeT* nd = nodes + w;
+        nd->lox[k] = b[0];
+        nd->loy[k] = b[1];
+        nd->loz[k] = b[2];
+        nd->hix[k] = b[3];
+        nd->hiy[k] = b[4];
+        nd->hiz[k] = b[5];
+        const uint2 upn = nodeUp[w];
+        const uint32_t need = nkids[w];
+        // release: this slot's stores before the arrival; acquire: the other slots' after it
+        if (arrive_acq_rel(&arrive[w]) + 1u != need) return;
+        node_union_cg(nd, b);
+        if (upn.x == kEmpty) return;  // the root
+        up = upn;
+    }
 }
 
 // Cuts of the wide BVH: the root expanded three and four times (leaves met on
@@ -577,12 +596,13 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t 
     double* box64 = nullptr;
     unsigned* cb = nullptr;
     uint32_t *k0 = nullptr, *v0 = nullptr, *k1 = nullptr, *v1 = nullptr, *counts = nullptr, *stemp = nullptr;
-    uint2* child = nullptr;
+    uint4* child = nullptr;
     int* parent = nullptr;
-    unsigned* flags = nullptr;
-    uint32_t *wide = nullptr, *widx = nullptr, *cnt = nullptr;
+    unsigned* arrive = nullptr;
+    uint2 *leafUp = nullptr, *nodeUp = nullptr;
+    uint32_t* nkids = nullptr;
+    uint32_t *wide = nullptr, *widx = nullptr;
     uint8_t* tab = nullptr;
-    void* nodeBox = nullptr;
     constexpr int kMortonDigit = 10;  // 30-bit keys: three passes
     size_t cw = radix_counts_words<kMortonDigit>(n);
     size_t sw = scan_temp_words(cw > n ? cw : n);
@@ -617,22 +637,15 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t 
         m.root = kLeaf | 0u;
         m.nnodes = 0;
     } else {
-        GI_TRY(pool_alloc(&child, sizeof(uint2) * (n - 1), pool, st));
+        GI_TRY(pool_alloc(&child, sizeof(uint4) * (n - 1), pool, st));
         GI_TRY(pool_alloc(&parent, sizeof(int) * (2 * (size_t)n - 1), pool, st));
-        GI_TRY(pool_alloc(&flags, sizeof(unsigned) * (n - 1), pool, st));
         GI_TRY(pool_alloc(&wide, sizeof(uint32_t) * (n - 1), pool, st));
-        GI_TRY(pool_alloc(&cnt, sizeof(uint32_t) * (n - 1), pool, st));
         GI_TRY(pool_alloc(&tab, sizeof(uint8_t) * (n - 1), pool, st));
         GI_TRY(pool_alloc(&widx, sizeof(uint32_t) * (n - 1), pool, st));
-        GI_TRY(pool_alloc(&nodeBox, (fp64 ? sizeof(double) : sizeof(float)) * 6 * (n - 1), pool, st));
-        GI_TRY(cudaMemsetAsync(flags, 0, sizeof(unsigned) * (n - 1), st));
+        GI_TRY(pool_alloc(&leafUp, sizeof(uint2) * n, pool, st));
         int gi_ = (int)((n - 1 + tb - 1) / tb);
-        k_karras<<<gi_, tb, 0, st>>>(k0, (int)n, child, parent, cnt);
-        if (!fp64)
-            k_refit<float><<<gb, tb, 0, st>>>((int)n, child, parent, m.leafBox, (float*)nodeBox, flags);
-        else
-            k_refit<double><<<gb, tb, 0, st>>>((int)n, child, parent, m.leafBox64, (double*)nodeBox, flags);
-        k_state_tables<<<gi_, tb, 0, st>>>((int)n, child, parent, cnt, tab);
+        k_karras<<<gi_, tb, 0, st>>>(k0, (int)n, child, parent);
+        k_state_tables<<<gi_, tb, 0, st>>>((int)n, child, parent, tab);
         k_wide_flags<<<gi_, tb, 0, st>>>((int)n, parent, tab, wide);
         scan_exclusive(wide, widx, n - 1, stemp, st);
         // number of wide nodes = widx[n-2] + wide[n-2]
@@ -641,14 +654,22 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t 
         GI_TRY(cudaMemcpyAsync(&last[1], wide + (n - 2), sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         GI_TRY(cudaStreamSynchronize(st));
         uint32_t nw = last[0] + last[1];
+        GI_TRY(pool_alloc(&nodeUp, sizeof(uint2) * (size_t)nw, pool, st));
+        GI_TRY(pool_alloc(&nkids, sizeof(uint32_t) * (size_t)nw, pool, st));
+        GI_TRY(pool_alloc(&arrive, sizeof(unsigned) * (size_t)nw, pool, st));
+        GI_TRY(cudaMemsetAsync(arrive, 0, sizeof(unsigned) * (size_t)nw, st));
         if (!fp64) {
             GI_TRY(pool_alloc(&m.nodes, sizeof(WNode) * (size_t)nw, pool, st));
-            k_collapse<float, WNode><<<gi_, tb, 0, st>>>((int)n, child, cnt, wide, widx, nw, m.leafBox,
-                                                         (float*)nodeBox, m.nodes, d_err);
+            k_collapse<float, WNode><<<gi_, tb, 0, st>>>((int)n, child, wide, widx, nw, m.nodes, leafUp, nodeUp,
+                                                         nkids, d_err);
+            k_refit_wide<float, WNode><<<gb, tb, 0, st>>>(n, nw, leafUp, nodeUp, nkids, m.leafBox, m.nodes, arrive,
+                                                          d_err);
         } else {
             GI_TRY(pool_alloc(&m.nodes64, sizeof(WNode64) * (size_t)nw, pool, st));
-            k_collapse<double, WNode64><<<gi_, tb, 0, st>>>((int)n, child, cnt, wide, widx, nw, m.leafBox64,
-                                                            (double*)nodeBox, m.nodes64, d_err);
+            k_collapse<double, WNode64><<<gi_, tb, 0, st>>>((int)n, child, wide, widx, nw, m.nodes64, leafUp,
+                                                            nodeUp, nkids, d_err);
+            k_refit_wide<double, WNode64><<<gb, tb, 0, st>>>(n, nw, leafUp, nodeUp, nkids, m.leafBox64, m.nodes64,
+                                                             arrive, d_err);
         }
         m.nnodes = nw;
         m.root = 0;
@@ -680,12 +701,13 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t 
     cudaFreeAsync(stemp, st);
     if (child) cudaFreeAsync(child, st);
     if (parent) cudaFreeAsync(parent, st);
-    if (flags) cudaFreeAsync(flags, st);
+    if (arrive) cudaFreeAsync(arrive, st);
+    if (leafUp) cudaFreeAsync(leafUp, st);
+    if (nodeUp) cudaFreeAsync(nodeUp, st);
+    if (nkids) cudaFreeAsync(nkids, st);
     if (wide) cudaFreeAsync(wide, st);
-    if (cnt) cudaFreeAsync(cnt, st);
     if (tab) cudaFreeAsync(tab, st);
     if (widx) cudaFreeAsync(widx, st);
-    if (nodeBox) cudaFreeAsync(nodeBox, st);
     if (!fp64)
         m.bytes += sizeof(float) * 6 * (size_t)n + sizeof(uint4) * (size_t)n + sizeof(WNode) * (size_t)m.nnodes;
     else

@@ -41,7 +41,8 @@ cudaError_t launch_validate(const double* verts, uint32_t nv, const uint32_t* tr
                             cudaStream_t st);
 
 // Builds the 4-wide BVH (FP32 boxes) or, with fp64 = true, the FP64 node copy.
-// d_err: bit 2 (4u) is set if the collapse met an inconsistent tree (not expected).
+// d_err: a device word (required); bit 2 (4u) is set if the wide tree came out
+// inconsistent (not expected; the kernels then skip the bad links).
 cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t pool, cudaStream_t st);
 
 // Intersect launch configuration.
