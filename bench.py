@@ -42,8 +42,8 @@ sys.path.insert(0, PKG)
 
 METRIC = "ms/intersect at 2×1.3M tris & tri-pair tests/s; pose-update p50/p99 vs FP64 path"
 # DRAM bytes of one k_traverse launch on the level-8 pose workload, from an ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum = 18.27 MB + 0.86 MB)
-TRAVERSE_DRAM_BYTES = 19.17e6
+# capture (dram__bytes_read.sum + dram__bytes_write.sum = 17.08 MB + 0.87 MB)
+TRAVERSE_DRAM_BYTES = 17.94e6
 
 
 def parse():
