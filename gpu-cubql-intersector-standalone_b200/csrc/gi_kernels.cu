@@ -359,17 +359,19 @@ __global__ void k_wide_flags(int n, const int* __restrict__ parent, const uint8_
 }
 
 // Writes wide node widx[i] from binary node i: the size-greedy expansion of i
-// (the same choices as k_state_tables).  Topology only: the child refs, and
-// for each child the (wide node, slot) it sits in (leafUp for leaves, nodeUp
-// for wide nodes; the root's is kEmpty) and the node's child count, from
-// which k_refit_wide fills the slot boxes.  An internal part that is not a
-// wide node, or whose index is out of range, cannot arise; it is written as
-// an empty slot and flagged in *bad rather than followed.
+// (the same choices as k_state_tables), with the boxes of its leaf children
+// (consecutive leaves: the loads of neighbouring threads share lines); the
+// boxes of wide children are filled by k_refit_wide.  For each wide child it
+// writes the (wide node, slot) it sits in (nodeUp; the root's is kEmpty),
+// and per node kids | leaf kids << 8 (nkids) and the arrival count so far,
+// its leaf kids (arrive).  An internal part that is not a wide node, or whose
+// index is out of range, cannot arise; it is written as an empty slot and
+// flagged in *bad rather than followed.
 template <class S, class NodeT>
 __global__ void k_collapse(int n, const uint4* __restrict__ child, const uint32_t* __restrict__ wide,
-                           const uint32_t* __restrict__ widx, uint32_t nw, NodeT* __restrict__ nodes,
-                           uint2* __restrict__ leafUp, uint2* __restrict__ nodeUp, uint32_t* __restrict__ nkids,
-                           unsigned* __restrict__ bad)
+                           const uint32_t* __restrict__ widx, uint32_t nw, const S* __restrict__ leafBox,
+                           NodeT* __restrict__ nodes, uint2* __restrict__ nodeUp, uint32_t* __restrict__ nkids,
+                           unsigned* __restrict__ arrive, unsigned* __restrict__ bad)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1 || !wide[i]) return;
@@ -401,31 +403,37 @@ __global__ void k_collapse(int n, const uint4* __restrict__ child, const uint32_
         ns++;
     }
     NodeT out;
-    uint32_t kids = 0;
+    uint32_t kids = 0, leaves = 0;
     for (int k = 0; k < 4; k++) {
         uint32_t r = k < ns ? slot[k] : kEmpty;
         if (r != kEmpty && !(r & kLeaf) && (!wide[r] || widx[r] >= nw)) {
             atomicOr(bad, kErrBuild);
             r = kEmpty;
         }
-        out.lox[k] = out.loy[k] = out.loz[k] = (S)INFINITY;
-        out.hix[k] = out.hiy[k] = out.hiz[k] = (S)-INFINITY;
+        S bx[6] = {(S)INFINITY, (S)INFINITY, (S)INFINITY, (S)-INFINITY, (S)-INFINITY, (S)-INFINITY};
         if (r == kEmpty) {
             out.child[k] = kEmpty;
-            continue;
-        }
-        kids++;
-        if (r & kLeaf) {
+        } else if (r & kLeaf) {
+            load_box_cg(leafBox + 6 * (size_t)(r & ~kLeaf), bx);
             out.child[k] = r;
-            leafUp[r & ~kLeaf] = make_uint2(wi, (uint32_t)k);
+            kids++;
+            leaves++;
         } else {
             const uint32_t cw = widx[r];
             out.child[k] = cw;
             nodeUp[cw] = make_uint2(wi, (uint32_t)k);
+            kids++;
         }
+        out.lox[k] = bx[0];
+        out.loy[k] = bx[1];
+        out.loz[k] = bx[2];
+        out.hix[k] = bx[3];
+        out.hiy[k] = bx[4];
+        out.hiz[k] = bx[5];
     }
     for (int k = 0; k < (int)(sizeof(out.pad) / sizeof(out.pad[0])); k++) out.pad[k] = 0;
-    nkids[wi] = kids;
+    nkids[wi] = kids | (leaves << 8);
+    arrive[wi] = leaves;
     nodes[wi] = out;
 }
 
@@ -451,24 +459,27 @@ __device__ __forceinline__ void node_union_cg(const WNode64* nd, double b[6])
     }
 }
 
-// Bottom-up refit of the wide tree, one thread per leaf: a thread stores its
-// box into its slot of the node above and arrives there; the thread that
-// arrives last (after the node's other children) takes the union of the
-// node's slots and climbs on.  The links of the node above are loaded while
-// the arrival is in flight, so a level costs the slot stores, the arrival
-// atomic and one read of the node's six box fields; the wide tree has about
-// half the levels of the binary one.
+// Bottom-up refit of the wide tree, one thread per wide node.  A node whose
+// children are all leaves is complete after k_collapse: its thread takes the
+// union of its slots, stores it into its slot of the node above and arrives
+// there; the thread that arrives last (after the node's other children) takes
+// that node's union and climbs on.  Nodes with a wide child return at once.
+// The links of the node above are loaded while the arrival is in flight, so a
+// level costs the slot stores, the arrival atomic and one read of the node's
+// six box fields; the wide tree has about half the levels of the binary one.
 template <class S, class NodeT>
-__global__ void k_refit_wide(uint32_t n, uint32_t nw, const uint2* __restrict__ leafUp,
-                             const uint2* __restrict__ nodeUp, const uint32_t* __restrict__ nkids,
-                             const S* __restrict__ leafBox, NodeT* nodes, unsigned* arrive, unsigned* bad)
+__global__ void k_refit_wide(uint32_t nw, const uint2* __restrict__ nodeUp, const uint32_t* __restrict__ nkids,
+                             NodeT* nodes, unsigned* arrive, unsigned* bad)
 {
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
+    const uint32_t w0 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w0 >= nw) return;
+    const uint32_t k0 = nkids[w0];
+    if ((k0 & 0xffu) != (k0 >> 8)) return;  // a wide child completes this node
     S b[6];
-    load_box_cg(leafBox + 6 * (size_t)p, b);
-    uint2 up = leafUp[p];
-    for (uint32_t guard = 0; guard < n; guard++) {
+    node_union_cg(nodes + w0, b);
+    uint2 up = nodeUp[w0];
+    for (uint32_t guard = 0; guard < nw; guard++) {
+        if (up.x == kEmpty) return;  // the root is complete
         const uint32_t w = up.x, k = up.y & 3u;
         if (w >= nw) {
             atomicOr(bad, kErrBuild);
@@ -482,11 +493,10 @@ __global__ void k_refit_wide(uint32_t n, uint32_t nw, const uint2* __restrict__ 
         nd->hiy[k] = b[4];
         nd->hiz[k] = b[5];
         const uint2 upn = nodeUp[w];
-        const uint32_t need = nkids[w];
+        const uint32_t need = nkids[w] & 0xffu;
         // release: this slot's stores before the arrival; acquire: the other slots' after it
         if (arrive_acq_rel(&arrive[w]) + 1u != need) return;
         node_union_cg(nd, b);
-        if (upn.x == kEmpty) return;  // the root
         up = upn;
     }
 }
@@ -599,7 +609,7 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t 
     uint4* child = nullptr;
     int* parent = nullptr;
     unsigned* arrive = nullptr;
-    uint2 *leafUp = nullptr, *nodeUp = nullptr;
+    uint2* nodeUp = nullptr;
     uint32_t* nkids = nullptr;
     uint32_t *wide = nullptr, *widx = nullptr;
     uint8_t* tab = nullptr;
@@ -642,7 +652,6 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t 
         GI_TRY(pool_alloc(&wide, sizeof(uint32_t) * (n - 1), pool, st));
         GI_TRY(pool_alloc(&tab, sizeof(uint8_t) * (n - 1), pool, st));
         GI_TRY(pool_alloc(&widx, sizeof(uint32_t) * (n - 1), pool, st));
-        GI_TRY(pool_alloc(&leafUp, sizeof(uint2) * n, pool, st));
         int gi_ = (int)((n - 1 + tb - 1) / tb);
         k_karras<<<gi_, tb, 0, st>>>(k0, (int)n, child, parent);
         k_state_tables<<<gi_, tb, 0, st>>>((int)n, child, parent, tab);
@@ -657,19 +666,17 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t 
         GI_TRY(pool_alloc(&nodeUp, sizeof(uint2) * (size_t)nw, pool, st));
         GI_TRY(pool_alloc(&nkids, sizeof(uint32_t) * (size_t)nw, pool, st));
         GI_TRY(pool_alloc(&arrive, sizeof(unsigned) * (size_t)nw, pool, st));
-        GI_TRY(cudaMemsetAsync(arrive, 0, sizeof(unsigned) * (size_t)nw, st));
+        const int gw = (int)((nw + tb - 1) / tb);
         if (!fp64) {
             GI_TRY(pool_alloc(&m.nodes, sizeof(WNode) * (size_t)nw, pool, st));
-            k_collapse<float, WNode><<<gi_, tb, 0, st>>>((int)n, child, wide, widx, nw, m.nodes, leafUp, nodeUp,
-                                                         nkids, d_err);
-            k_refit_wide<float, WNode><<<gb, tb, 0, st>>>(n, nw, leafUp, nodeUp, nkids, m.leafBox, m.nodes, arrive,
-                                                          d_err);
+            k_collapse<float, WNode><<<gi_, tb, 0, st>>>((int)n, child, wide, widx, nw, m.leafBox, m.nodes,
+                                                         nodeUp, nkids, arrive, d_err);
+            k_refit_wide<float, WNode><<<gw, tb, 0, st>>>(nw, nodeUp, nkids, m.nodes, arrive, d_err);
         } else {
             GI_TRY(pool_alloc(&m.nodes64, sizeof(WNode64) * (size_t)nw, pool, st));
-            k_collapse<double, WNode64><<<gi_, tb, 0, st>>>((int)n, child, wide, widx, nw, m.nodes64, leafUp,
-                                                            nodeUp, nkids, d_err);
-            k_refit_wide<double, WNode64><<<gb, tb, 0, st>>>(n, nw, leafUp, nodeUp, nkids, m.leafBox64, m.nodes64,
-                                                             arrive, d_err);
+            k_collapse<double, WNode64><<<gi_, tb, 0, st>>>((int)n, child, wide, widx, nw, m.leafBox64,
+                                                            m.nodes64, nodeUp, nkids, arrive, d_err);
+            k_refit_wide<double, WNode64><<<gw, tb, 0, st>>>(nw, nodeUp, nkids, m.nodes64, arrive, d_err);
         }
         m.nnodes = nw;
         m.root = 0;
@@ -702,7 +709,6 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t 
     if (child) cudaFreeAsync(child, st);
     if (parent) cudaFreeAsync(parent, st);
     if (arrive) cudaFreeAsync(arrive, st);
-    if (leafUp) cudaFreeAsync(leafUp, st);
     if (nodeUp) cudaFreeAsync(nodeUp, st);
     if (nkids) cudaFreeAsync(nkids, st);
     if (wide) cudaFreeAsync(wide, st);
