@@ -3,7 +3,7 @@
 // Build (once per mesh, replaces the reference's level-cut / forest builders,
 // include/third-party/cubql/level_cut_builder.h:278-364 and forest_builder.h:405-517,
 // which loop on the host with a device sync per tree level):
-//   k_validate -> k_tri_boxes -> k_morton -> radix sort -> k_karras -> k_leaves
+//   k_validate -> k_tri_boxes -> k_morton -> radix sort -> k_karras_leaves (leaves + binary tree)
 //   -> k_state_tables -> k_wide_flags -> scan -> k_collapse (size-greedy 4-wide nodes,
 //   topology) -> k_refit_wide (bottom-up over the wide tree, atomic arrival counters)
 // One host round trip, for the wide-node count (the node array's size).
@@ -202,12 +202,12 @@ __device__ __forceinline__ int kdelta(const uint32_t* __restrict__ keys, int n, 
     return __clz(a ^ b);
 }
 
-// Karras 2012 radix-tree construction over sorted Morton keys (ties by index).
-// child[i] = (left ref, right ref, leaves under left, leaves under right).
-__global__ void k_karras(const uint32_t* __restrict__ keys, int n, uint4* __restrict__ child, int* __restrict__ parent)
+// Karras 2012 radix-tree construction over sorted Morton keys (ties by index),
+// internal node i (i < n - 1).  child[i] = (left ref, right ref, leaves under
+// left, leaves under right); parent[] of the internal children (the root's is -1).
+__device__ __forceinline__ void karras_node(int i, const uint32_t* __restrict__ keys, int n, uint4* __restrict__ child,
+                                            int* __restrict__ parent)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n - 1) return;
     int d = (kdelta(keys, n, i, i + 1) - kdelta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
     int dmin = kdelta(keys, n, i, i - d);
     int lmax = 2;
@@ -227,22 +227,31 @@ __global__ void k_karras(const uint32_t* __restrict__ keys, int n, uint4* __rest
     uint32_t right = (max(i, j) == gamma + 1) ? (kLeaf | (uint32_t)(gamma + 1)) : (uint32_t)(gamma + 1);
     const int lo = min(i, j), hi = max(i, j);
     child[i] = make_uint4(left, right, (uint32_t)(gamma - lo + 1), (uint32_t)(hi - gamma));
-    parent[(left & kLeaf) ? (n - 1 + (int)(left & ~kLeaf)) : (int)left] = i;
-    parent[(right & kLeaf) ? (n - 1 + (int)(right & ~kLeaf)) : (int)right] = i;
+    if (!(left & kLeaf)) parent[left] = i;
+    if (!(right & kLeaf)) parent[right] = i;
     if (i == 0) parent[0] = -1;
 }
 
+// Leaves in sorted order (position p < n: the box and the vertex indices of
+// triangle vals[p]) and the radix tree's internal node p (p < n - 1), in one
+// launch: both are gathers or searches bound by latency, so each thread has
+// two independent chains in flight.
 template <class S>
-__global__ void k_leaves(const uint32_t* __restrict__ vals, uint32_t n, const uint32_t* __restrict__ T,
-                         const S* __restrict__ boxOrig, S* __restrict__ leafBox, uint4* __restrict__ leafTri)
+__global__ void k_karras_leaves(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, int n,
+                                const uint32_t* __restrict__ T, const S* __restrict__ boxOrig,
+                                S* __restrict__ leafBox, uint4* __restrict__ leafTri, uint4* __restrict__ child,
+                                int* __restrict__ parent)
 {
-    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
-    uint32_t tri = vals[p];
+    const uint32_t tri = vals[p];
     S b[6];
     load_box_cg(boxOrig + 6 * (size_t)tri, b);
+    uint4 t4 = make_uint4(0u, 0u, 0u, 0u);
+    if (leafTri) t4 = make_uint4(T[3 * (size_t)tri], T[3 * (size_t)tri + 1], T[3 * (size_t)tri + 2], tri);
+    if (p < n - 1) karras_node(p, keys, n, child, parent);
     store_box(leafBox + 6 * (size_t)p, b);
-    if (leafTri) leafTri[p] = make_uint4(T[3 * (size_t)tri], T[3 * (size_t)tri + 1], T[3 * (size_t)tri + 2], tri);
+    if (leafTri) leafTri[p] = t4;
 }
 
 template <class S>
@@ -634,26 +643,28 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t 
     k_tri_boxes<<<gboxes < 592 ? gboxes : 592, kTriBoxThreads, 0, st>>>(m.verts, m.nv, m.tris, n, box, box64, cb);
     k_morton<<<gb, tb, 0, st>>>(box, n, cb, k0, v0);
     radix_sort<uint32_t, kMortonDigit>(k0, v0, k1, v1, n, 30, counts, stemp, st);
-    // leaves in sorted order
+    if (n > 1) {
+        GI_TRY(pool_alloc(&child, sizeof(uint4) * (n - 1), pool, st));
+        GI_TRY(pool_alloc(&parent, sizeof(int) * (n - 1), pool, st));
+    }
+    // leaves in sorted order, and the binary radix tree
     if (!fp64) {
         GI_TRY(pool_alloc(&m.leafBox, sizeof(float) * 6 * n, pool, st));
         GI_TRY(pool_alloc(&m.leafTri, sizeof(uint4) * n, pool, st));
-        k_leaves<float><<<gb, tb, 0, st>>>(v0, n, m.tris, box, m.leafBox, m.leafTri);
+        k_karras_leaves<float><<<gb, tb, 0, st>>>(k0, v0, (int)n, m.tris, box, m.leafBox, m.leafTri, child, parent);
     } else {
         GI_TRY(pool_alloc(&m.leafBox64, sizeof(double) * 6 * n, pool, st));
-        k_leaves<double><<<gb, tb, 0, st>>>(v0, n, m.tris, box64, m.leafBox64, nullptr);
+        k_karras_leaves<double><<<gb, tb, 0, st>>>(k0, v0, (int)n, m.tris, box64, m.leafBox64, nullptr, child,
+                                                   parent);
     }
     if (n == 1) {
         m.root = kLeaf | 0u;
         m.nnodes = 0;
     } else {
-        GI_TRY(pool_alloc(&child, sizeof(uint4) * (n - 1), pool, st));
-        GI_TRY(pool_alloc(&parent, sizeof(int) * (2 * (size_t)n - 1), pool, st));
         GI_TRY(pool_alloc(&wide, sizeof(uint32_t) * (n - 1), pool, st));
         GI_TRY(pool_alloc(&tab, sizeof(uint8_t) * (n - 1), pool, st));
         GI_TRY(pool_alloc(&widx, sizeof(uint32_t) * (n - 1), pool, st));
         int gi_ = (int)((n - 1 + tb - 1) / tb);
-        k_karras<<<gi_, tb, 0, st>>>(k0, (int)n, child, parent);
         k_state_tables<<<gi_, tb, 0, st>>>((int)n, child, parent, tab);
         k_wide_flags<<<gi_, tb, 0, st>>>((int)n, parent, tab, wide);
         scan_exclusive(wide, widx, n - 1, stemp, st);

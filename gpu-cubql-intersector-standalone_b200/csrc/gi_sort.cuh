@@ -102,6 +102,24 @@ inline void scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, uint32
     note_launches(2);
 }
 
+// Exclusive scan left in two parts: out[] holds the scan within each tile of
+// kScanTile words and *sums (nullptr for a single tile) the scanned tile
+// totals, so that the full scan at j is out[j] + sums[j / kScanTile].  A
+// consumer that adds the tile offset itself saves the add pass.
+inline void scan_exclusive_split(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* temp, const uint32_t** sums,
+                                 cudaStream_t st)
+{
+    *sums = nullptr;
+    if (n == 0) return;
+    uint32_t tiles = (n + kScanTile - 1) / kScanTile;
+    k_scan_tiles<<<tiles, kScanThreads, 0, st>>>(in, out, n, tiles > 1 ? temp : nullptr);
+    note_launches(1);
+    if (tiles > 1) {
+        scan_exclusive(temp, temp, tiles, temp + tiles + 1, st);
+        *sums = temp;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Radix sort
 // ---------------------------------------------------------------------------
@@ -132,14 +150,17 @@ template <class K, int BITS>
 __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                            K* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t n,
                                                            int shift, const uint32_t* __restrict__ offsets,
-                                                           uint32_t ntiles)
+                                                           const uint32_t* __restrict__ tile_sums, uint32_t ntiles)
 {
     constexpr uint32_t kDig = 1u << BITS;
     __shared__ uint32_t wc[kRsWarps][kDig];
     __shared__ uint32_t tile_off[kDig];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (uint32_t d = lane; d < kDig; d += 32) wc[w][d] = 0;
-    for (uint32_t d = threadIdx.x; d < kDig; d += kRsThreads) tile_off[d] = offsets[d * ntiles + blockIdx.x];
+    for (uint32_t d = threadIdx.x; d < kDig; d += kRsThreads) {
+        const uint32_t j = d * ntiles + blockIdx.x;
+        tile_off[d] = offsets[j] + (tile_sums ? tile_sums[j / kScanTile] : 0u);
+    }
     __syncwarp();
     const uint32_t seg = blockIdx.x * kRsTile + w * 32 * kRsItems;
     K key[kRsItems];
@@ -186,10 +207,12 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K* __restrict__
 }
 
 // Sorts (keys, vals) by the low `bits` bits of the key in passes of BITS-bit
-// digits; result ends in (k0, v0).  Scratch: k1/v1 the same size, counts
+// digits.  The passes alternate between the two buffer pairs; on return
+// (k0, v0) point to the pair that holds the result and (k1, v1) to the other
+// (swapped after an odd number of passes, nothing copied).  Scratch: counts
 // radix_counts_words<BITS>(n) words, scan temp.
 template <class K, int BITS = 8>
-void radix_sort(K* k0, uint32_t* v0, K* k1, uint32_t* v1, uint32_t n, int bits, uint32_t* counts, uint32_t* temp,
+void radix_sort(K*& k0, uint32_t*& v0, K*& k1, uint32_t*& v1, uint32_t n, int bits, uint32_t* counts, uint32_t* temp,
                 cudaStream_t st)
 {
     if (n <= 1) return;
@@ -201,8 +224,9 @@ void radix_sort(K* k0, uint32_t* v0, K* k1, uint32_t* v1, uint32_t n, int bits, 
     uint32_t* vd = v1;
     for (int p = 0; p < passes; p++) {
         k_rs_hist<K, BITS><<<ntiles, kRsThreads, 0, st>>>(ks, n, BITS * p, counts, ntiles);
-        scan_exclusive(counts, counts, (1u << BITS) * ntiles, temp, st);
-        k_rs_scatter<K, BITS><<<ntiles, kRsThreads, 0, st>>>(ks, vs, kd, vd, n, BITS * p, counts, ntiles);
+        const uint32_t* sums = nullptr;
+        scan_exclusive_split(counts, counts, (1u << BITS) * ntiles, temp, &sums, st);
+        k_rs_scatter<K, BITS><<<ntiles, kRsThreads, 0, st>>>(ks, vs, kd, vd, n, BITS * p, counts, sums, ntiles);
         note_launches(2);
         K* tk = ks;
         ks = kd;
@@ -211,10 +235,10 @@ void radix_sort(K* k0, uint32_t* v0, K* k1, uint32_t* v1, uint32_t n, int bits, 
         vs = vd;
         vd = tv;
     }
-    if (ks != k0) {
-        cudaMemcpyAsync(k0, ks, sizeof(K) * n, cudaMemcpyDeviceToDevice, st);
-        cudaMemcpyAsync(v0, vs, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st);
-    }
+    k1 = kd;
+    v1 = vd;
+    k0 = ks;
+    v0 = vs;
 }
 
 template <int BITS = 8>
