@@ -2156,7 +2156,9 @@ __global__ void __launch_bounds__(kOrderSmallThreads, 1)
             }
             if (lane <= wlast && pos < n) perm[pos] = val;
         }
-        grid_barrier(&C->obar, ++bar, &C->err, &s_ok);
+        // the placing phase reads every block's perm entries; a separate
+        // placing launch is ordered after this one by the kernel boundary
+        if (phases & kOrderPlace) grid_barrier(&C->obar, ++bar, &C->err, &s_ok);
     }
     if (!(phases & kOrderPlace)) return;
     // ---- phase 3: gather pairs, place segments (one sorted position per thread) ----
@@ -2229,9 +2231,9 @@ cudaError_t launch_order_small_phases(const Bufs& b, const OrderBufs& O, bool so
     const double* a_segs = segs;
     const uint32_t* a_nseg = nseg;
     int ws = want_segments ? 1 : 0, so = sort ? 1 : 0;
-    // the ranking phases pass two grid barriers; a placing launch that follows
-    // a ranking launch of the same call counts its barrier after them
-    unsigned ph = phases, b0 = (sort && !(phases & kOrderRank)) ? 2u : 0u;
+    // a ranking launch without the placing phase passes one grid barrier; a
+    // placing launch that follows it in the same call counts its barrier after it
+    unsigned ph = phases, b0 = (sort && !(phases & kOrderRank)) ? 1u : 0u;
     void* args[] = {&bb, &oo, &a_segs, &a_nseg, &pairs_out, &job_out, &segs_out, &segpair_out, &ws, &so, &ph, &b0};
     e = cudaLaunchCooperativeKernel((const void*)k_order_small, dim3(kOrderSmallBlocks), dim3(kOrderSmallThreads),
                                     args, dyn, st);
