@@ -254,19 +254,6 @@ __global__ void k_karras_leaves(const uint32_t* __restrict__ keys, const uint32_
     if (leafTri) leafTri[p] = t4;
 }
 
-template <class S>
-__device__ __forceinline__ S ldcg_s(const S* p);
-template <>
-__device__ __forceinline__ float ldcg_s<float>(const float* p)
-{
-    return __ldcg(p);
-}
-template <>
-__device__ __forceinline__ double ldcg_s<double>(const double* p)
-{
-    return __ldcg(p);
-}
-
 __device__ __forceinline__ unsigned arrive_acq_rel(unsigned* f)
 {
     unsigned old;
@@ -284,8 +271,8 @@ __device__ __forceinline__ unsigned arrive_acq_rel(unsigned* f)
 // step of its wide ancestor's expansion.  Opening the largest part shrinks
 // the largest subtree of a wide node faster than taking grandchildren by
 // depth parity does on the unbalanced trees that Morton splits give on a
-// surface: on a 1.3 M-triangle sphere the pair tree of two such meshes has a
-// level and a fifth of its node pairs fewer.
+// surface: on a 1.3 M-triangle sphere the pair tree of two such meshes has
+// one level and a fifth of its node pairs fewer.
 //
 // A node's state follows from its parent's through a 3-entry table that
 // depends only on the leaf counts around it (k_state_tables).  k_wide_flags
