@@ -1231,6 +1231,15 @@ __device__ __forceinline__ unsigned ld_vol(const unsigned* p)
 
 // Release / acquire fence at GPU scope: orders entry stores before the tag
 // stores that follow, and an observed tag before the entry loads that follow.
+// acquire load: the loads after it see what the writer published before its
+// release (fence + tag store), without waiting for this thread's own stores
+__device__ __forceinline__ unsigned ld_acq(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ void fence_acq_rel()
 {
     asm volatile("fence.acq_rel.gpu;" ::: "memory");
@@ -1405,8 +1414,8 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
         // round trip overlaps the node loads of a warp that works from its stack.
         unsigned ab = 0;
         if (lane == 0 && (iter & 7u) == 0u) ab = ld_vol(&C->abort_);
-        const unsigned ntag = nslot ? ld_vol(B.qflag + ns) : 0u;
-        const unsigned ctag = cslot ? ld_vol(B.cflag + i) : 0u;
+        const unsigned ntag = nslot ? ld_acq(B.qflag + ns) : 0u;
+        const unsigned ctag = cslot ? ld_acq(B.cflag + i) : 0u;
         const bool from_queue = nslot && ntag == B.tag;  // the same in every lane of a unit
         const unsigned qball = __ballot_sync(0xffffffffu, from_queue && sub == 0u);  // a unit's first lane: ready
         if (sn != 0u || qball != 0u) {
@@ -1421,8 +1430,7 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
             if (from_stack) {
                 ent = S[sn - 1u - rank];
             } else if (from_queue) {
-                fence_acq_rel();
-                ent = __ldcg(B.queue + ns);
+                ent = __ldcg(B.queue + ns);  // ordered after the tag's acquire load
             }
             sn -= take;
             __syncwarp();  // popped entries are read before the pushes below reuse their slots
@@ -1536,8 +1544,7 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
             backoff = 32;
             uint4 c = make_uint4(0u, 0u, 0u, 0u);
             if (cready) {
-                fence_acq_rel();
-                c = __ldcg(B.cand + i);
+                c = __ldcg(B.cand + i);  // ordered after the tag's acquire load
             }
             filter_candidates<F64>(B, cready, c, decided, tested);
             cpend &= ~cavail;
