@@ -742,7 +742,7 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
                 return (uint32_t)std::min<uint64_t>(v, 0x7fffffffu);
             };
             if (H.overflow & kOvfFrontier) need_front = g4(c->cap_front, H.q_tail);
-            if (H.overflow & kOvfCand) need_cand = g4(c->cap_cand, H.cand);
+            if (H.overflow & kOvfCand) need_cand = g4(c->cap_cand, (uint32_t)(H.work_cand >> 32));
             if (H.overflow & (kOvfRes | kOvfCand)) need_res = g4(c->cap_res, H.res);
             if (H.overflow & (kOvfEsc | kOvfCand)) need_esc = g4(c->cap_esc, H.esc);
             continue;

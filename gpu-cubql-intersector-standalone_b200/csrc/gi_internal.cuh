@@ -85,10 +85,14 @@ struct Counters {
     unsigned int pad0[31];
     unsigned int q_head;  // queue slots handed out as tickets
     unsigned int pad1[31];
-    unsigned int work;    // node pairs that exist (made, not yet expanded), modulo 2^32
-    unsigned int pad2[31];
-    unsigned int cand;    // candidate slots reserved
-    unsigned int pad3[31];
+    // low half: node pairs that exist (made, not yet expanded; never below
+    // zero); high half: candidate slots reserved.  One word, so that an
+    // expansion reserves its candidate slots and updates the node-pair count
+    // in one atomic, and a warp that reads the node-pair count at zero reads
+    // the final candidate count in the same load.
+    unsigned long long work_cand;
+    unsigned int pad2[30];
+    unsigned int pad3[32];
     unsigned int c_head;  // candidate slots handed out as tickets
     unsigned int pad4[31];
     unsigned int res;     // intersecting pairs

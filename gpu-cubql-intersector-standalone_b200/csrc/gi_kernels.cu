@@ -1315,7 +1315,12 @@ __device__ __forceinline__ void seed_cut_pairs(const Bufs& B, unsigned total)
                 atomicExch(&C->abort_, 1u);
             }
         }
-        unsigned pc = warp_append(cand, &C->cand);
+        // candidate slots and node pairs counted in one atomic, before any seed is published
+        const unsigned cm = __ballot_sync(0xffffffffu, cand);
+        unsigned long long old = 0;
+        if (lane == 0 && (cm || nfront))
+            old = atomicAdd(&C->work_cand, ((unsigned long long)__popc(cm) << 32) + nfront);
+        const unsigned pc = (unsigned)(__shfl_sync(0xffffffffu, old, 0) >> 32) + __popc(cm & ((1u << lane) - 1u));
         if (cand) {
             if (pc < B.cap_cand) B.cand[pc] = make_uint4(job, ra & ~kLeaf, rb & ~kLeaf, 0u);
             else {
@@ -1323,7 +1328,6 @@ __device__ __forceinline__ void seed_cut_pairs(const Bufs& B, unsigned total)
                 atomicExch(&C->abort_, 1u);
             }
         }
-        if (lane == 0 && nfront) atomicAdd(&C->work, nfront);  // counted before any seed is published
         __syncwarp();
         fence_acq_rel();
         if (front && pf < B.cap_queue) *(volatile unsigned*)(B.qflag + pf) = B.tag;
@@ -1465,14 +1469,16 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
             const unsigned keep = min(kf, kStack - sn);
             unsigned qb = 0, cg = 0;
             if (lane == 31) {
-                if (kc) cg = atomicAdd(&C->cand, kc);
                 if (kf > keep) qb = atomicAdd(&C->q_tail, kf - keep);
-                // then node pairs made minus expanded, before any child is
-                // published: work reaches zero only after the candidate slots
-                // of the last expansion are reserved, so a warp that sees
-                // work == 0 reads the final candidate count
-                fence_acq_rel();
-                if (kf != done) atomicAdd(&C->work, kf - done);
+                // candidate slots and node pairs made minus expanded in one
+                // atomic, before any child is published: the node-pair count
+                // reaches zero in the same update that reserves the last
+                // expansion's candidate slots
+                if (kc || kf != done) {
+                    const unsigned long long old = atomicAdd(
+                        &C->work_cand, ((unsigned long long)kc << 32) + (unsigned long long)(long long)(int)(kf - done));
+                    cg = (unsigned)(old >> 32);
+                }
             }
             qb = __shfl_sync(0xffffffffu, qb, 31);
             cg = __shfl_sync(0xffffffffu, cg, 31);
@@ -1563,10 +1569,9 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
             if (lane == 0) {
                 const unsigned sd = ld_vol(&C->seed_done);
                 fence_acq_rel();
-                const unsigned w = ld_vol(&C->work);
-                fence_acq_rel();
-                over = sd == seed_total && w == 0u;
-                ncand = min(ld_vol(&C->cand), B.cap_cand);
+                const unsigned long long wc = *(const volatile unsigned long long*)&C->work_cand;
+                over = sd == seed_total && (unsigned)wc == 0u;
+                ncand = min((unsigned)(wc >> 32), B.cap_cand);
             }
             over = __shfl_sync(0xffffffffu, over, 0);
             ncand = __shfl_sync(0xffffffffu, ncand, 0);
