@@ -1205,18 +1205,20 @@ __device__ __forceinline__ void expand_quad(const Bufs& B, const uint4& ent, boo
 // atomic per warp, write the entries and, after a release fence, store the
 // call's tag in each slot's flag word.  A warp takes a ticket of 32
 // consecutive slots (one atomicAdd on the head counter), polls their 32 tag
-// words (one 128-byte line, so polling has no hot spot) and keeps the ticket
+// words with acquire loads (one 128-byte line, so polling has no hot spot;
+// a ready tag orders the entry's load after it) and keeps the ticket
 // until all 32 slots are processed.  Only warps with empty stacks take node
 // tickets, and ready queue slots come before stack entries, so queued work
 // never waits behind a warp that is busy with its own.
 //
-// Termination: `work` is the number of node pairs that exist.  Seeds add to it
+// Termination: the low half of `work_cand` is the number of node pairs that
+// exist, its high half the candidate slots reserved.  Seeds add to both
 // before the seed count completes; an expansion adds (children - expanded
-// pairs) in one atomic, issued after its candidate slots are reserved and
-// before any child is published, so the count never passes through zero
-// while a node pair exists, and once it is zero the candidate count is final.
-// Reading seed_done == all seed tests and then work == 0 proves the traversal
-// is over.  Every wait is bounded; overflow or a spent wait raises the abort
+// pairs) and its candidates in one atomic, before any child is published, so
+// the node-pair count never passes through zero while a node pair exists, and
+// the load that reads it at zero reads the final candidate count.  Reading
+// seed_done == all seed tests and then a zero node-pair count proves the
+// traversal is over.  Every wait is bounded; overflow or a spent wait raises the abort
 // flag.
 // ---------------------------------------------------------------------------
 constexpr unsigned kIdleSpins = 1u << 22;     // consecutive idle polls of one warp (~1 s)
