@@ -1,9 +1,9 @@
-"""The size-greedy 4-wide collapse of the build (csrc/gi_kernels.cu: k_karras,
-k_state_tables, k_wide_flags, k_collapse), restated on the CPU: the per-node
-state tables composed up the parent chain pick exactly the wide nodes of a
-top-down greedy expansion (open the part with the most leaves, ties to the
-leftmost, twice after the node itself), on radix trees of random and of
-clustered sorted keys.  The kernels' own output is covered by the GPU parity
+"""The size-greedy 4-wide collapse of the build (csrc/gi_kernels.cu:
+karras_node in k_karras_leaves, k_state_tables, k_wide_flags, k_collapse),
+restated on the CPU: the per-node state tables composed up the parent chain
+pick exactly the wide nodes of a top-down greedy expansion (open the part with
+the most leaves, ties to the leftmost, twice after the node itself), on radix
+trees of uniform, clustered and duplicate sorted keys.  The kernels' own output is covered by the GPU parity
 tests; this pins the equivalence the kernels rely on."""
 import random
 
