@@ -62,8 +62,10 @@ def parse():
     ap.add_argument("--pairs", type=int, default=0, help="batch: 4096 pairs; serving: 64 pairs (default)")
     ap.add_argument("--rate", type=float, default=2000.0, help="serving: mean requests per second")
     ap.add_argument("--duration", type=float, default=3.0, help="serving: seconds of offered load")
+    ap.add_argument("--pose-samples", type=int, default=1000,
+                    help="pose-update latency: wall-clock samples of gi_intersect after the timed steps")
     ap.add_argument("--shape", type=int, default=-1,
-                    help="pin the traversal shape (0..3) instead of autotuning it (for profiling runs)")
+                    help="pin the traversal shape (0..7) instead of autotuning it (for profiling runs)")
     return ap.parse_args()
 
 
@@ -73,6 +75,13 @@ def workload(level):
     cfg = mg.config2(level=level)
     rng = np.random.default_rng(22)
     return cfg, rng
+
+
+def pose_config(level, cfg):
+    """The workload's identity, the same in both arms (ours and --impl reference)."""
+    return {"workload": "icosphere L%d displaced x2 (%d tris each), pose-update stream" % (level, int(cfg["tA"].shape[0])),
+            "tris_per_mesh": int(cfg["tA"].shape[0]), "pose_stream": "seeded 22, <= 5 deg and <= 0.05 r per step",
+            "segments": True}
 
 
 def step_poses(cfg, rng, n):
@@ -194,8 +203,7 @@ def run_reference(args):
         "metric": METRIC, "impl": "reference", "value": v, "unit": "ms", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded displaced icospheres)",
-        "config": {"workload": "icosphere L8 displaced x2 (1,310,720 tris each), pose-update stream",
-                   "tris_per_mesh": int(cfg["tA"].shape[0]), "parallelism": "cpu threads"},
+        "config": pose_config(args.level, cfg), "parallelism": "cpu threads",
         "cpu_baseline": {"value": v, "unit": "ms", "cores": ncores, "kind": "port",
                          "sample": "full intersect (BVH over B + exact predicates + segments) per step, "
                                    "%d steps; CPU %s" % (args.steps, cpu_model())},
@@ -232,7 +240,7 @@ def run_batch(args, gi, world, rank, dist):
         R, C, T = j["poseB"]
         jobs.append((A, None, B, gi.pose_raw(R, C, T)))
     upload_s = time.perf_counter() - t_up
-    for k in range(8 + args.warmup):  # autotuning, then warm-up (untimed)
+    for k in range(2 * gi._abi.GI_TRAVERSE_SHAPES + args.warmup):  # autotuning, then warm-up (untimed)
         rs = ctx.intersect_batch(jobs, want_segments=True)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     dev, wall, st = [], [], None
@@ -525,7 +533,9 @@ def main():
             dist.destroy_process_group()
         return
     cfg, rng = workload(args.level)
-    poses = step_poses(cfg, rng, args.warmup + args.steps)
+    # the pose-update samples take the poses after the timed steps' (the stream
+    # is drawn pose by pose, so the first warmup + steps poses do not depend on it)
+    poses = step_poses(cfg, rng, args.warmup + args.steps + args.pose_samples)
     flags = 0 if args.shape < 0 else (gi._abi.GI_FLAG_FIXED_SHAPE | gi._abi.GI_FLAG_SHAPE(args.shape))
     ctx = gi.Context(local, flags=flags)
     A = ctx.upload(cfg["vA"], cfg["tA"])
@@ -539,7 +549,7 @@ def main():
     # autotuning: the library times each traversal shape (expansion form x
     # blocks per SM) twice per workload class on its own calls, then keeps the
     # fastest; these calls precede the warm-up and are not timed
-    for k in range(8 if args.shape < 0 else 0):
+    for k in range(2 * gi._abi.GI_TRAVERSE_SHAPES if args.shape < 0 else 0):
         one(poses[0])
         one(poses[0], precision=1)
     for k in range(args.warmup):
@@ -580,6 +590,47 @@ def main():
         fp64_ms.append(r64.stats["ms_total"])
         assert np.array_equal(r64.pairs, r.pairs) or k != args.steps - 1
 
+    # pose-update latency (the serving loop's steady state): resident meshes, a
+    # new pose in, the pairs and segments usable on the host; no L2 flush.
+    # Collections of Python's garbage collector are logged with their times, so
+    # that a slow sample can be put down to the host or to the device.
+    import gc
+
+    gc_log = []
+
+    def _gc_cb(phase, info):
+        gc_log.append((phase, info.get("generation", -1), time.perf_counter()))
+
+    pu_wall, pu_dev, pu_span = [], [], []
+    gc.callbacks.append(_gc_cb)
+    try:
+        base = args.warmup + args.steps
+        for k in range(args.pose_samples):
+            t0 = time.perf_counter()
+            rr = one(poses[base + k])
+            rr.pairs
+            t1 = time.perf_counter()
+            pu_wall.append((t1 - t0) * 1e3)
+            pu_dev.append(rr.stats["ms_total"])
+            pu_span.append((t0, t1))
+        del rr
+    finally:
+        gc.callbacks.remove(_gc_cb)
+    pose_update = {"what": "gi_intersect wall clock, resident meshes, a new pose per call, results on the host",
+                   "samples": len(pu_wall)}
+    if pu_wall:
+        w = np.array(pu_wall)
+        slow = np.nonzero(w > 1.0)[0]
+        gc_starts = [t for ph, g, t in gc_log if ph == "start"]
+        slow_gc = sum(1 for i in slow if any(pu_span[i][0] <= t <= pu_span[i][1] for t in gc_starts))
+        pose_update.update({
+            "p50_ms": float(np.percentile(w, 50)), "p99_ms": float(np.percentile(w, 99)),
+            "p999_ms": float(np.percentile(w, 99.9)), "max_ms": float(w.max()),
+            "device_p50_ms": float(np.percentile(pu_dev, 50)), "device_max_ms": float(np.max(pu_dev)),
+            "over_1ms": int(slow.size), "over_1ms_with_gc": int(slow_gc),
+            "over_1ms_device_over_1ms": int(sum(1 for i in slow if pu_dev[i] > 1.0)),
+            "gc_collections": len(gc_starts)})
+
     # e2e: one-shot from host arrays in pinned memory (the inputs' H2D, both
     # builds, the intersect and the D2H of its results are inside the timing)
     def pinned(a, dt):
@@ -617,6 +668,7 @@ def main():
     t2 = time.perf_counter()
     er = ctx.intersect(eA, eB, None, gi.pose_raw(R, C, T), want_segments=True)
     t3 = time.perf_counter()
+    e2e_build_ms = [eA.info()["build_ms"], eB.info()["build_ms"]]
     eA.release()
     eB.release()
     t4 = time.perf_counter()
@@ -629,6 +681,13 @@ def main():
     d2h = int(last_e2e.pairs.nbytes + last_e2e.segments.nbytes + last_e2e.seg_pair.nbytes)
 
     st = stats[-1]
+    # BVH build roofline: the algorithmic bytes of one build of a T-triangle,
+    # V-vertex mesh (read the mesh 24V + 12T, a 32-bit key sort 64T, write 2T-1
+    # nodes of 32 B and T ids, read the nodes once to refit) over the device time
+    # of the build kernels (gi_mesh_build_ms), averaged over the builds above
+    T, V = int(cfg["tA"].shape[0]), int(cfg["vA"].shape[0])
+    build_bytes = 24 * V + 12 * T + 64 * T + 32 * (2 * T - 1) + 4 * T + 32 * (2 * T - 1)
+    build_ms = [m.info()["build_ms"] for m in (A, B)] + e2e_build_ms
     # curve assembly (downstream of the path) on the last step's result
     t0 = time.perf_counter()
     cv_verts, cv = r.curves()
@@ -653,21 +712,20 @@ def main():
         "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": value, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded displaced icospheres, seeded pose stream)",
-        "config": {"workload": "icosphere L%d displaced x2 (%d tris each), pose-update stream" % (
-            args.level, int(cfg["tA"].shape[0])), "tris_per_mesh": int(cfg["tA"].shape[0]),
-            "parallelism": "replicas" if world > 1 else "single", "l2": "flushed (256 MB write) before each step",
-            "precision": "fp32 filter -> fp64 filter -> exact", "segments": True,
-            "traverse_shape": int(st["traverse_shape"]), "autotuned": args.shape < 0},
+        "config": pose_config(args.level, cfg),
+        "parallelism": "replicas" if world > 1 else "single",
+        "impl_config": {"l2": "flushed (256 MB write) before each step", "precision": "fp32 filter -> fp64 filter -> exact",
+                        "traverse_shape": int(st["traverse_shape"]), "autotuned": args.shape < 0},
         "pairs": int(st["pairs"]), "segments": int(st["segments"]), "candidates": int(cand),
         "tri_pair_tests_per_s": tests_per_s,
         "filter_decided_frac": float(st["filter_decided"] / max(1, st["candidates"])),
         "escalated": int(st["escalated"]), "exact_signs": int(st["exact_signs"]),
         "levels": int(st["levels"]), "node_pairs": int(st["node_pairs"]),
+        "level_end_ms": [round(x, 4) for x in st.get("level_end_ms", [])],
         "stage_ms": {"traverse_filter": trav, "exact": float(np.mean([s["ms_exact"] for s in stats])),
                      "segments": float(np.mean([s["ms_segments"] for s in stats])),
                      "ordering": float(np.mean([s["ms_sort"] for s in stats]))},
-        "pose_update": {"p50_ms": float(np.percentile(wall_ms, 50)), "p99_ms": float(np.percentile(wall_ms, 99)),
-                        "what": "gi_intersect wall clock, resident meshes, results on host"},
+        "pose_update": pose_update,
         "curve_assembly": {"ms": curves_ms, "curves": len(cv), "closed": int(sum(1 for _, c in cv if c)),
                            "vertices": int(cv_verts.shape[0]), "what": "gi_curves_build on the host, last step"},
         "fp64_form": {"value": float(np.mean(fp64_ms)), "unit": "ms",
@@ -685,6 +743,12 @@ def main():
                      "alg_bytes_per_launch": float(alg_bytes),
                      "note": "output-sensitive traversal: bytes = node pairs x 2 nodes x 128 B + leaf pairs x "
                              "2 x (16 B record + 3 x 24 B vertices) + results x 16 B"},
+        "build_roofline": {"bound": "hbm", "achieved": build_bytes / (np.mean(build_ms) * 1e-3) / 1e9, "peak": peak,
+                           "unit": "GB/s", "frac": build_bytes / (np.mean(build_ms) * 1e-3) / 1e9 / peak,
+                           "build_ms": float(np.mean(build_ms)), "builds": len(build_ms),
+                           "alg_bytes_per_mesh": build_bytes, "peak_source": peak_src,
+                           "note": "24V + 12T (mesh) + 64T (32-bit key sort) + 32(2T-1) + 4T (nodes, ids) + "
+                                   "32(2T-1) (refit read) over the device time of validation + build kernels"},
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

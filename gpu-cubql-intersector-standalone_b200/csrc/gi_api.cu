@@ -84,7 +84,7 @@ extern "C" gi_status gi_create(const gi_options* opts, gi_ctx** out)
     c->device = opts ? opts->device : 0;
     c->budget = opts ? opts->hbm_budget_bytes : 0;
     c->flags = opts ? opts->flags : 0;
-    if (c->flags & GI_FLAG_FIXED_SHAPE) c->fixed_shape = (int)((c->flags >> 9) & 3u);
+    if (c->flags & GI_FLAG_FIXED_SHAPE) c->fixed_shape = (int)((c->flags >> 9) & 7u);
     if (c->device < 0 || c->device >= ndev) {
         delete c;
         return GI_ERR_INVALID_ARG;
@@ -186,8 +186,14 @@ static gi_status mesh_finish(gi_ctx* c, gi_mesh* m, gi_mesh** out, cudaStream_t 
     unsigned* d_err = nullptr;
     CKS(sk, pool_alloc(&d_err, sizeof(unsigned), c->pool, st), "alloc");
     CKS(sk, cudaMemsetAsync(d_err, 0, sizeof(unsigned), st), "memset");
-    CKS(sk, launch_validate(m->b.verts, m->b.nv, m->b.tris, m->b.nt, d_err, st), "validate");
-    cudaError_t e = build_bvh(m->b, false, d_err, c->pool, st);
+    // device time of validation + build (the reference's buildRefitMesh*Ms);
+    // events of this call only, as two meshes may build at once on two streams
+    cudaEvent_t eb[2] = {nullptr, nullptr};
+    bool timed = cudaEventCreate(&eb[0]) == cudaSuccess && cudaEventCreate(&eb[1]) == cudaSuccess &&
+                 cudaEventRecord(eb[0], st) == cudaSuccess;
+    cudaError_t e = launch_validate(m->b.verts, m->b.nv, m->b.tris, m->b.nt, d_err, st);
+    if (e == cudaSuccess) e = build_bvh(m->b, false, d_err, c->pool, st);
+    timed = timed && cudaEventRecord(eb[1], st) == cudaSuccess;
     unsigned herr = 0;
     // a pageable destination: the copy returns when the stream has reached it (the build is done)
     cudaError_t es = cudaMemcpyAsync(&herr, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
@@ -195,6 +201,11 @@ static gi_status mesh_finish(gi_ctx* c, gi_mesh* m, gi_mesh** out, cudaStream_t 
     const cudaError_t es2 = cudaStreamSynchronize(st);
     if (es == cudaSuccess) es = es2;
     if (e == cudaSuccess) e = es;
+    float bms = 0.0f;
+    if (timed && e == cudaSuccess && cudaEventElapsedTime(&bms, eb[0], eb[1]) == cudaSuccess) m->build_ms = bms;
+    for (cudaEvent_t ev : eb)
+        if (ev) cudaEventDestroy(ev);
+    cudaGetLastError();  // a failed event call above is not the build's error
     cudaFreeAsync(d_err, st);
     if (e != cudaSuccess) {
         mesh_free(c, m, st);
@@ -306,6 +317,19 @@ extern "C" gi_status gi_mesh_upload(gi_ctx* c, const double* verts, uint32_t nv,
     return mesh_upload_on(c, verts, nv, tris, nt, out, c->st, UploadSink{c, nullptr});
 }
 
+extern "C" gi_status gi_wait_stream(gi_ctx* c, void* stream)
+{
+    if (!c) return GI_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(c, cudaSetDevice(c->device), "set device");
+    // ev[7] is kept for this hand-off: recorded on the caller's stream, waited
+    // on by the context's two streams (the wait binds the work recorded now)
+    CK(c, cudaEventRecord(c->ev[7], static_cast<cudaStream_t>(stream)), "record on the caller's stream");
+    CK(c, cudaStreamWaitEvent(c->st, c->ev[7], 0), "stream wait");
+    CK(c, cudaStreamWaitEvent(c->st2, c->ev[7], 0), "stream wait");
+    return GI_OK;
+}
+
 extern "C" gi_status gi_mesh_upload_device(gi_ctx* c, const double* d_verts, uint32_t nv, const uint32_t* d_tris,
                                            uint32_t nt, gi_mesh** out)
 {
@@ -341,6 +365,13 @@ extern "C" gi_status gi_mesh_release(gi_ctx* c, gi_mesh* m)
     if (!c || !m || m->ctx != c) return GI_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
     mesh_free(c, m, c->st);
+    return GI_OK;
+}
+
+extern "C" gi_status gi_mesh_build_ms(const gi_mesh* m, double* ms)
+{
+    if (!m || !ms) return GI_ERR_INVALID_ARG;
+    *ms = m->build_ms;
     return GI_OK;
 }
 
@@ -854,6 +885,14 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         s2.ms_segments = ms_seg;
         s2.ms_sort = ms_sort;
         s2.ms_total = ms_total;
+        static_assert(sizeof(s2.level_end_ms) / sizeof(double) == (size_t)kLevelTimes, "level time slots");
+        if (trav_shape(shape).levels && H.t_start) {
+            const uint32_t nl = std::min<uint32_t>(H.levels + 1u, (uint32_t)kLevelTimes);
+            for (uint32_t l = 0; l < nl && H.level_ns[l] >= H.t_start; l++) {
+                s2.level_end_ms[l] = 1e-6 * double(H.level_ns[l] - H.t_start);
+                s2.level_times = l + 1;
+            }
+        }
     }
     buf = nullptr;  // now held by the results
     return GI_OK;

@@ -217,45 +217,62 @@ static __device__ int classify_fast(const double3* P, const double3* Q)
 // Exact signs: FP64 filter (Shewchuk's orient3d/orient2d bound A, same
 // operation order as the oracle), then integer arithmetic on a common grid.
 // ---------------------------------------------------------------------------
+// FP64 filter of one orient3d sign (Shewchuk's bound A): +1 / -1, or kUnsure.
+__device__ __forceinline__ int o3_filter64(const double3& a, const double3& b, const double3& c, const double3& d)
+{
+    double adx = __dsub_rn(a.x, d.x), ady = __dsub_rn(a.y, d.y), adz = __dsub_rn(a.z, d.z);
+    double bdx = __dsub_rn(b.x, d.x), bdy = __dsub_rn(b.y, d.y), bdz = __dsub_rn(b.z, d.z);
+    double cdx = __dsub_rn(c.x, d.x), cdy = __dsub_rn(c.y, d.y), cdz = __dsub_rn(c.z, d.z);
+    double bdxcdy = __dmul_rn(bdx, cdy), cdxbdy = __dmul_rn(cdx, bdy);
+    double cdxady = __dmul_rn(cdx, ady), adxcdy = __dmul_rn(adx, cdy);
+    double adxbdy = __dmul_rn(adx, bdy), bdxady = __dmul_rn(bdx, ady);
+    double det = __dadd_rn(__dadd_rn(__dmul_rn(adz, __dsub_rn(bdxcdy, cdxbdy)),
+                                     __dmul_rn(bdz, __dsub_rn(cdxady, adxcdy))),
+                           __dmul_rn(cdz, __dsub_rn(adxbdy, bdxady)));
+    double perm = __dadd_rn(
+        __dadd_rn(__dmul_rn(__dadd_rn(fabs(bdxcdy), fabs(cdxbdy)), fabs(adz)),
+                  __dmul_rn(__dadd_rn(fabs(cdxady), fabs(adxcdy)), fabs(bdz))),
+        __dmul_rn(__dadd_rn(fabs(adxbdy), fabs(bdxady)), fabs(cdz)));
+    double eb = __dmul_rn((7.0 + 56.0 * 0x1p-53) * 0x1p-53, perm);
+    if (det > eb) return 1;
+    if (-det > eb) return -1;
+    return kUnsure;
+}
+
+// FP64 filter of one orient2d sign in the plane that drops axis `drop`
+// (Shewchuk's bound A): +1 / -1, or kUnsure.
+__device__ __forceinline__ int o2_filter64(const double3& a, const double3& b, const double3& c, int drop)
+{
+    const double* A = &a.x;
+    const double* B = &b.x;
+    const double* C = &c.x;
+    int u = (drop + 1) % 3, v = (drop + 2) % 3;
+    double l = __dmul_rn(__dsub_rn(A[u], C[u]), __dsub_rn(B[v], C[v]));
+    double r = __dmul_rn(__dsub_rn(A[v], C[v]), __dsub_rn(B[u], C[u]));
+    double det = __dsub_rn(l, r);
+    double eb = __dmul_rn((3.0 + 16.0 * 0x1p-53) * 0x1p-53, __dadd_rn(fabs(l), fabs(r)));
+    if (det > eb) return 1;
+    if (-det > eb) return -1;
+    return kUnsure;
+}
+
 struct ExactSigns {
     unsigned* err;
     unsigned long long nexact;
 
     __device__ __noinline__ int o3(const double3& a, const double3& b, const double3& c, const double3& d)
     {
-        double adx = __dsub_rn(a.x, d.x), ady = __dsub_rn(a.y, d.y), adz = __dsub_rn(a.z, d.z);
-        double bdx = __dsub_rn(b.x, d.x), bdy = __dsub_rn(b.y, d.y), bdz = __dsub_rn(b.z, d.z);
-        double cdx = __dsub_rn(c.x, d.x), cdy = __dsub_rn(c.y, d.y), cdz = __dsub_rn(c.z, d.z);
-        double bdxcdy = __dmul_rn(bdx, cdy), cdxbdy = __dmul_rn(cdx, bdy);
-        double cdxady = __dmul_rn(cdx, ady), adxcdy = __dmul_rn(adx, cdy);
-        double adxbdy = __dmul_rn(adx, bdy), bdxady = __dmul_rn(bdx, ady);
-        double det = __dadd_rn(__dadd_rn(__dmul_rn(adz, __dsub_rn(bdxcdy, cdxbdy)),
-                                         __dmul_rn(bdz, __dsub_rn(cdxady, adxcdy))),
-                               __dmul_rn(cdz, __dsub_rn(adxbdy, bdxady)));
-        double perm = __dadd_rn(
-            __dadd_rn(__dmul_rn(__dadd_rn(fabs(bdxcdy), fabs(cdxbdy)), fabs(adz)),
-                      __dmul_rn(__dadd_rn(fabs(cdxady), fabs(adxcdy)), fabs(bdz))),
-            __dmul_rn(__dadd_rn(fabs(adxbdy), fabs(bdxady)), fabs(cdz)));
-        double eb = __dmul_rn((7.0 + 56.0 * 0x1p-53) * 0x1p-53, perm);
-        if (det > eb) return 1;
-        if (-det > eb) return -1;
+        const int f = o3_filter64(a, b, c, d);
+        if (f != kUnsure) return f;
         nexact++;
         return ex::o3_exact_sign(&a.x, &b.x, &c.x, &d.x, err);
     }
     __device__ __noinline__ int o2(const double3& a, const double3& b, const double3& c, int drop)
     {
-        const double* A = &a.x;
-        const double* B = &b.x;
-        const double* C = &c.x;
-        int u = (drop + 1) % 3, v = (drop + 2) % 3;
-        double l = __dmul_rn(__dsub_rn(A[u], C[u]), __dsub_rn(B[v], C[v]));
-        double r = __dmul_rn(__dsub_rn(A[v], C[v]), __dsub_rn(B[u], C[u]));
-        double det = __dsub_rn(l, r);
-        double eb = __dmul_rn((3.0 + 16.0 * 0x1p-53) * 0x1p-53, __dadd_rn(fabs(l), fabs(r)));
-        if (det > eb) return 1;
-        if (-det > eb) return -1;
+        const int f = o2_filter64(a, b, c, drop);
+        if (f != kUnsure) return f;
         nexact++;
-        return ex::o2_exact_sign(A, B, C, drop, err);
+        return ex::o2_exact_sign(&a.x, &b.x, &c.x, drop, err);
     }
 };
 

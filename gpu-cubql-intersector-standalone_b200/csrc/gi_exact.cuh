@@ -266,8 +266,13 @@ __device__ __forceinline__ long long scaled_i64(const DBits& d, int E)
     return d.neg ? -v : v;
 }
 
+// Integer branch that decided an exact sign (reported through `path`).
+constexpr int kPathInt128 = 0, kPathMultiLimb = 1, kPathCapacity = 2;
+
 // det[a-d; b-d; c-d] exact sign. err |= kErrExactCapacity if outside capacity.
-static __device__ __noinline__ int o3_exact_sign(const double* a, const double* b, const double* c, const double* d, unsigned* err)
+// path (optional): the branch that ran, kPathInt128 or kPathMultiLimb (kPathCapacity on failure).
+static __device__ __noinline__ int o3_exact_sign(const double* a, const double* b, const double* c, const double* d,
+                                                 unsigned* err, int* path = nullptr)
 {
     DBits bits[12];
     const double* P[4] = {a, b, c, d};
@@ -279,6 +284,7 @@ static __device__ __noinline__ int o3_exact_sign(const double* a, const double* 
         }
     grid_finish(g);
     if (g.span <= 40) {
+        if (path) *path = kPathInt128;
         long long v[12];
         for (int i = 0; i < 12; i++) v[i] = scaled_i64(bits[i], g.E);
         __int128 adx = v[0] - v[9], ady = v[1] - v[10], adz = v[2] - v[11];
@@ -287,9 +293,11 @@ static __device__ __noinline__ int o3_exact_sign(const double* a, const double* 
         __int128 det = adz * (bdx * cdy - cdx * bdy) + bdz * (cdx * ady - adx * cdy) + cdz * (adx * bdy - bdx * ady);
         return (det > 0) - (det < 0);
     }
+    if (path) *path = kPathMultiLimb;
     Big V[12];
     for (int i = 0; i < 12; i++)
         if (!big_from_bits(bits[i], g.E, V[i])) {
+            if (path) *path = kPathCapacity;
             atomicOr(err, 2u);
             return 0;
         }
@@ -313,13 +321,15 @@ static __device__ __noinline__ int o3_exact_sign(const double* a, const double* 
         ok &= big_addsub(acc, t2, +1, acc);
     }
     if (!ok) {
+        if (path) *path = kPathCapacity;
         atomicOr(err, 2u);
         return 0;
     }
     return big_sign(acc);
 }
 
-static __device__ __noinline__ int o2_exact_sign(const double* a, const double* b, const double* c, int drop, unsigned* err)
+static __device__ __noinline__ int o2_exact_sign(const double* a, const double* b, const double* c, int drop,
+                                                 unsigned* err, int* path = nullptr)
 {
     int u = (drop + 1) % 3, v = (drop + 2) % 3;
     double q[6] = {a[u], a[v], b[u], b[v], c[u], c[v]};
@@ -331,6 +341,7 @@ static __device__ __noinline__ int o2_exact_sign(const double* a, const double* 
     }
     grid_finish(g);
     if (g.span <= 60) {
+        if (path) *path = kPathInt128;
         __int128 s[6];
         for (int i = 0; i < 6; i++) {
             if (bits[i].mant == 0) {
@@ -344,9 +355,11 @@ static __device__ __noinline__ int o2_exact_sign(const double* a, const double* 
         __int128 det = acu * bcv - acv * bcu;
         return (det > 0) - (det < 0);
     }
+    if (path) *path = kPathMultiLimb;
     Big V[6];
     for (int i = 0; i < 6; i++)
         if (!big_from_bits(bits[i], g.E, V[i])) {
+            if (path) *path = kPathCapacity;
             atomicOr(err, 2u);
             return 0;
         }
@@ -360,6 +373,7 @@ static __device__ __noinline__ int o2_exact_sign(const double* a, const double* 
     ok &= big_mul(V[1], V[2], t2);
     ok &= big_addsub(t1, t2, -1, t1);
     if (!ok) {
+        if (path) *path = kPathCapacity;
         atomicOr(err, 2u);
         return 0;
     }

@@ -24,6 +24,7 @@ struct gi_mesh {
     gi_ctx* ctx = nullptr;
     gi::MeshBuffers b;
     bool has64 = false;
+    double build_ms = 0.0;  // device time of validation + BVH build (CUDA events on the build stream)
 };
 
 // Pinned host blocks that results are copied into.  A call takes one block

@@ -78,6 +78,8 @@ struct JobDev {
     DevPose pa, pb;
 };
 
+constexpr int kLevelTimes = 32;  // levels whose end times are recorded
+
 // Device counters of one intersect launch sequence (zeroed by the host).
 struct Counters {
     // hot counters, each on its own 128-byte line (polled and updated by every warp)
@@ -112,6 +114,18 @@ struct Counters {
     unsigned long long exact_signs;
     unsigned long long exact_points;
     unsigned long long tested;  // candidates run through the first filter stage
+    // level-synchronous traversal: per level slot (level % 3), node pairs made
+    // (low half) and leaf pairs made (high half) during that level
+    unsigned pad6[16];
+    unsigned long long lvl[3];
+    unsigned pad7[26];
+    unsigned bar_count;  // grid barrier: blocks arrived
+    unsigned pad8[31];
+    unsigned bar_gen;    // grid barrier: barriers completed
+    unsigned bstop;      // decision of the last completed barrier: 1 = the traversal is over
+    unsigned pad9[30];
+    unsigned long long t_start;                 // globaltimer at the launch's start (ns)
+    unsigned long long level_ns[kLevelTimes];   // globaltimer when level l ended (its barrier completed)
 };
 
 constexpr unsigned kOvfFrontier = 1u, kOvfCand = 2u, kOvfRes = 4u, kOvfEsc = 8u;
@@ -136,6 +150,7 @@ struct Bufs {
     int precision;    // 0 FP32 cascade, 1 FP64
     int two_frame;    // also test child boxes in B's own frame (fewer pairs, more work per pair)
     int deep_seed;    // seed from the depth-4 cuts (single-pair calls) instead of the depth-3 cuts
+    unsigned quad_below;  // level-synchronous traversal: levels of at most this many node pairs use the quad form
 };
 
 }  // namespace gi

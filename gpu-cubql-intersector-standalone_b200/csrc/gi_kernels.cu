@@ -1603,6 +1603,289 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Level-synchronous BVH4 x BVH4 traversal (one cooperative launch).
+//
+// In the queue traversal above, the levels' end times advance by 12-15 us while
+// one warp iteration takes about 3 us: most of a level is the hand-off of node
+// pairs between warps through tagged queue slots.  Here the grid moves level by
+// level instead.  All node pairs of a level, and the leaf pairs the previous
+// level made, are split among all warps in static chunks (warp w takes chunks
+// w, w + warps, ...); the children form the next level's list; one grid barrier
+// (about a microsecond) separates the levels, so a level costs one or a few warp
+// iterations plus the barrier.  A level of at most `quad_below` node pairs is
+// expanded in the quad form (a quarter of the dependent chain, 8 node pairs per
+// warp), a wider one in the lane form (32 per warp).
+//
+// Level l appends its node children (low half) and its leaf pairs (high half)
+// to the 64-bit counter lvl[l % 3], one atomic per warp and chunk.  The last
+// block to arrive at the barrier that ends level l decides whether the
+// traversal is over (no pair made, or the abort flag set: the same decision
+// for every block), clears lvl[(l + 2) % 3] (last read before level l began)
+// and stamps the level's end time.  Node pairs of level l live in half l % 2 of
+// the queue buffer; leaf pairs are appended to the candidate list in level
+// order, so level l + 1 filters candidates [snap_l, snap_l + count) with snap
+// summed from the counters in every block alike.  Every barrier wait is
+// bounded; a spent wait sets kErrTimeout and the abort flag and the block ends.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid barrier ending level `lev` of the level-synchronous traversal.  Returns
+// false when the block's wait ran out (the block must leave the kernel).
+__device__ __forceinline__ bool level_barrier(const Bufs& B, unsigned& gen, unsigned lev)
+{
+    __shared__ unsigned s_ok;
+    Counters* C = B.cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_ok = 1u;
+        __threadfence();
+        const unsigned arrived = atomicAdd(&C->bar_count, 1u) + 1u;
+        if (arrived == gridDim.x) {
+            // every block has arrived: the counts of this level are final
+            C->bar_count = 0u;
+            const unsigned long long v = __ldcg(&C->lvl[lev % 3u]);
+            const unsigned ab = ld_vol(&C->abort_);
+            C->bstop = (ab != 0u || v == 0ull) ? 1u : 0u;
+            C->lvl[(lev + 2u) % 3u] = 0ull;
+            atomicMax(&C->q_tail, 2u * (unsigned)v);  // both halves of the queue buffer must hold the widest level
+            if (lev < (unsigned)kLevelTimes) C->level_ns[lev] = globaltimer_ns();
+            __threadfence();
+            atomicExch(&C->bar_gen, gen + 1u);
+        } else {
+            unsigned spins = 0;
+            while (ld_acq(&C->bar_gen) == gen) {
+                if (++spins > kIdleSpins) {
+                    atomicOr(&C->err, kErrTimeout);
+                    atomicExch(&C->abort_, 1u);
+                    s_ok = 0u;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        gen++;
+    }
+    __syncthreads();
+    return s_ok != 0u;
+}
+
+// Level 0: every pair of the two meshes' cut entries; overlapping pairs become
+// the first level's node pairs or candidates.
+template <bool F64>
+__device__ __forceinline__ void seed_levels(const Bufs& B, unsigned gw, unsigned nw, uint4* front, uint32_t capL)
+{
+    using S = typename Prec<F64>::S;
+    Counters* C = B.cnt;
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned per_job = seed_tests_per_job(B);
+    const unsigned total = B.njobs * per_job;
+    const unsigned coff = B.deep_seed ? (unsigned)kCutMax : 0u;
+    for (unsigned base = gw * 32u; base < total; base += nw * 32u) {
+        const unsigned g = base + lane;
+        bool fr = false, cand = false;
+        uint32_t ra = 0, rb = 0, job = 0;
+        if (g < total) {
+            job = g / per_job;
+            const unsigned t = g % per_job;
+            const JobDev& J = B.jobs[job];
+            const bool both = J.A.nt && J.B.nt;
+            const unsigned nA = both ? __ldg(J.A.ncuts + (B.deep_seed ? 1 : 0)) : 0u;
+            const unsigned nB = both ? __ldg(J.B.ncuts + (B.deep_seed ? 1 : 0)) : 0u;
+            if (t < nA * nB) {
+                const unsigned i = coff + t / nB, j = coff + t % nB;
+                const S* ba_ = F64 ? (const S*)J.A.cutBox64 : (const S*)J.A.cutBox;
+                const S* bb_ = F64 ? (const S*)J.B.cutBox64 : (const S*)J.B.cutBox;
+                Box<S> ba, bb;
+                for (int k = 0; k < 3; k++) {
+                    ba.lo[k] = ba_[6 * i + k];
+                    ba.hi[k] = ba_[6 * i + 3 + k];
+                    bb.lo[k] = bb_[6 * j + k];
+                    bb.hi[k] = bb_[6 * j + 3 + k];
+                }
+                if (!J.pa.identity) world_box(J.pa, ba);
+                if (!J.pb.identity) world_box(J.pb, bb);
+                if (overlap(ba, bb)) {
+                    ra = J.A.cutRef[i];
+                    rb = J.B.cutRef[j];
+                    cand = (ra & kLeaf) && (rb & kLeaf);
+                    fr = !cand;
+                }
+            }
+        }
+        const unsigned fb = __ballot_sync(0xffffffffu, fr), cb = __ballot_sync(0xffffffffu, cand);
+        if (!(fb | cb)) continue;
+        unsigned long long old = 0;
+        if (lane == 0) old = atomicAdd(&C->lvl[0], ((unsigned long long)__popc(cb) << 32) + __popc(fb));
+        old = __shfl_sync(0xffffffffu, old, 0);
+        const unsigned lt = (1u << lane) - 1u;
+        if (fr) {
+            const unsigned pf = (unsigned)old + __popc(fb & lt);
+            if (pf < capL) {
+                front[pf] = make_uint4(job, ra, rb, 0u);
+            } else {
+                atomicOr(&C->overflow, kOvfFrontier);
+                atomicExch(&C->abort_, 1u);
+            }
+        }
+        if (cand) {
+            const unsigned pc = (unsigned)(old >> 32) + __popc(cb & lt);
+            if (pc < B.cap_cand) {
+                B.cand[pc] = make_uint4(job, ra & ~kLeaf, rb & ~kLeaf, 0u);
+            } else {
+                atomicOr(&C->overflow, kOvfCand);
+                atomicExch(&C->abort_, 1u);
+            }
+        }
+    }
+}
+
+// Reserves the warp's children in one atomic: node pairs of the next level and
+// candidates of this level.  nf / nc: this lane's counts.  Returns this lane's
+// first node-pair slot (f) and first candidate slot (c).
+__device__ __forceinline__ void level_reserve(const Bufs& B, unsigned lev, unsigned snap, unsigned nf, unsigned nc,
+                                              unsigned& f, unsigned& c)
+{
+    const unsigned lane = threadIdx.x & 31;
+    unsigned incf = nf, incc = nc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned yf = __shfl_up_sync(0xffffffffu, incf, o);
+        const unsigned yc = __shfl_up_sync(0xffffffffu, incc, o);
+        if (lane >= (unsigned)o) {
+            incf += yf;
+            incc += yc;
+        }
+    }
+    unsigned long long old = 0;
+    if (lane == 31 && (incf | incc))
+        old = atomicAdd(&B.cnt->lvl[lev % 3u], ((unsigned long long)incc << 32) + incf);
+    old = __shfl_sync(0xffffffffu, old, 31);
+    f = (unsigned)old + incf - nf;
+    c = snap + (unsigned)(old >> 32) + incc - nc;
+}
+
+template <bool F64>
+__global__ void __launch_bounds__(kTravThreads, 2) k_traverse_levels(Bufs B)
+{
+    Counters* C = B.cnt;
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned nw = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t capL = B.cap_queue / 2u;
+    uint4* const front0 = B.queue;
+    uint4* const front1 = B.queue + capL;
+    if (blockIdx.x == 0 && threadIdx.x == 0) C->t_start = globaltimer_ns();
+    unsigned long long visited = 0, decided = 0, tested = 0;
+    unsigned gen = 0, snap = 0, lev = 0;
+    bool ovf_f = false, ovf_c = false;
+    seed_levels<F64>(B, gw, nw, front0, capL);
+    for (;;) {
+        if (!level_barrier(B, gen, lev)) return;
+        if (__ldcg(&C->bstop)) break;
+        // the pairs made by level `lev`, expanded and filtered by level lev + 1
+        const unsigned long long v = __ldcg(&C->lvl[lev % 3u]);
+        const unsigned n = min((unsigned)v, capL);
+        const unsigned cbase = snap, cend = min(snap + (unsigned)(v >> 32), B.cap_cand);
+        snap += (unsigned)(v >> 32);
+        ++lev;
+        const uint4* cur = (lev & 1u) ? front0 : front1;
+        uint4* nxt = (lev & 1u) ? front1 : front0;
+        const bool quad = n <= B.quad_below;
+        const unsigned per = quad ? 8u : 32u;
+        const unsigned node_chunks = (n + per - 1u) / per;
+        const unsigned chunks = node_chunks + (cend > cbase ? (cend - cbase + 31u) / 32u : 0u);
+        for (unsigned k = gw; k < chunks; k += nw) {
+            if (k < node_chunks) {
+                if (quad) {
+                    const unsigned unit = lane >> 2, sub = lane & 3u;
+                    const unsigned idx = k * 8u + unit;
+                    const bool have = idx < n;
+                    const uint4 ent = have ? __ldcg(cur + idx) : make_uint4(0u, kEmpty, kEmpty, 0u);
+                    visited += (have && sub == 0u) ? 1u : 0u;
+                    unsigned fm = 0, cm = 0;
+                    uint32_t ca = kEmpty, cb[4];
+                    expand_quad<F64>(B, ent, have, sub, fm, cm, ca, cb);
+                    unsigned f, c;
+                    level_reserve(B, lev, snap, __popc(fm), __popc(cm), f, c);
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        if ((fm >> j) & 1u) {
+                            if (f < capL) nxt[f] = make_uint4(ent.x, ca, cb[j], 0u);
+                            else ovf_f = true;
+                            f++;
+                        }
+                        if ((cm >> j) & 1u) {
+                            if (c < B.cap_cand) B.cand[c] = make_uint4(ent.x, ca & ~kLeaf, cb[j] & ~kLeaf, 0u);
+                            else ovf_c = true;
+                            c++;
+                        }
+                    }
+                } else {
+                    const unsigned idx = k * 32u + lane;
+                    const bool have = idx < n;
+                    uint4 ent = make_uint4(0u, kEmpty, kEmpty, 0u);
+                    unsigned fm = 0, cm = 0;
+                    uint32_t ca[4], cb[4];
+                    if (have) {
+                        ent = __ldcg(cur + idx);
+                        visited++;
+                        expand_pair<F64>(B, ent, fm, cm, ca, cb);
+                    }
+                    unsigned f, c;
+                    level_reserve(B, lev, snap, __popc(fm), __popc(cm), f, c);
+                    // child slot q = 4i + j is the pair (A child i, B child j); the
+                    // unrolled loop indexes the registers with constants
+#pragma unroll
+                    for (int q = 0; q < 16; q++) {
+                        if ((fm >> q) & 1u) {
+                            if (f < capL) nxt[f] = make_uint4(ent.x, ca[q >> 2], cb[q & 3], 0u);
+                            else ovf_f = true;
+                            f++;
+                        }
+                        if ((cm >> q) & 1u) {
+                            if (c < B.cap_cand)
+                                B.cand[c] = make_uint4(ent.x, ca[q >> 2] & ~kLeaf, cb[q & 3] & ~kLeaf, 0u);
+                            else ovf_c = true;
+                            c++;
+                        }
+                    }
+                }
+            } else {
+                const unsigned i = cbase + (k - node_chunks) * 32u + lane;
+                const bool have = i < cend;
+                const uint4 cnd = have ? __ldcg(B.cand + i) : make_uint4(0u, 0u, 0u, 0u);
+                filter_candidates<F64>(B, have, cnd, decided, tested);
+            }
+        }
+        if (ovf_f || ovf_c) {
+            if (ovf_f) atomicOr(&C->overflow, kOvfFrontier);
+            if (ovf_c) atomicOr(&C->overflow, kOvfCand);
+            atomicExch(&C->abort_, 1u);
+            ovf_f = ovf_c = false;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        visited += __shfl_xor_sync(0xffffffffu, visited, o);
+        decided += __shfl_xor_sync(0xffffffffu, decided, o);
+        tested += __shfl_xor_sync(0xffffffffu, tested, o);
+    }
+    if (lane == 0) {
+        if (visited) atomicAdd(&C->node_pairs, visited);
+        if (decided) atomicAdd(&C->filter_decided, decided);
+        if (tested) atomicAdd(&C->tested, tested);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        C->levels = lev;
+        C->work_cand = (unsigned long long)snap << 32;  // candidates made, for the host's retry sizing
+    }
+}
+
 // ===========================================================================
 // Exact stage and segments
 // ===========================================================================
@@ -2251,7 +2534,10 @@ cudaError_t query_launch(int device, LaunchCfg* cfg)
     cudaDeviceProp prop;
     GI_TRY(cudaGetDeviceProperties(&prop, device));
     cfg->sms = prop.multiProcessorCount;
-    int n[2][2] = {};
+    int n[2][2] = {}, nl[2] = {};
+    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nl[0], k_traverse_levels<false>, kTravThreads, 0));
+    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nl[1], k_traverse_levels<true>, kTravThreads, 0));
+    for (int a = 0; a < 2; a++) cfg->levels_per_sm[a] = nl[a] < 1 ? 1 : (nl[a] > 2 ? 2 : nl[a]);
     GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n[0][0], k_traverse<false, false>, kTravThreads, 0));
     GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n[0][1], k_traverse<false, true>, kTravThreads, 0));
     GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n[1][0], k_traverse<true, false>, kTravThreads, 0));
@@ -2269,6 +2555,15 @@ cudaError_t launch_traverse(const Bufs& b, const LaunchCfg& cfg, int precision, 
 {
     note_launches(1);
     const int f64 = precision == 1 ? 1 : 0, q = shape.quad ? 1 : 0;
+    if (shape.levels) {
+        // cooperative: the grid barriers need every block resident
+        const int grid = (shape.one_per_sm ? 1 : cfg.levels_per_sm[f64]) * cfg.sms;
+        Bufs bb = b;
+        bb.quad_below = shape.quad ? (unsigned)(grid * (kTravThreads / 32) * 8) : 0u;
+        void* args[] = {&bb};
+        return cudaLaunchCooperativeKernel(f64 ? (const void*)k_traverse_levels<true> : (const void*)k_traverse_levels<false>,
+                                           dim3(grid), dim3(kTravThreads), args, 0, st);
+    }
     const int grid = (shape.one_per_sm ? 1 : cfg.trav_per_sm[f64][q]) * cfg.sms;
     if (f64) {
         if (q) k_traverse<true, true><<<grid, kTravThreads, 0, st>>>(b);

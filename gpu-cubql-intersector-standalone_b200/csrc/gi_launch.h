@@ -49,21 +49,26 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t 
 struct LaunchCfg {
     int sms = 0;
     int trav_per_sm[2][2] = {};  // resident traversal blocks per SM, [FP64][quad form]
+    int levels_per_sm[2] = {};   // resident blocks of the level-synchronous traversal (at most 2), [FP64]
     int trav_threads = 256;
 };
 
-// Traversal shapes the tuner chooses from: expansion form (one node pair per
-// lane or per quad) x blocks per SM (all resident, or one).
+// Traversal shapes the tuner chooses from: the work-queue traversal or the
+// level-synchronous one (bit 2); expansion form (bit 1: one node pair per quad
+// of lanes; for the level-synchronous traversal, the quad form on levels of at
+// most 8 node pairs per warp) x blocks per SM (bit 0: one, else all resident).
 struct TravShape {
     bool quad = false;
     bool one_per_sm = false;
+    bool levels = false;
 };
-constexpr int kTravShapes = 4;
+constexpr int kTravShapes = 8;
 inline TravShape trav_shape(int k)
 {
     TravShape t;
     t.quad = (k & 2) != 0;
     t.one_per_sm = (k & 1) != 0;
+    t.levels = (k & 4) != 0;
     return t;
 }
 cudaError_t query_launch(int device, LaunchCfg* cfg);

@@ -230,6 +230,12 @@ class Context:
         self.check(rc, "gi_intersect_oneshot")
         return Result(r)
 
+    def wait_stream(self, stream_ptr):
+        """Orders the library's streams after the work queued so far on a CUDA
+        stream (its cudaStream_t as an int, e.g. torch.cuda.current_stream().cuda_stream):
+        call it before passing device inputs produced on that stream."""
+        self.check(self._lib.gi_wait_stream(self.handle, ctypes.c_void_p(int(stream_ptr) or None)), "gi_wait_stream")
+
     def classify_pairs(self, A, B, pose_a, pose_b, d_pairs_ptr, npairs, d_out_ptr, precision=GI_PREC_FP32_CASCADE):
         """Exact test of npairs candidate pairs (device pointers: int32 pairs, uint8 out)."""
         rc = self._lib.gi_classify_pairs(self.handle, A.handle, ctypes.byref(pose_a) if pose_a is not None else None,
@@ -248,6 +254,28 @@ class Context:
                                                  ctypes.c_void_p(d_pairs_ptr), npairs, int(precision),
                                                  ctypes.c_void_p(d_out_ptr))
         self.check(rc, "gi_classify_pairs_noalloc")
+
+    def predicate_signs(self, kind, pts, drop=None):
+        """The device's orientation predicates, stage by stage, on host arrays:
+        pts (n, 12) for GI_PRED_ORIENT3D (a, b, c, d) or (n, 9) for GI_PRED_ORIENT2D
+        (a, b, c) with drop (n,) axes.  Returns int8 (n, 8): FP32 filter (line,
+        plane form), FP64 semi-static filter (line, plane form), the exact
+        stage's FP64 filter, the exact integer sign, the exact stage's answer, and
+        the integer branch (0 int128, 1 multi-limb)."""
+        per = 12 if kind == _abi.GI_PRED_ORIENT3D else 9
+        p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, per)
+        n = p.shape[0]
+        out = np.zeros((n, 8), dtype=np.int8)
+        d = None
+        if kind == _abi.GI_PRED_ORIENT2D:
+            d = np.ascontiguousarray(drop, dtype=np.int32).reshape(-1)
+            if d.shape[0] != n:
+                raise ValueError("one drop axis per query")
+        rc = self._lib.gi_predicate_signs(self.handle, int(kind), p.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                          d.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) if d is not None else None,
+                                          n, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int8)))
+        self.check(rc, "gi_predicate_signs")
+        return out
 
     def load_scene(self, path_a, path_b, scale_to_unit=True):
         """Both OFF files loaded, the scene normalised on the device and both meshes
@@ -348,7 +376,9 @@ class Mesh:
         nodes, nbytes = ctypes.c_uint64(), ctypes.c_uint64()
         self.ctx._lib.gi_mesh_info(self.handle, ctypes.byref(nv), ctypes.byref(nt), ctypes.byref(nodes),
                                    ctypes.byref(nbytes))
-        return dict(nv=nv.value, nt=nt.value, nodes=nodes.value, bytes=nbytes.value)
+        ms = ctypes.c_double()
+        self.ctx._lib.gi_mesh_build_ms(self.handle, ctypes.byref(ms))
+        return dict(nv=nv.value, nt=nt.value, nodes=nodes.value, bytes=nbytes.value, build_ms=ms.value)
 
     def download(self):
         """The vertices as stored on the device (after any normalisation), (nv, 3) float64."""

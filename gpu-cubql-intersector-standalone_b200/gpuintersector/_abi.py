@@ -19,21 +19,31 @@ GI_FLAG_TINY_BUFFERS = 1
 GI_FLAG_FIXED_SHAPE = 0x100
 
 
+GI_TRAVERSE_SHAPES = 8
+
+
 def GI_FLAG_SHAPE(k):
-    return (int(k) & 3) << 9
+    return (int(k) & 7) << 9
 
 
 GI_PREC_FP32_CASCADE = 0
 GI_PREC_FP64 = 1
 GI_NOALLOC_MAX_PAIRS = 1 << 20
+GI_PRED_ORIENT3D = 0
+GI_PRED_ORIENT2D = 1
+GI_SIGN_UNDECIDED = 2
+GI_SIGN_NA = 3
+GI_BRANCH_INT128 = 0
+GI_BRANCH_MULTILIMB = 1
+GI_BRANCH_CAPACITY = 2
 
 # every symbol include/gi/gi.h declares (checked by the CPU tests)
 EXPORTED = [
-    "gi_create", "gi_destroy", "gi_status_string", "gi_last_error", "gi_device_count",
-    "gi_mesh_upload", "gi_mesh_upload_device", "gi_mesh_release", "gi_mesh_info",
+    "gi_create", "gi_destroy", "gi_status_string", "gi_last_error", "gi_device_count", "gi_wait_stream",
+    "gi_mesh_upload", "gi_mesh_upload_device", "gi_mesh_release", "gi_mesh_info", "gi_mesh_build_ms",
     "gi_pose_identity", "gi_pose_from_euler_deg", "gi_pose_apply",
     "gi_intersect_opts_default", "gi_intersect", "gi_intersect_oneshot", "gi_intersect_batch",
-    "gi_classify_pairs", "gi_classify_pairs_noalloc",
+    "gi_classify_pairs", "gi_classify_pairs_noalloc", "gi_predicate_signs",
     "gi_off_load", "gi_off_arrays", "gi_off_free", "gi_scene_load", "gi_mesh_download",
     "gi_curves_build", "gi_result_curves", "gi_curves_vertices", "gi_curves_polylines", "gi_curves_free",
     "gi_records_write_csv", "gi_pairs_diff", "gi_sweep_poses",
@@ -87,10 +97,14 @@ class Stats(ctypes.Structure):
                 ("segments", ctypes.c_uint64), ("levels", ctypes.c_uint32), ("retries", ctypes.c_uint32),
                 ("launches", ctypes.c_uint32), ("traverse_shape", ctypes.c_uint32),
                 ("ms_traverse", ctypes.c_double), ("ms_exact", ctypes.c_double), ("ms_segments", ctypes.c_double),
-                ("ms_sort", ctypes.c_double), ("ms_total", ctypes.c_double)]
+                ("ms_sort", ctypes.c_double), ("ms_total", ctypes.c_double),
+                ("level_times", ctypes.c_uint32), ("reserved2", ctypes.c_uint32),
+                ("level_end_ms", ctypes.c_double * 32)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("level_end_ms", "reserved2")}
+        d["level_end_ms"] = [self.level_end_ms[i] for i in range(min(self.level_times, 32))]
+        return d
 
 
 class PairJob(ctypes.Structure):
@@ -123,10 +137,12 @@ def load(path=None):
         "gi_status_string": ([ctypes.c_int], ctypes.c_char_p),
         "gi_last_error": ([vp], ctypes.c_char_p),
         "gi_device_count": ([ctypes.POINTER(ctypes.c_int32)], st),
+        "gi_wait_stream": ([vp, vp], st),
         "gi_mesh_upload": ([vp, dp, ctypes.c_uint32, up, ctypes.c_uint32, ctypes.POINTER(vp)], st),
         "gi_mesh_upload_device": ([vp, vp, ctypes.c_uint32, vp, ctypes.c_uint32, ctypes.POINTER(vp)], st),
         "gi_mesh_release": ([vp, vp], st),
         "gi_mesh_info": ([vp, up, up, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)], st),
+        "gi_mesh_build_ms": ([vp, dp], st),
         "gi_pose_identity": ([ctypes.POINTER(Pose)], st),
         "gi_pose_from_euler_deg": ([dp, dp, dp, ctypes.POINTER(Pose)], st),
         "gi_pose_apply": ([ctypes.POINTER(Pose), dp, ctypes.c_uint64, dp], st),
@@ -142,6 +158,8 @@ def load(path=None):
                                ctypes.c_int32, vp], st),
         "gi_classify_pairs_noalloc": ([vp, vp, ctypes.POINTER(Pose), vp, ctypes.POINTER(Pose), vp, ctypes.c_uint32,
                                        ctypes.c_int32, vp], st),
+        "gi_predicate_signs": ([vp, ctypes.c_int32, dp, ctypes.POINTER(ctypes.c_int32), ctypes.c_uint64,
+                                ctypes.POINTER(ctypes.c_int8)], st),
         "gi_off_load": ([ctypes.c_char_p, ctypes.c_uint32, ctypes.POINTER(vp), ctypes.POINTER(OffReport)], st),
         "gi_off_arrays": ([vp, ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(up),
                            ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(up)], st),

@@ -43,6 +43,16 @@
  *
  * Threading: one gi_ctx owns one CUDA stream; calls on the same context are
  * serialised by the caller.  Different contexts may run concurrently.
+ *
+ * Device-pointer arguments (gi_mesh_upload_device, gi_classify_pairs,
+ * gi_classify_pairs_noalloc): the library reads and writes them on the
+ * context's own stream, which is a non-blocking stream and is NOT ordered after
+ * the caller's streams (for example torch's current stream).  Before such a
+ * call, the work that produces the inputs (and any earlier work on the output
+ * buffer) must be complete: synchronise the producing stream, or call
+ * gi_wait_stream with it.  These calls block until their own device work is
+ * done, so the outputs are complete when they return and later work on any
+ * stream may read or overwrite them.
  */
 #ifndef GI_GI_H
 #define GI_GI_H
@@ -77,12 +87,15 @@ typedef struct gi_server gi_server;
 /* gi_options.flags */
 #define GI_FLAG_TINY_BUFFERS 1u /* start every intersect buffer at 64 entries: exercises the
                                    capacity-overflow / retry path (host-side fault injection) */
-/* The traversal shape (expansion form x blocks per SM) is autotuned per workload
- * class on the context's own calls.  GI_FLAG_FIXED_SHAPE | GI_FLAG_SHAPE(k),
- * k in 0..3 (bit 1: one node pair per quad of lanes, bit 0: one block per SM),
- * fixes it instead (every shape gives the same results). */
+/* The traversal shape is autotuned per workload class on the context's own
+ * calls.  GI_FLAG_FIXED_SHAPE | GI_FLAG_SHAPE(k), k in 0..7, fixes it instead
+ * (every shape gives the same results): bit 2 selects the level-synchronous
+ * traversal (grid barriers between the levels) over the work-queue one; bit 1
+ * the quad form (one node pair per quad of lanes; level-synchronous: on levels
+ * of at most 8 node pairs per warp); bit 0 one block per SM instead of all
+ * resident blocks. */
 #define GI_FLAG_FIXED_SHAPE 0x100u
-#define GI_FLAG_SHAPE(k) ((((uint32_t)(k)) & 3u) << 9)
+#define GI_FLAG_SHAPE(k) ((((uint32_t)(k)) & 7u) << 9)
 
 typedef struct {
     int32_t device;             /* CUDA device ordinal */
@@ -125,13 +138,20 @@ typedef struct {
     uint32_t levels;                  /* traversal levels */
     uint32_t retries;                 /* capacity retries */
     uint32_t launches;                /* kernels launched by this call */
-    uint32_t traverse_shape;          /* traversal shape used: bit 1 quad form, bit 0 one block per SM */
+    uint32_t traverse_shape;          /* traversal shape used (GI_FLAG_SHAPE numbering) */
     double ms_traverse;               /* device time: traversal + first filter */
     double ms_exact;                  /* device time: FP64 / exact stage */
     double ms_segments;               /* device time: segment construction */
     double ms_sort;                   /* device time: output ordering (the part after segment construction
                                          ends; ranking overlaps the segments) */
     double ms_total;                  /* device time of the whole call */
+    /* level-synchronous traversal only (else level_times = 0): level_end_ms[l]
+     * is the time from the traversal's start to the end of level l (level 0:
+     * the seeding from the cut pairs; level l > 0 expands the node pairs made
+     * by level l - 1 and filters its leaf pairs), for the first level_times levels */
+    uint32_t level_times;
+    uint32_t reserved2;
+    double level_end_ms[32];
 } gi_stats;
 
 /* Batched job: one mesh pair with its poses. */
@@ -155,6 +175,13 @@ gi_status gi_destroy(gi_ctx* ctx);
 const char* gi_status_string(gi_status s);
 const char* gi_last_error(const gi_ctx* ctx);
 gi_status gi_device_count(int32_t* n);
+/* Orders the context's streams after all work queued so far on `stream` (a
+ * cudaStream_t passed as a pointer; NULL names the legacy default stream), so
+ * that device inputs produced there are complete before the context's next
+ * call reads them.  Queues a wait; does not block the host.  No counterpart in
+ * the reference, whose calls run on the legacy default stream with device-wide
+ * synchronisation (src/GPUIntersector/KernelBVHController.cu:258-261). */
+gi_status gi_wait_stream(gi_ctx* ctx, void* stream);
 
 /* ---- meshes (KernelBVHController::construct) ----------------------------- */
 /* Host arrays: verts_xyz[3*nv] doubles, tris[3*nt] vertex indices. */
@@ -165,6 +192,11 @@ gi_status gi_mesh_upload_device(gi_ctx* ctx, const double* d_verts_xyz, uint32_t
                                 uint32_t nt, gi_mesh** out);
 gi_status gi_mesh_release(gi_ctx* ctx, gi_mesh* mesh);
 gi_status gi_mesh_info(const gi_mesh* mesh, uint32_t* nv, uint32_t* nt, uint64_t* nodes, uint64_t* device_bytes);
+/* Device time in ms of the mesh's validation and BVH build (CUDA events around
+ * the build kernels on the build stream; the upload's copies are not in it):
+ * ExecutionStats::buildRefitMeshAMs / buildRefitMeshBMs
+ * (src/common/ExecutionStats.h:25-26). */
+gi_status gi_mesh_build_ms(const gi_mesh* mesh, double* ms);
 
 /* ---- poses (setTransformBoth, RotationTools.h:28-70) ---------------------- */
 gi_status gi_pose_identity(gi_pose* out);
@@ -207,14 +239,49 @@ gi_status gi_classify_pairs(gi_ctx* ctx, const gi_mesh* A, const gi_pose* pose_a
  * scratch is one fixed 4 MiB array in the library's device memory per device.
  *  - npairs above GI_NOALLOC_MAX_PAIRS -> GI_ERR_CAPACITY, nothing queued;
  *  - the first call on a device does a one-time set-up (looks up the array's
- *    device address); make it before any stream capture begins;
+ *    device address with that device current); make that first call before
+ *    any stream capture begins;
  *  - the array is shared by all contexts on a device: calls whose device work
- *    overlaps in time race on it.  Calls are blocking, so calls issued one
- *    after another are safe. */
+ *    overlaps in time race on it.  Every call blocks until its device work is
+ *    done, so calls issued one after another from the host are safe. */
 #define GI_NOALLOC_MAX_PAIRS 1048576u
 gi_status gi_classify_pairs_noalloc(gi_ctx* ctx, const gi_mesh* A, const gi_pose* pose_a, const gi_mesh* B,
                                     const gi_pose* pose_b, const int32_t* d_pairs, uint32_t npairs,
                                     int32_t precision_mode, uint8_t* d_out);
+
+/* ---- predicate signs (diagnostics of the exact path) ----------------------- */
+/* The device's orientation predicates on caller-given points, stage by stage,
+ * so that every sign the intersection path can take is checkable against an
+ * exact evaluation.  Replaces, for inspection, the reference's device
+ * predicates: orient3d_interval (src/GPU_exact_predicates/GPUPredicatesCommon.h:
+ * 38-100), orient3d_double_interval (src/GPU_exact_predicates/DoublePredicate.cu:
+ * 75-93) and orient3d_exact_V2 / the 2D SAT tests
+ * (src/GPU_exact_predicates/ExactBigIntPredicate.cu:180-212, 236-272).
+ *   GI_PRED_ORIENT3D: pts holds 12 doubles per query (a, b, c, d); the sign is
+ *     that of det[a - d; b - d; c - d] (positive when d lies below the plane
+ *     through a, b, c oriented counter-clockwise).
+ *   GI_PRED_ORIENT2D: pts holds 9 doubles per query (a, b, c) and drop[i] in
+ *     0..2 names the coordinate left out; with (u, v) = (drop + 1, drop + 2) mod
+ *     3 the sign is that of (a_u - c_u)(b_v - c_v) - (a_v - c_v)(b_u - c_u).
+ * out receives 8 bytes per query:
+ *   [0] FP32 semi-static filter, line-order form   [1] FP32 filter, vertex-versus-plane form
+ *   [2] FP64 semi-static filter, line-order form   [3] FP64 filter, vertex-versus-plane form
+ *   [4] FP64 filter of the exact stage             [5] exact integer sign (always computed)
+ *   [6] the exact stage's answer (filter, then integers)
+ *   [7] integer branch of [5]: GI_BRANCH_INT128, GI_BRANCH_MULTILIMB or GI_BRANCH_CAPACITY
+ * Signs are -1, 0, +1; a filter that does not decide gives GI_SIGN_UNDECIDED;
+ * orient2d has no FP32 or semi-static form (GI_SIGN_NA in [0..3]).
+ * Host arrays in and out; the call blocks.  Coordinates outside the supported
+ * domain give GI_ERR_RANGE, at most 2^26 queries per call. */
+#define GI_PRED_ORIENT3D 0
+#define GI_PRED_ORIENT2D 1
+#define GI_SIGN_UNDECIDED 2
+#define GI_SIGN_NA 3
+#define GI_BRANCH_INT128 0
+#define GI_BRANCH_MULTILIMB 1
+#define GI_BRANCH_CAPACITY 2
+gi_status gi_predicate_signs(gi_ctx* ctx, int32_t kind, const double* pts, const int32_t* drop, uint64_t n,
+                             int8_t* out);
 
 /* ---- ingestion (upstream of the path) -------------------------------------- */
 /* OFF files as the reference loads them (src/CPU/RobustOffLoader.h:120-186,

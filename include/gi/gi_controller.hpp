@@ -15,10 +15,15 @@
 //  * level / leafThreshold / batchMultiplier / dual-tree step counts tune the
 //    reference's level-cut BVH and are accepted and ignored (the LBVH has no
 //    level cut and the traversal sizes itself);
-//  * predicate modes 0-4 (apps/mainApplication.cpp:1595-1607) all begin with
-//    the float filter; every one maps to the exact FP32 cascade here, so all
-//    give the exact pair set.  setPrecisionMode(GI_PREC_FP64) selects the
-//    plain FP64 form;
+//  * the predicate mode argument (runIntersectionPipeline's gpuDouble,
+//    KernelBVHController.h:60-63; runGridForestIntersectionPipeline's
+//    gpuPredicateMode) is honoured: the reference's modes 0-4
+//    (apps/mainApplication.cpp:1595-1607) all begin with the float filter and
+//    escalate through (simulated) double or integers to CPU CGAL, which is what
+//    the FP32 cascade does on the device (float filter -> FP64 filter -> exact
+//    integers), so they select GI_PREC_FP32_CASCADE; the added mode
+//    kPredicateModePlainFP64 (5) selects the plain FP64 form, and any other
+//    value throws gi::Error(GI_ERR_INVALID_ARG) instead of being ignored;
 //  * the output int2* is malloc-owned by the callee and released by the
 //    caller with std::free, as in the reference
 //    (SingleTreeBatchIntersector.cu:149-167); pairs come sorted by (a, b);
@@ -114,6 +119,15 @@ inline void xyz(const P& p, double out[3])
     out[1] = static_cast<double>(p.y());
     out[2] = static_cast<double>(p.z());
 }
+// The reference's predicate modes 0-4 and the added plain-FP64 mode -> GI_PREC_*.
+constexpr int kPredicateModePlainFP64 = 5;
+inline int32_t precision_for_predicate_mode(int mode)
+{
+    if (mode >= 0 && mode <= 4) return GI_PREC_FP32_CASCADE;
+    if (mode == kPredicateModePlainFP64) return GI_PREC_FP64;
+    throw Error(GI_ERR_INVALID_ARG, "predicate mode " + std::to_string(mode) +
+                                        " (reference modes are 0-4; 5 selects the plain FP64 form)");
+}
 inline void fill(ExecutionStats& s, const gi_stats& d)
 {
     s.detail = d;
@@ -200,9 +214,9 @@ public:
     // poses are applied, so a new pose costs one traversal and no rebuild.
     void runIntersectionPipeline(int /*batchMultiplier*/, int /*numberOfDualTreeSteps*/,
                                  int /*activateAsyncDownload*/, pair2i*& outFinalExactPairs, size_t& outFinalCount,
-                                 ExecutionStats& stats, int /*gpuDouble*/)
+                                 ExecutionStats& stats, int gpuDouble)
     {
-        gi_result* r = run(want_segments_);
+        gi_result* r = run(want_segments_, detail::precision_for_predicate_mode(gpuDouble));
         try {
             detail::take_pairs(r, outFinalExactPairs, outFinalCount, ctx_);
             keep_segments(r);
@@ -265,8 +279,6 @@ public:
     // src/CPU/MeshIntersectionCurves.cpp:27-91, on the device).
     void setWantSegments(bool on) { want_segments_ = on; }
     const std::vector<IntersectionSegment>& lastSegments() const { return segs_; }
-    // GI_PREC_FP32_CASCADE (default) or GI_PREC_FP64 (plain FP64 form).
-    void setPrecisionMode(int32_t mode) { precision_ = mode; }
     gi_ctx* context() const { return ctx_; }
     const gi_mesh* meshA() const { return A_; }
     const gi_mesh* meshB() const { return B_; }
@@ -304,13 +316,13 @@ private:
         stats.meshBTotalNodes = uint32_t(nodes);
     }
 
-    gi_result* run(bool segments)
+    gi_result* run(bool segments, int32_t precision)
     {
         if (!isGPUAllocated()) throw Error(GI_ERR_INVALID_ARG, "runIntersectionPipeline before construct");
         gi_intersect_opts o;
         gi_intersect_opts_default(&o);
         o.want_segments = segments ? 1 : 0;
-        o.precision_mode = precision_;
+        o.precision_mode = precision;
         gi_result* r = nullptr;
         detail::check(gi_intersect(ctx_, A_, &poseA_, B_, &poseB_, &o, &r), ctx_, "gi_intersect");
         return r;
@@ -345,7 +357,6 @@ private:
     double cA_[3] = {0, 0, 0}, cB_[3] = {0, 0, 0};
     double rotA_[3] = {0, 0, 0}, transA_[3] = {0, 0, 0}, rotB_[3] = {0, 0, 0}, transB_[3] = {0, 0, 0};
     gi_pose poseA_{}, poseB_{};
-    int32_t precision_ = GI_PREC_FP32_CASCADE;
     bool want_segments_ = false;
     std::vector<IntersectionSegment> segs_;
 };
@@ -358,7 +369,7 @@ inline void runGridForestIntersectionPipeline(MeshT&, MeshT&, const vec3d* hVert
                                               const tri3u* hIndicesA, int numTrianglesA, int /*maxCellSizeA*/,
                                               const vec3d* hVertsB, int numVertsB, const tri3u* hIndicesB,
                                               int numTrianglesB, int /*maxCellSizeB*/, int /*batchMultiplier*/,
-                                              int /*numberOfDualTreeSteps*/, int /*gpuPredicateMode*/,
+                                              int /*numberOfDualTreeSteps*/, int gpuPredicateMode,
                                               int /*leafThreshold*/, ExecutionStats& stats,
                                               pair2i*& outFinalExactPairs, size_t& outFinalCount,
                                               const PointT& centerA, const PointT& centerB, vec3d rotA, vec3d transA,
@@ -380,6 +391,7 @@ inline void runGridForestIntersectionPipeline(MeshT&, MeshT&, const vec3d* hVert
         gi_intersect_opts io;
         gi_intersect_opts_default(&io);
         io.want_segments = 0;
+        io.precision_mode = detail::precision_for_predicate_mode(gpuPredicateMode);
         detail::check(gi_intersect_oneshot(c, reinterpret_cast<const double*>(hVertsA), uint32_t(numVertsA),
                                            reinterpret_cast<const uint32_t*>(hIndicesA), uint32_t(numTrianglesA),
                                            &pa, reinterpret_cast<const double*>(hVertsB), uint32_t(numVertsB),

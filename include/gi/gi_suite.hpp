@@ -58,7 +58,7 @@ struct TestConfig {
     int numSteps = 10;
     double maxTranslation = 0.5;
     double maxRotationDeg = 15.0;
-    int enableGpuPrecision = GI_PREC_FP32_CASCADE;  // precision mode of the controller path
+    int enableGpuPrecision = 1;  // predicate mode of the controller path (reference modes 0-4; 5 = plain FP64)
     unsigned int seed = 1337;
     std::string csvOutputPath = "benchmark_results.csv";
     bool testMainGpuPipeline = true;
@@ -181,7 +181,6 @@ public:
         }
         if (config.testMainGpuPipeline) {
             if (!ctl_.isGPUAllocated()) ctl_.reconstructGPU(res.mainStats);
-            ctl_.setPrecisionMode(config.enableGpuPrecision);
             const auto t0 = std::chrono::steady_clock::now();
             float t[5];
             ctl_.setTransformBoth(rotA, transA, rotB, transB, t[0], t[1], t[2], t[3], t[4]);
@@ -204,7 +203,8 @@ public:
             const vec3d zero{0.0, 0.0, 0.0};
             runGridForestIntersectionPipeline(ma, mb, reinterpret_cast<const vec3d*>(pA.data()), A_.nv, A_.t, A_.nt,
                                               0, reinterpret_cast<const vec3d*>(pB.data()), B_.nv, B_.t, B_.nt, 0, 1,
-                                              0, 0, 4, res.standaloneStats, out, cnt, cA, cB, zero, zero, zero, zero);
+                                              0, config.enableGpuPrecision, 4, res.standaloneStats, out, cnt, cA, cB,
+                                              zero, zero, zero, zero);
             res.standaloneTimeMs = detail::ms_since(t0);
             const PairList got = take(out, cnt);
             res.standaloneCount = got.size();

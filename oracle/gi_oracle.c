@@ -211,7 +211,7 @@ static int o3_exact(const double* a, const double* b, const double* c, const dou
     return na;
 }
 
-int oc_orient3d(const double* a, const double* b, const double* c, const double* d)
+static int orient3d_sign(const double* a, const double* b, const double* c, const double* d)
 {
     double adx = a[0] - d[0], ady = a[1] - d[1], adz = a[2] - d[2];
     double bdx = b[0] - d[0], bdy = b[1] - d[1], bdz = b[2] - d[2];
@@ -252,7 +252,7 @@ static int o2_exact(const double* a, const double* b, const double* c, int drop,
     return exp_add(n1, t1, n2, t2, out);
 }
 
-int oc_orient2d(const double* a, const double* b, const double* c, int drop)
+static int orient2d_sign(const double* a, const double* b, const double* c, int drop)
 {
     int u, v;
     proj_axes(drop, &u, &v);
@@ -266,6 +266,79 @@ int oc_orient2d(const double* a, const double* b, const double* c, int drop)
     double e[20];
     int n = o2_exact(a, b, c, drop, e);
     return exp_sign(n, e);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Sign log (test hook): while enabled, every orient3d / orient2d call of the  */
+/* decision procedure is recorded with its inputs and exact sign, so that a    */
+/* test can replay the same calls through the device's predicates.            */
+/* ------------------------------------------------------------------------- */
+static pthread_mutex_t g_log_mu = PTHREAD_MUTEX_INITIALIZER;
+static volatile int g_log_on;
+static double* g_log_pts;   /* 12 doubles per entry (orient2d: 9 used) */
+static int32_t* g_log_meta; /* kind (0 orient3d, 1 orient2d), drop, sign per entry */
+static uint64_t g_log_n, g_log_cap;
+
+static void sign_log(int kind, const double* a, const double* b, const double* c, const double* d, int drop, int sgn)
+{
+    pthread_mutex_lock(&g_log_mu);
+    if (g_log_on && g_log_n < g_log_cap) {
+        double* p = g_log_pts + 12 * g_log_n;
+        memset(p, 0, 12 * sizeof(double));
+        memcpy(p, a, 3 * sizeof(double));
+        memcpy(p + 3, b, 3 * sizeof(double));
+        memcpy(p + 6, c, 3 * sizeof(double));
+        if (d) memcpy(p + 9, d, 3 * sizeof(double));
+        int32_t* m = g_log_meta + 3 * g_log_n;
+        m[0] = kind;
+        m[1] = drop;
+        m[2] = sgn;
+        g_log_n++;
+    }
+    pthread_mutex_unlock(&g_log_mu);
+}
+
+int oc_sign_log_begin(uint64_t cap)
+{
+    pthread_mutex_lock(&g_log_mu);
+    free(g_log_pts);
+    free(g_log_meta);
+    g_log_pts = (double*)malloc(sizeof(double) * 12 * (cap ? cap : 1));
+    g_log_meta = (int32_t*)malloc(sizeof(int32_t) * 3 * (cap ? cap : 1));
+    g_log_n = 0;
+    g_log_cap = (g_log_pts && g_log_meta) ? cap : 0;
+    g_log_on = g_log_cap != 0;
+    int ok = g_log_on ? 0 : -1;
+    pthread_mutex_unlock(&g_log_mu);
+    return ok;
+}
+
+uint64_t oc_sign_log_end(double** pts, int32_t** meta)
+{
+    pthread_mutex_lock(&g_log_mu);
+    g_log_on = 0;
+    uint64_t n = g_log_n;
+    *pts = g_log_pts;
+    *meta = g_log_meta;
+    g_log_pts = NULL;
+    g_log_meta = NULL;
+    g_log_n = g_log_cap = 0;
+    pthread_mutex_unlock(&g_log_mu);
+    return n;
+}
+
+int oc_orient3d(const double* a, const double* b, const double* c, const double* d)
+{
+    const int s = orient3d_sign(a, b, c, d);
+    if (g_log_on) sign_log(0, a, b, c, d, -1, s);
+    return s;
+}
+
+int oc_orient2d(const double* a, const double* b, const double* c, int drop)
+{
+    const int s = orient2d_sign(a, b, c, drop);
+    if (g_log_on) sign_log(1, a, b, c, NULL, drop, s);
+    return s;
 }
 
 /* ------------------------------------------------------------------------- */

@@ -73,6 +73,14 @@ int oc_orient3d(const double* a, const double* b, const double* c, const double*
  * using the cyclic pair (drop+1, drop+2). */
 int oc_orient2d(const double* a, const double* b, const double* c, int drop);
 
+/* Sign log (test hook): between begin and end, every oc_orient3d / oc_orient2d
+ * call (also those made inside the intersection tests) is recorded, up to cap
+ * entries: 12 doubles per entry (a, b, c, d; orient2d leaves d zero) and 3
+ * int32 (kind 0 = orient3d / 1 = orient2d, drop axis or -1, exact sign).  end
+ * returns the count and hands over both arrays (free with oc_free). */
+int oc_sign_log_begin(uint64_t cap);
+uint64_t oc_sign_log_end(double** pts, int32_t** meta);
+
 /* Closed-triangle intersection test (9 doubles per triangle, vertex-major). */
 int oc_tri_tri_intersect(const double* t1, const double* t2);
 

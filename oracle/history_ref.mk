@@ -2,7 +2,9 @@
 # (src/CPU/IntersectionHistory.h) compiled where it lies, with the program
 # history_ref_main.cpp.  Test infrastructure; needs the reference tree (REF) and
 # CUDA's vector_types.h.  Usage: make -f history_ref.mk REF=<reference root>
-REF ?= /root/reference
+ifndef REF
+$(error REF must name the reference project's root directory)
+endif
 CUDA ?= /usr/local/cuda
 CXX ?= g++
 HERE := $(dir $(lastword $(MAKEFILE_LIST)))

@@ -74,6 +74,10 @@ def lib():
             ctypes.POINTER(ctypes.c_int32), ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint8), ctypes.c_int]
         L.oc_classify_pairs.restype = ctypes.c_int
         L.oc_free.argtypes = [ctypes.c_void_p]
+        L.oc_sign_log_begin.argtypes = [ctypes.c_uint64]
+        L.oc_sign_log_begin.restype = ctypes.c_int
+        L.oc_sign_log_end.argtypes = [ctypes.POINTER(dp), ctypes.POINTER(ctypes.POINTER(ctypes.c_int32))]
+        L.oc_sign_log_end.restype = ctypes.c_uint64
         L.oc_hw_threads.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -128,6 +132,27 @@ def orient3d(a, b, c, d):
 def orient2d(a, b, c, drop):
     arr = [np.ascontiguousarray(x, dtype=np.float64) for x in (a, b, c)]
     return lib().oc_orient2d(*[_dp(x) for x in arr], int(drop))
+
+
+def record_signs(fn, cap=1 << 22):
+    """Runs fn() with the oracle's sign log on: every orient3d / orient2d call it
+    makes is returned with its exact sign as (pts (n, 12) float64, kind (n,),
+    drop (n,), sign (n,)), plus fn's return value.  Use nthreads=1 inside fn so
+    that the calls are logged in order."""
+    L = lib()
+    if L.oc_sign_log_begin(int(cap)) != 0:
+        raise MemoryError("oc_sign_log_begin")
+    pp = ctypes.POINTER(ctypes.c_double)()
+    mp = ctypes.POINTER(ctypes.c_int32)()
+    try:
+        ret = fn()
+    finally:
+        n = L.oc_sign_log_end(ctypes.byref(pp), ctypes.byref(mp))
+    pts = np.ctypeslib.as_array(pp, shape=(n * 12,)).reshape(n, 12).copy() if n else np.zeros((0, 12))
+    meta = np.ctypeslib.as_array(mp, shape=(n * 3,)).reshape(n, 3).copy() if n else np.zeros((0, 3), np.int32)
+    L.oc_free(ctypes.cast(pp, ctypes.c_void_p))
+    L.oc_free(ctypes.cast(mp, ctypes.c_void_p))
+    return (pts, meta[:, 0], meta[:, 1], meta[:, 2]), ret
 
 
 def tri_tri_intersect(t1, t2):

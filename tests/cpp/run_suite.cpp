@@ -143,12 +143,16 @@ int main(int argc, char** argv)
     int seg_ok = 0;
     if (segments) {
         ctl.setWantSegments(true);
+        int step = 0;
         for (const auto& r : res) {
             float t[5];
             ctl.setTransformBoth(r.rotA, r.transA, r.rotB, r.transB, t[0], t[1], t[2], t[3], t[4]);
             gi::pair2i* p = nullptr;
             size_t n = 0;
-            ctl.runIntersectionPipeline(1, 0, 0, p, n, st, 0);
+            // the reference's predicate modes 0-4 (FP32 cascade) and the plain FP64 mode in turn
+            const int mode = (step % 2) ? gi::detail::kPredicateModePlainFP64 : (step / 2) % 5;
+            ++step;
+            ctl.runIntersectionPipeline(1, 0, 0, p, n, st, mode);
             std::free(p);
             std::vector<double> pA(3 * A.v.size()), pB(3 * B.v.size());
             gi_pose_apply(&ctl.poseA(), reinterpret_cast<const double*>(A.v.data()), A.v.size(), pA.data());

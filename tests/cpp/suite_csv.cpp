@@ -38,6 +38,14 @@ int main(int argc, char** argv)
         return 3;
     if (!gi::TestSuite::exportStandaloneComputeCSV(gi::TestSuite::deriveFilename(base, "_standalone_breakdown"), rs))
         return 3;
+    // the reference's predicate modes (0-4) and the added plain-FP64 mode map to precision forms
+    for (int mode = -1; mode <= 6; ++mode) {
+        try {
+            std::printf("mode %d -> %d\n", mode, int(gi::detail::precision_for_predicate_mode(mode)));
+        } catch (const gi::Error& e) {
+            std::printf("mode %d -> error %d\n", mode, int(e.status));
+        }
+    }
     for (const char* p : {"benchmark_results.csv", "out.d/run", "run", "a/b.c/d.csv", ".hidden", "dir/.hidden"})
         std::printf("%s -> %s\n", p, gi::TestSuite::deriveFilename(p, "_x").c_str());
     return 0;

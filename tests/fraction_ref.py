@@ -56,6 +56,23 @@ def _dedupe(pts):
     return out
 
 
+def orient3d(a, b, c, d):
+    """Exact sign of det[a - d; b - d; c - d] (the orient3d convention of the
+    device predicates and the oracle), from the doubles as exact rationals."""
+    a, b, c, d = _F(a), _F(b), _F(c), _F(d)
+    v = _dot(_sub(a, d), _cross(_sub(b, d), _sub(c, d)))
+    return (v > 0) - (v < 0)
+
+
+def orient2d(a, b, c, drop):
+    """Exact sign of (a_u - c_u)(b_v - c_v) - (a_v - c_v)(b_u - c_u) with
+    (u, v) = ((drop + 1) % 3, (drop + 2) % 3)."""
+    u, v = (drop + 1) % 3, (drop + 2) % 3
+    a, b, c = _F(a), _F(b), _F(c)
+    x = (a[u] - c[u]) * (b[v] - c[v]) - (a[v] - c[v]) * (b[u] - c[u])
+    return (x > 0) - (x < 0)
+
+
 def _shape(tri):
     """Return ('tri', pts) / ('seg', (e0, e1)) / ('pt', (p,))."""
     p, q, r = tri

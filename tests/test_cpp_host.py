@@ -91,6 +91,10 @@ def test_suite_csv_files_and_names(gi, tmp_path):
     names = dict(line.split(" -> ") for line in r.stdout.splitlines())
     assert names["benchmark_results.csv"] == "benchmark_results_x.csv"
     assert names["out.d/run"] == "out.d/run_x.csv" and names["a/b.c/d.csv"] == "a/b.c/d_x.csv"
+    # runIntersectionPipeline's predicate mode: the reference's modes 0-4 select the
+    # FP32 cascade, 5 the plain FP64 form, anything else is an invalid argument
+    assert [names["mode %d" % m] for m in range(0, 6)] == ["0", "0", "0", "0", "0", "1"]
+    assert names["mode -1"] == "error 1" and names["mode 6"] == "error 1"
     summary = open(tmp_path / "sweep.csv").read().splitlines()
     assert summary[0] == SUMMARY_HEADER
     assert summary[1] == "0,768,12345,409010176,3.018262313e-05,0.0123456789,0.3333333333,12.5,333.3333333,0,1,1,0"

@@ -169,11 +169,12 @@ def test_ordering_paths_and_redo(gi, oc):
         B.release()
 
 
-@pytest.mark.parametrize("shape", [0, 1, 2, 3])
+@pytest.mark.parametrize("shape", list(range(8)))
 def test_every_traversal_shape(gi, oc, shape):
-    """Each traversal shape the autotuner may pick (expansion per lane or per
-    quad, all resident blocks or one per SM) gives the oracle's pairs and
-    segments, in both precision forms and in a batch."""
+    """Each traversal shape the autotuner may pick (work queue or level-synchronous
+    with grid barriers, expansion per lane or per quad, all resident blocks or
+    one per SM) gives the oracle's pairs and segments, in both precision forms
+    and in a batch."""
     from gpuintersector import meshgen as mg
 
     flags = gi._abi.GI_FLAG_FIXED_SHAPE | gi._abi.GI_FLAG_SHAPE(shape)
@@ -275,6 +276,69 @@ def test_batch_equals_individual(ctx, gi, oc):
         assert_same(single, ref)
     for m in meshes:
         m.release()
+
+
+def test_config4_full_batch_sampled_vs_oracle(ctx, gi, oc):
+    """The full batched configuration (4,096 mesh pairs of displaced geodesic
+    spheres, 1k-200k triangles per mesh, B offset by 0.2-1.5 radius and rotated)
+    in one gi_intersect_batch call; 64 jobs spread evenly over the size range
+    are compared with the oracle (pair sets and endpoints), as the reference's
+    suite compares every step with its ground truth (src/CPU/TestSuite.cpp:235-321)."""
+    from types import SimpleNamespace
+
+    from gpuintersector import meshgen as mg
+
+    sizes = np.array([a + b for a, b in mg.config4_sizes(seed=4)])
+    order = np.argsort(sizes, kind="stable")
+    pick = set(order[np.linspace(0, len(sizes) - 1, 64).astype(int)].tolist())
+    meshes, jobs, kept = [], [], {}
+    for p, j in enumerate(mg.config4_iter(seed=4)):
+        A, B = ctx.upload(j["vA"], j["tA"]), ctx.upload(j["vB"], j["tB"])
+        meshes += [A, B]
+        jobs.append((A, None, B, gi_pose(gi, j["poseB"])))
+        if p in pick:
+            kept[p] = j
+    assert len(jobs) == 4096 and len(kept) == 64
+    flat = ctx.intersect_batch_flat(jobs, want_segments=True)
+    assert flat.stats["pairs"] > 1_000_000
+    nonempty = 0
+    for p in sorted(kept):
+        j = kept[p]
+        ref = oc.intersect_meshes(j["vA"], j["tA"], oc.pose_identity(), j["vB"], j["tB"],
+                                  oracle_pose(oc, j["poseB"]), want_segments=True)
+        a, e = flat.offsets[p], flat.offsets[p + 1]
+        sel = (flat.seg_pair >= a) & (flat.seg_pair < e)
+        got = SimpleNamespace(pairs=flat.pairs[a:e], segments=flat.segments[sel], seg_pair=flat.seg_pair[sel] - a)
+        assert_same(got, ref)
+        nonempty += len(ref["pairs"]) > 0
+    assert nonempty >= 32
+    del flat
+    for m in meshes:
+        m.release()
+
+
+def test_classify_pairs_after_wait_stream(ctx, gi, oc):
+    """Inputs produced on a side stream of the caller reach gi_classify_pairs
+    through gi_wait_stream (the library's stream waits for the caller's work)."""
+    import torch
+    from gpuintersector import meshgen as mg
+
+    cfg = mg.config1(seed=12)
+    rng = np.random.default_rng(4)
+    pairs, _ = _candidate_pairs(cfg, oc, rng, n_random=20000)
+    exp = oc.classify_pairs(cfg["vA"], cfg["tA"], oc.pose_identity(), cfg["vB"], cfg["tB"],
+                            oracle_pose(oc, cfg["poseB"]), pairs)
+    A, B = ctx.upload(cfg["vA"], cfg["tA"]), ctx.upload(cfg["vB"], cfg["tB"])
+    side = torch.cuda.Stream()
+    host = torch.from_numpy(pairs).pin_memory()
+    with torch.cuda.stream(side):
+        d_pairs = host.to("cuda", non_blocking=True)
+        d_out = torch.full((len(pairs),), 7, dtype=torch.uint8, device="cuda")
+    ctx.wait_stream(side.cuda_stream)
+    ctx.classify_pairs(A, B, None, gi_pose(gi, cfg["poseB"]), d_pairs.data_ptr(), len(pairs), d_out.data_ptr())
+    assert np.array_equal(d_out.cpu().numpy(), exp)
+    A.release()
+    B.release()
 
 
 def test_batch_flat_matches_per_job_results(ctx, gi):
@@ -401,10 +465,14 @@ def test_capacity_retry_path(gi, oc):
     from gpuintersector import meshgen as mg
 
     cfg = mg.config1(seed=4)
-    with gi.Context(0, flags=gi._abi.GI_FLAG_TINY_BUFFERS) as c:
-        r, ref = run_cfg(c, gi, oc, cfg)
-    assert r.stats["retries"] > 0
-    assert_same(r, ref)
+    for shape in (None, 1, 5):  # tuned, the work-queue traversal, the level-synchronous one
+        flags = gi._abi.GI_FLAG_TINY_BUFFERS
+        if shape is not None:
+            flags |= gi._abi.GI_FLAG_FIXED_SHAPE | gi._abi.GI_FLAG_SHAPE(shape)
+        with gi.Context(0, flags=flags) as c:
+            r, ref = run_cfg(c, gi, oc, cfg)
+        assert r.stats["retries"] > 0
+        assert_same(r, ref)
 
 
 def test_hbm_budget_admission(gi):
@@ -465,6 +533,7 @@ def test_classify_pairs_vs_oracle(ctx, gi, oc):
     d_pairs = torch.from_numpy(pairs).cuda()
     for prec in (0, 1):
         d_out = torch.full((len(pairs),), 7, dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()  # the library's stream is not ordered after torch's
         ctx.classify_pairs(A, B, None, gi_pose(gi, cfg["poseB"]), d_pairs.data_ptr(), len(pairs), d_out.data_ptr(),
                            precision=prec)
         torch.cuda.synchronize()
@@ -472,6 +541,7 @@ def test_classify_pairs_vs_oracle(ctx, gi, oc):
     assert exp[:len(ref["pairs"])].all()
     bad = torch.tensor([[0, cfg["tB"].shape[0]]], dtype=torch.int32, device="cuda")
     out = torch.zeros(1, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
     with pytest.raises(gi.GIError) as e:
         ctx.classify_pairs(A, B, None, None, bad.data_ptr(), 1, out.data_ptr())
     assert e.value.status == 1

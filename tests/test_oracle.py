@@ -168,3 +168,28 @@ def test_oracle_classify_pairs_list(oc):
     assert int(out.sum()) == sum(1 for p in map(tuple, pairs.tolist()) if p in hit_set)
     with pytest.raises(ValueError):
         oc.classify_pairs(cfg["vA"], cfg["tA"], oc.pose_identity(), cfg["vB"], cfg["tB"], pB, np.array([[0, nt]]))
+
+
+def test_oracle_signs_vs_fractions_per_call(oc):
+    """Every orient3d / orient2d call the oracle's decision procedure makes on the
+    frozen and fresh near-degenerate pairs (its sign log), and its signs on
+    exactly degenerate point sets with exponent spans beyond 2^40 / 2^60 and
+    their one-unit perturbations, equal the exact rational signs.  These are the
+    signs the device sign test (test_gpu_signs.py) is held to."""
+    import sign_families as sf
+
+    for tris in (sf.frozen_pairs(GOLDEN), sf.fresh_pairs(21)):
+        (pts, kind, drop, sign), _ = oc.record_signs(lambda: [oc.tri_tri_construct(a, b) for a, b in tris])
+        assert len(sign) > 2000 and np.count_nonzero(sign == 0) > 100
+        for k in (sf.O3, sf.O2):
+            sel = kind == k
+            assert np.array_equal(sf.exact_signs(pts[sel], k, drop[sel]), sign[sel])
+    rng = random.Random(44)
+    p3 = sf.wide_span_o3(rng, 100)
+    assert np.all(sf.expected_branch(p3, sf.O3) == 1)
+    got = np.array([oc.orient3d(r[0:3], r[3:6], r[6:9], r[9:12]) for r in p3])
+    assert np.array_equal(got, sf.exact_signs(p3, sf.O3, None))
+    p2, d2 = sf.wide_span_o2(rng, 100)
+    assert np.all(sf.expected_branch(p2, sf.O2, d2) == 1)
+    got = np.array([oc.orient2d(r[0:3], r[3:6], r[6:9], int(d)) for r, d in zip(p2, d2)])
+    assert np.array_equal(got, sf.exact_signs(p2, sf.O2, d2))
