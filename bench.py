@@ -60,6 +60,9 @@ def parse():
                          "mesh pairs of uneven size in one call; serving: resident pairs under an HBM "
                          "budget with a Poisson pose stream")
     ap.add_argument("--pairs", type=int, default=0, help="batch: 4096 pairs; serving: 64 pairs (default)")
+    ap.add_argument("--classify-config", type=int, default=2, choices=[2, 3],
+                    help="classify: the displaced icospheres (2) or the coplanar integer grids (3), whose "
+                         "candidate pairs escalate to the exact stage")
     ap.add_argument("--rate", type=float, default=2000.0, help="serving: mean requests per second")
     ap.add_argument("--duration", type=float, default=3.0, help="serving: seconds of offered load")
     ap.add_argument("--pose-samples", type=int, default=1000,
@@ -420,13 +423,19 @@ def run_classify(args, gi, world, rank):
     from gpuintersector import meshgen as mg
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    cfg = mg.config2(level=args.level)
+    cfg = mg.config2(level=args.level) if args.classify_config == 2 else mg.config3()
     local = int(os.environ.get("LOCAL_RANK", "0"))
     ctx = gi.Context(local)
     A, B = ctx.upload(cfg["vA"], cfg["tA"]), ctx.upload(cfg["vB"], cfg["tB"])
-    R, C, T = cfg["poseB"]
-    pose = gi.pose_raw(R, C, T)
+    if cfg["poseB"] is not None:
+        R, C, T = cfg["poseB"]
+        pose = gi.pose_raw(R, C, T)
+    else:
+        R, C, T = np.eye(3), np.zeros(3), np.zeros(3)
+        pose = None
     hits = ctx.intersect(A, B, None, pose, want_segments=False).pairs
+    if args.classify_config == 3:  # 1.33 M intersecting pairs: a sample of them keeps the list near 1 M
+        hits = hits[np.random.default_rng(3).choice(len(hits), 11000, replace=False)]
     nt = int(cfg["tB"].shape[0])
     d = np.arange(-48, 48)
     pairs = np.stack([np.repeat(hits[:, 0], d.size), (np.repeat(hits[:, 1], d.size) + np.tile(d, len(hits))) % nt], 1)
@@ -451,7 +460,7 @@ def run_classify(args, gi, world, rank):
     # CPU baseline: the exact oracle over the same list on all host threads
     import oracle as oc
 
-    pA, pB = oc.pose_identity(), oc.pose_raw(R, C, T)
+    pA, pB = oc.pose_identity(), (oc.pose_raw(R, C, T) if pose is not None else oc.pose_identity())
     reps, t0 = 0, time.perf_counter()
     while True:
         exp = oc.classify_pairs(cfg["vA"], cfg["tA"], pA, cfg["vB"], cfg["tB"], pB, pairs)
@@ -473,7 +482,8 @@ def run_classify(args, gi, world, rank):
         "value": n / (res["fp32_cascade"] * 1e-3), "unit": "pairs/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": res["fp32_cascade"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (config-2 icospheres; intersecting pairs and their B-index neighbours)",
+        "data": "synthetic (%s; intersecting pairs and their B-index neighbours)" % (
+            "config-2 icospheres" if args.classify_config == 2 else "config-3 coplanar integer grids"),
         "config": {"workload": "%d candidate pairs, 2 x %d triangles" % (n, nt), "intersecting": int(out.sum()),
                    "l2": "flushed (256 MB write) before each step", "timing": "host wall of the blocking call"},
         "fp64_form_ms": res["fp64"],

@@ -176,11 +176,10 @@ __device__ __forceinline__ uint32_t spread10(uint32_t x)
     return x;
 }
 
-__global__ void k_morton(const float* __restrict__ box, uint32_t nt, const unsigned* __restrict__ cb,
-                         uint32_t* __restrict__ keys, uint32_t* __restrict__ vals)
+// 30-bit Morton key of triangle t: its box centre quantised to 10 bits per
+// axis over the centroid bounds cb (ordered-float min x, y, z, max x, y, z)
+__device__ __forceinline__ uint32_t morton_key(const float* __restrict__ box, uint32_t t, const unsigned* __restrict__ cb)
 {
-    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nt) return;
     uint32_t q[3];
     for (int k = 0; k < 3; k++) {
         float lo = ord2f(cb[k]), hi = ord2f(cb[3 + k]);
@@ -190,8 +189,38 @@ __global__ void k_morton(const float* __restrict__ box, uint32_t nt, const unsig
         f = fminf(fmaxf(f, 0.0f), 1.0f);
         q[k] = (uint32_t)fminf(f * 1024.0f, 1023.0f);
     }
-    keys[t] = (spread10(q[0]) << 2) | (spread10(q[1]) << 1) | spread10(q[2]);
+    return (spread10(q[0]) << 2) | (spread10(q[1]) << 1) | spread10(q[2]);
+}
+
+__global__ void k_morton(const float* __restrict__ box, uint32_t nt, const unsigned* __restrict__ cb,
+                         uint32_t* __restrict__ keys, uint32_t* __restrict__ vals)
+{
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    keys[t] = morton_key(box, t, cb);
     vals[t] = t;
+}
+
+// Morton keys and identity values, plus the 10-bit digit histograms of the
+// three one-sweep sort passes from the same read (block counts in shared
+// memory, one set of atomics per block; the last block scans them).
+__global__ void __launch_bounds__(kMsThreads) k_morton_hist(const float* __restrict__ box, uint32_t nt,
+                                                            const unsigned* __restrict__ cb, uint32_t* __restrict__ keys,
+                                                            uint32_t* __restrict__ vals, MsScratch S)
+{
+    __shared__ uint32_t h[kMsPasses][kMsDig];
+    for (uint32_t d = threadIdx.x; d < kMsDig; d += blockDim.x)
+#pragma unroll
+        for (int p = 0; p < kMsPasses; p++) h[p][d] = 0u;
+    __syncthreads();
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+        const uint32_t key = morton_key(box, t, cb);
+        keys[t] = key;
+        vals[t] = t;
+#pragma unroll
+        for (int p = 0; p < kMsPasses; p++) atomicAdd(&h[p][(key >> (kMsBits * p)) & (kMsDig - 1u)], 1u);
+    }
+    ms_hist_finish(h, S);
 }
 
 __device__ __forceinline__ int kdelta(const uint32_t* __restrict__ keys, int n, int i, int j)
@@ -610,8 +639,11 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t 
     uint32_t *wide = nullptr, *widx = nullptr;
     uint8_t* tab = nullptr;
     constexpr int kMortonDigit = 10;  // 30-bit keys: three passes
-    size_t cw = radix_counts_words<kMortonDigit>(n);
-    size_t sw = scan_temp_words(cw > n ? cw : n);
+    // one-sweep sort up to 2^30 keys (look-back counts have 30 bits), else
+    // histogram + scan + scatter per pass
+    const bool onesweep = n >= 2 && n < (1u << 30);
+    size_t cw = onesweep ? ms_scratch_words(n) : radix_counts_words<kMortonDigit>(n);
+    size_t sw = scan_temp_words(onesweep ? n : (cw > n ? cw : n));
     GI_TRY(pool_alloc(&box, sizeof(float) * 6 * n, pool, st));
     if (fp64) GI_TRY(pool_alloc(&box64, sizeof(double) * 6 * n, pool, st));
     GI_TRY(pool_alloc(&cb, sizeof(unsigned) * 8, pool, st));
@@ -628,8 +660,17 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t 
     // four resident blocks per SM, each looping: the centroid bounds take one set of atomics per block
     const int gboxes = (int)((n + 2 * kTriBoxThreads - 1) / (2 * kTriBoxThreads));
     k_tri_boxes<<<gboxes < 592 ? gboxes : 592, kTriBoxThreads, 0, st>>>(m.verts, m.nv, m.tris, n, box, box64, cb);
-    k_morton<<<gb, tb, 0, st>>>(box, n, cb, k0, v0);
-    radix_sort<uint32_t, kMortonDigit>(k0, v0, k1, v1, n, 30, counts, stemp, st);
+    if (onesweep) {
+        const MsScratch S = ms_scratch(counts);
+        GI_TRY(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * cw, st));
+        const int gm = (int)((n + kMsThreads - 1) / kMsThreads);
+        k_morton_hist<<<gm < 296 ? gm : 296, kMsThreads, 0, st>>>(box, n, cb, k0, v0, S);
+        note_launches(1);
+        ms_sort_passes(k0, v0, k1, v1, n, S, d_err, st);
+    } else {
+        k_morton<<<gb, tb, 0, st>>>(box, n, cb, k0, v0);
+        radix_sort<uint32_t, kMortonDigit>(k0, v0, k1, v1, n, 30, counts, stemp, st);
+    }
     if (n > 1) {
         GI_TRY(pool_alloc(&child, sizeof(uint4) * (n - 1), pool, st));
         GI_TRY(pool_alloc(&parent, sizeof(int) * (n - 1), pool, st));
@@ -1023,10 +1064,6 @@ __device__ __forceinline__ unsigned rows4(unsigned x)
            ((x & 8u) ? 0xF000u : 0u);
 }
 
-__device__ __forceinline__ uint32_t sel4(const uint32_t (&a)[4], unsigned k)
-{
-    return k == 0u ? a[0] : k == 1u ? a[1] : k == 2u ? a[2] : a[3];
-}
 
 // One node pair: load both nodes, map the child boxes to the world frame and
 // test the 4 x 4 child pairs without branches.  fm / cm: bit 4i+j set when
@@ -1487,10 +1524,15 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
             const unsigned f0 = incf - nf;  // this lane's first node child in the warp's order
             const unsigned c0 = cg + incc - nc;  // this lane's first candidate slot
             {
+                // child slot q: the pair (A child q / 4, B child q % 4) in the lane
+                // form, (own A child, B child q) in the quad form; the unrolled
+                // loop indexes the registers with constants and has no
+                // data-dependent trip count
+                constexpr int kQ = QUAD ? 4 : 16;
                 unsigned g = f0, h = c0;
-                for (unsigned mm = fm | cm; mm != 0u; mm &= mm - 1u) {
-                    const unsigned q = (unsigned)__ffs(mm) - 1u;
-                    const uint32_t ra = QUAD ? ca[0] : sel4(ca, q >> 2), rb = sel4(cb, QUAD ? q : (q & 3u));
+#pragma unroll
+                for (int q = 0; q < kQ; q++) {
+                    const uint32_t ra = QUAD ? ca[0] : ca[q >> 2], rb = QUAD ? cb[q] : cb[q & 3];
                     if ((fm >> q) & 1u) {
                         const uint4 e = make_uint4(ent.x, ra, rb, ent.w + 1u);
                         if (g < keep) {
@@ -1500,7 +1542,8 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
                             if (sl < B.cap_queue) B.queue[sl] = e;
                         }
                         g++;
-                    } else {
+                    }
+                    if ((cm >> q) & 1u) {
                         if (h < B.cap_cand) B.cand[h] = make_uint4(ent.x, ra & ~kLeaf, rb & ~kLeaf, 0u);
                         h++;
                     }
@@ -1993,8 +2036,6 @@ constexpr int kOsItems = 16;
 constexpr int kOsTile = kOsThreads * kOsItems;
 constexpr int kOsWarps = kOsThreads / 32;
 constexpr int kOsGatherTile = 1024;
-constexpr unsigned kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kCountMask = (1u << 30) - 1u;
-constexpr unsigned long long kLookbackSpins = 1ull << 22;
 
 __device__ __forceinline__ unsigned res_count(const Bufs& B)
 {
@@ -2053,40 +2094,6 @@ __global__ void __launch_bounds__(kOsThreads) k_os_hist(Bufs B, OrderBufs O)
         O.hist[p * 256 + threadIdx.x] = 0u;
     }
     if (threadIdx.x == 0) O.tile_ctr[kOsMaxPasses + 1] = 0u;
-}
-
-// Exclusive prefix of this tile over the preceding tiles, per status slot.
-// Returns false if a wait ran out (the error bit is set; results are invalid).
-__device__ __forceinline__ bool lookback(unsigned* status, unsigned tile, unsigned stride, unsigned own,
-                                         unsigned* excl_out, unsigned* err)
-{
-    unsigned excl = 0;
-    if (tile > 0) {
-        // publish the local aggregate first so successors need not wait for our prefix
-        atomicExch(status + (size_t)tile * stride, kFlagAgg | (own & kCountMask));
-        unsigned t = tile - 1;
-        for (;;) {
-            volatile unsigned* q = status + (size_t)t * stride;
-            unsigned v = *q;
-            unsigned long long spins = 0;
-            while ((v & ~kCountMask) == 0u) {
-                if (++spins > kLookbackSpins) {
-                    atomicOr(err, kErrTimeout);
-                    *excl_out = 0;
-                    return false;
-                }
-                __nanosleep(32);
-                v = *q;
-            }
-            excl += v & kCountMask;
-            if ((v & ~kCountMask) == kFlagInc || t == 0) break;
-            t--;
-        }
-    }
-    __threadfence();
-    atomicExch(status + (size_t)tile * stride, kFlagInc | ((excl + own) & kCountMask));
-    *excl_out = excl;
-    return true;
 }
 
 __global__ void __launch_bounds__(kOsThreads) k_os_scatter(Bufs B, OrderBufs O, int pass)
