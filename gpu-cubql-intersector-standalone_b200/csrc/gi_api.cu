@@ -215,7 +215,6 @@ static gi_status mesh_finish(gi_ctx* c, gi_mesh* m, gi_mesh** out, cudaStream_t 
         mesh_free(c, m, st);
         if (herr & 1u) return sk.fail(GI_ERR_INVALID_ARG, "triangle index out of range");
         if (herr & 2u) return sk.fail(GI_ERR_RANGE, "vertex coordinate outside the supported domain");
-        if (herr & kErrBuildTimeout) return sk.fail(GI_ERR_TIMEOUT, "BVH build: a bounded device wait ran out");
         return sk.fail(GI_ERR_CUDA, "BVH build: inconsistent wide-node collapse");
     }
     c->mesh_bytes += m->b.bytes;
@@ -567,7 +566,6 @@ static gi_status ensure_fp64(gi_ctx* c, gi_mesh* m)
     if (e == cudaSuccess) e = es;
     cudaFreeAsync(d_err, c->st);
     if (e != cudaSuccess) return set_err(c, GI_ERR_CUDA, "FP64 BVH build", e);
-    if (herr & kErrBuildTimeout) return set_err(c, GI_ERR_TIMEOUT, "FP64 BVH build: a bounded device wait ran out");
     if (herr) return set_err(c, GI_ERR_CUDA, "FP64 BVH build: inconsistent wide-node collapse");
     m->has64 = true;
     return GI_OK;

@@ -206,9 +206,12 @@ struct PinnedPool {
         }
         PinnedBuf* b = new (std::nothrow) PinnedBuf();
         if (!b) return nullptr;
-        // power-of-two sizes (at least 1 MB): a block serves later results of similar size
+        // power-of-two sizes (at least 1 MB) with at least half the request as
+        // headroom: a block serves later results of similar or somewhat larger
+        // size, so a result that grows a little does not pin a new block (pinning
+        // takes milliseconds) in the middle of a pose stream
         size_t want = (size_t)1 << 20;
-        while (want < bytes) want <<= 1;
+        while (want < bytes + bytes / 2) want <<= 1;
         if (cudaMallocHost(&b->p, want) != cudaSuccess) {
             delete b;
             return nullptr;

@@ -130,9 +130,6 @@ struct Counters {
 
 constexpr unsigned kOvfFrontier = 1u, kOvfCand = 2u, kOvfRes = 4u, kOvfEsc = 8u;
 constexpr unsigned kErrTimeout = 1u, kErrExactCapacity = 2u;
-// bits of a mesh build's error word: 1 bad index, 2 coordinate out of range,
-// 4 inconsistent wide tree (not expected), 8 a bounded wait of the sort ran out
-constexpr unsigned kErrBuildTimeout = 8u;
 
 // Per-call buffers handed to the kernels.
 struct Bufs {

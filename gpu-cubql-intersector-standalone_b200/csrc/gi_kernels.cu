@@ -201,28 +201,6 @@ __global__ void k_morton(const float* __restrict__ box, uint32_t nt, const unsig
     vals[t] = t;
 }
 
-// Morton keys and identity values, plus the 10-bit digit histograms of the
-// three one-sweep sort passes from the same read (block counts in shared
-// memory, one set of atomics per block; the last block scans them).
-__global__ void __launch_bounds__(kMsThreads) k_morton_hist(const float* __restrict__ box, uint32_t nt,
-                                                            const unsigned* __restrict__ cb, uint32_t* __restrict__ keys,
-                                                            uint32_t* __restrict__ vals, MsScratch S)
-{
-    __shared__ uint32_t h[kMsPasses][kMsDig];
-    for (uint32_t d = threadIdx.x; d < kMsDig; d += blockDim.x)
-#pragma unroll
-        for (int p = 0; p < kMsPasses; p++) h[p][d] = 0u;
-    __syncthreads();
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
-        const uint32_t key = morton_key(box, t, cb);
-        keys[t] = key;
-        vals[t] = t;
-#pragma unroll
-        for (int p = 0; p < kMsPasses; p++) atomicAdd(&h[p][(key >> (kMsBits * p)) & (kMsDig - 1u)], 1u);
-    }
-    ms_hist_finish(h, S);
-}
-
 __device__ __forceinline__ int kdelta(const uint32_t* __restrict__ keys, int n, int i, int j)
 {
     if (j < 0 || j >= n) return -1;
@@ -639,11 +617,8 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t 
     uint32_t *wide = nullptr, *widx = nullptr;
     uint8_t* tab = nullptr;
     constexpr int kMortonDigit = 10;  // 30-bit keys: three passes
-    // one-sweep sort up to 2^30 keys (look-back counts have 30 bits), else
-    // histogram + scan + scatter per pass
-    const bool onesweep = n >= 2 && n < (1u << 30);
-    size_t cw = onesweep ? ms_scratch_words(n) : radix_counts_words<kMortonDigit>(n);
-    size_t sw = scan_temp_words(onesweep ? n : (cw > n ? cw : n));
+    size_t cw = radix_counts_words<kMortonDigit>(n);
+    size_t sw = scan_temp_words(cw > n ? cw : n);
     GI_TRY(pool_alloc(&box, sizeof(float) * 6 * n, pool, st));
     if (fp64) GI_TRY(pool_alloc(&box64, sizeof(double) * 6 * n, pool, st));
     GI_TRY(pool_alloc(&cb, sizeof(unsigned) * 8, pool, st));
@@ -660,17 +635,8 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t 
     // four resident blocks per SM, each looping: the centroid bounds take one set of atomics per block
     const int gboxes = (int)((n + 2 * kTriBoxThreads - 1) / (2 * kTriBoxThreads));
     k_tri_boxes<<<gboxes < 592 ? gboxes : 592, kTriBoxThreads, 0, st>>>(m.verts, m.nv, m.tris, n, box, box64, cb);
-    if (onesweep) {
-        const MsScratch S = ms_scratch(counts);
-        GI_TRY(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * cw, st));
-        const int gm = (int)((n + kMsThreads - 1) / kMsThreads);
-        k_morton_hist<<<gm < 296 ? gm : 296, kMsThreads, 0, st>>>(box, n, cb, k0, v0, S);
-        note_launches(1);
-        ms_sort_passes(k0, v0, k1, v1, n, S, d_err, st);
-    } else {
-        k_morton<<<gb, tb, 0, st>>>(box, n, cb, k0, v0);
-        radix_sort<uint32_t, kMortonDigit>(k0, v0, k1, v1, n, 30, counts, stemp, st);
-    }
+    k_morton<<<gb, tb, 0, st>>>(box, n, cb, k0, v0);
+    radix_sort<uint32_t, kMortonDigit>(k0, v0, k1, v1, n, 30, counts, stemp, st);
     if (n > 1) {
         GI_TRY(pool_alloc(&child, sizeof(uint4) * (n - 1), pool, st));
         GI_TRY(pool_alloc(&parent, sizeof(int) * (n - 1), pool, st));

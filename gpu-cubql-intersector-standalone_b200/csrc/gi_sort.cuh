@@ -133,7 +133,7 @@ constexpr unsigned long long kLookbackSpins = 1ull << 22;
 // Exclusive prefix of this tile over the preceding tiles, per status slot.
 // Returns false if a wait ran out (the error bit is set; results are invalid).
 __device__ __forceinline__ bool lookback(unsigned* status, unsigned tile, unsigned stride, unsigned own,
-                                         unsigned* excl_out, unsigned* err, unsigned err_bit = kErrTimeout)
+                                         unsigned* excl_out, unsigned* err)
 {
     unsigned excl = 0;
     if (tile > 0) {
@@ -146,7 +146,7 @@ __device__ __forceinline__ bool lookback(unsigned* status, unsigned tile, unsign
             unsigned long long spins = 0;
             while ((v & ~kCountMask) == 0u) {
                 if (++spins > kLookbackSpins) {
-                    atomicOr(err, err_bit);
+                    atomicOr(err, kErrTimeout);
                     *excl_out = 0;
                     return false;
                 }
@@ -283,165 +283,6 @@ void radix_sort(K*& k0, uint32_t*& v0, K*& k1, uint32_t*& v1, uint32_t n, int bi
     v1 = vd;
     k0 = ks;
     v0 = vs;
-}
-
-// ---------------------------------------------------------------------------
-// One-sweep LSD radix sort of 32-bit keys with 32-bit values in 10-bit digits
-// (the BVH build's 30-bit Morton keys: three passes).  The digit histograms of
-// every pass come from the kernel that makes the keys (one read, scanned by
-// its last block into digit bases); each pass is then one scatter launch
-// whose tiles take a ticket in launch order, rank their keys per warp and find
-// their global offset per digit by decoupled look-back over the preceding
-// tiles.  Four launches in all, where a histogram, a scan and a scatter per
-// pass took twelve and more.
-// ---------------------------------------------------------------------------
-constexpr int kMsBits = 10;
-constexpr uint32_t kMsDig = 1u << kMsBits;
-constexpr int kMsPasses = 3;
-constexpr int kMsThreads = 256;
-constexpr int kMsItems = 16;
-constexpr uint32_t kMsTile = kMsThreads * kMsItems;
-constexpr int kMsWarps = kMsThreads / 32;
-
-// Scratch of the one-sweep sort, zeroed before the key kernel runs.
-struct MsScratch {
-    uint32_t* hist;      // kMsPasses x kMsDig digit counts
-    uint32_t* base;      // kMsPasses x kMsDig exclusive digit bases
-    uint32_t* ctr;       // [0, kMsPasses): tile tickets per pass; [kMsPasses]: finished key blocks
-    uint32_t* status;    // kMsPasses x ntiles x kMsDig look-back words
-};
-__host__ __device__ inline uint32_t ms_tiles(uint32_t n)
-{
-    return (n + kMsTile - 1) / kMsTile;
-}
-inline size_t ms_scratch_words(uint32_t n)
-{
-    return 2 * (size_t)kMsPasses * kMsDig + 8 + (size_t)kMsPasses * ms_tiles(n) * kMsDig;
-}
-inline MsScratch ms_scratch(uint32_t* w)
-{
-    MsScratch s;
-    s.hist = w;
-    s.base = w + kMsPasses * kMsDig;
-    s.ctr = w + 2 * kMsPasses * kMsDig;
-    s.status = w + 2 * kMsPasses * kMsDig + 8;
-    return s;
-}
-
-// Adds a block's digit counts (shared) into the global histograms; the last
-// block to finish turns the histograms into exclusive digit bases.
-__device__ __forceinline__ void ms_hist_finish(uint32_t (*h)[kMsDig], const MsScratch& S)
-{
-    __shared__ uint32_t sw[33];
-    __shared__ unsigned s_last;
-    __syncthreads();
-    for (uint32_t d = threadIdx.x; d < kMsDig; d += blockDim.x)
-#pragma unroll
-        for (int p = 0; p < kMsPasses; p++)
-            if (h[p][d]) atomicAdd(&S.hist[p * kMsDig + d], h[p][d]);
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) s_last = atomicAdd(&S.ctr[kMsPasses], 1u) == gridDim.x - 1 ? 1u : 0u;
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    // blockDim.x = 256 threads, 4 consecutive digits each
-    for (int p = 0; p < kMsPasses; p++) {
-        uint32_t v[4], sum = 0;
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            v[k] = __ldcg(&S.hist[p * kMsDig + 4 * threadIdx.x + k]);
-            sum += v[k];
-        }
-        uint32_t tot;
-        uint32_t ex = block_exclusive_scan(sum, sw, &tot);
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            S.base[p * kMsDig + 4 * threadIdx.x + k] = ex;
-            ex += v[k];
-        }
-    }
-}
-
-__global__ void __launch_bounds__(kMsThreads) k_ms_scatter(const uint32_t* __restrict__ kin,
-                                                           const uint32_t* __restrict__ vin,
-                                                           uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
-                                                           uint32_t n, int pass, MsScratch S, unsigned* err)
-{
-    __shared__ uint32_t wc[kMsWarps][kMsDig];
-    __shared__ uint32_t tile_base[kMsDig];
-    __shared__ uint32_t s_tile;
-    if (threadIdx.x == 0) s_tile = atomicAdd(&S.ctr[pass], 1u);
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (uint32_t d = lane; d < kMsDig; d += 32) wc[w][d] = 0u;
-    __syncthreads();
-    const uint32_t tile = s_tile, ntiles = ms_tiles(n);
-    if (tile >= ntiles) return;
-    const int shift = kMsBits * pass;
-    const uint32_t seg = tile * kMsTile + w * 32 * kMsItems;
-    uint32_t key[kMsItems], val[kMsItems], rank[kMsItems], dig[kMsItems];
-    const unsigned lt = (1u << lane) - 1u;
-#pragma unroll
-    for (int c = 0; c < kMsItems; c++) {
-        const uint32_t i = seg + c * 32 + lane;
-        key[c] = i < n ? __ldcg(kin + i) : 0u;
-        val[c] = i < n ? __ldcg(vin + i) : 0u;
-    }
-#pragma unroll
-    for (int c = 0; c < kMsItems; c++) {
-        const uint32_t i = seg + c * 32 + lane;
-        const bool ok = i < n;
-        const uint32_t d = ok ? ((key[c] >> shift) & (kMsDig - 1u)) : kMsDig;
-        dig[c] = d;
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
-        rank[c] = ok ? wc[w][d] + __popc(peers & lt) : 0u;
-        __syncwarp();
-        if (ok && (peers & lt) == 0) wc[w][d] += __popc(peers);
-        __syncwarp();
-    }
-    __syncthreads();
-    uint32_t* st = S.status + (size_t)pass * ntiles * kMsDig;
-    for (uint32_t d = threadIdx.x; d < kMsDig; d += kMsThreads) {
-        uint32_t run = 0;
-#pragma unroll
-        for (int q = 0; q < kMsWarps; q++) {
-            const uint32_t t = wc[q][d];
-            wc[q][d] = run;
-            run += t;
-        }
-        unsigned excl = 0;
-        lookback(st + d, tile, kMsDig, run, &excl, err, kErrBuildTimeout);
-        tile_base[d] = S.base[pass * kMsDig + d] + excl;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int c = 0; c < kMsItems; c++) {
-        const uint32_t d = dig[c];
-        if (d < kMsDig) {
-            const uint32_t pos = tile_base[d] + wc[w][d] + rank[c];
-            kout[pos] = key[c];
-            vout[pos] = val[c];
-        }
-    }
-}
-
-// The scatter passes of the one-sweep sort (the key kernel has filled the keys,
-// the values and the digit bases).  Same buffer convention as radix_sort: on
-// return (k0, v0) hold the result.
-inline void ms_sort_passes(uint32_t*& k0, uint32_t*& v0, uint32_t*& k1, uint32_t*& v1, uint32_t n,
-                           const MsScratch& S, unsigned* err, cudaStream_t st)
-{
-    const uint32_t ntiles = ms_tiles(n);
-    for (int p = 0; p < kMsPasses; p++) {
-        k_ms_scatter<<<ntiles, kMsThreads, 0, st>>>(k0, v0, k1, v1, n, p, S, err);
-        note_launches(1);
-        uint32_t* t = k0;
-        k0 = k1;
-        k1 = t;
-        t = v0;
-        v0 = v1;
-        v1 = t;
-    }
 }
 
 template <int BITS = 8>
