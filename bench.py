@@ -41,9 +41,10 @@ PKG = os.path.join(ROOT, "gpu-cubql-intersector-standalone_b200")
 sys.path.insert(0, PKG)
 
 METRIC = "ms/intersect at 2×1.3M tris & tri-pair tests/s; pose-update p50/p99 vs FP64 path"
-# DRAM bytes of one k_traverse launch on the level-8 pose workload, from an ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum = 17.08 MB + 0.87 MB)
-TRAVERSE_DRAM_BYTES = 17.94e6
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one traversal
+# launch on the level-8 pose workload with L2 flushed, from the ncu captures
+# summarised in profiles/k_traverse_config2.md, per traversal shape captured
+TRAVERSE_DRAM_BYTES = {0: 19.51e6 + 4.05e6, 6: 19.46e6 + 4.23e6}
 
 
 def parse():
@@ -678,7 +679,6 @@ def main():
     t2 = time.perf_counter()
     er = ctx.intersect(eA, eB, None, gi.pose_raw(R, C, T), want_segments=True)
     t3 = time.perf_counter()
-    e2e_build_ms = [eA.info()["build_ms"], eB.info()["build_ms"]]
     eA.release()
     eB.release()
     t4 = time.perf_counter()
@@ -697,7 +697,13 @@ def main():
     # of the build kernels (gi_mesh_build_ms), averaged over the builds above
     T, V = int(cfg["tA"].shape[0]), int(cfg["vA"].shape[0])
     build_bytes = 24 * V + 12 * T + 64 * T + 32 * (2 * T - 1) + 4 * T + 32 * (2 * T - 1)
-    build_ms = [m.info()["build_ms"] for m in (A, B)] + e2e_build_ms
+    # warm builds only (the first launches of a process also load the kernels)
+    build_ms = []
+    for k in range(5):
+        wm = ctx.upload(hvA, htA)
+        build_ms.append(wm.info()["build_ms"])
+        wm.release()
+    build_ms = build_ms[1:]
     # curve assembly (downstream of the path) on the last step's result
     t0 = time.perf_counter()
     cv_verts, cv = r.curves()
@@ -746,9 +752,9 @@ def main():
                 "samples_ms": [round(x, 3) for x in e2e_ms], "split": e2e_split},
         "gpu_launches": int(np.sum([s["launches"] for s in stats])),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": TRAVERSE_DRAM_BYTES if args.level == 8 else None,
-                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of "
-                                       "k_traverse on this workload (shape 1)",
+                     "traffic": TRAVERSE_DRAM_BYTES.get(int(st["traverse_shape"])) if args.level == 8 else None,
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the "
+                                       "traversal on this workload with the same shape (null: shape not captured)",
                      "kernel": "k_traverse", "peak_source": peak_src,
                      "alg_bytes_per_launch": float(alg_bytes),
                      "note": "output-sensitive traversal: bytes = node pairs x 2 nodes x 128 B + leaf pairs x "
@@ -756,6 +762,8 @@ def main():
         "build_roofline": {"bound": "hbm", "achieved": build_bytes / (np.mean(build_ms) * 1e-3) / 1e9, "peak": peak,
                            "unit": "GB/s", "frac": build_bytes / (np.mean(build_ms) * 1e-3) / 1e9 / peak,
                            "build_ms": float(np.mean(build_ms)), "builds": len(build_ms),
+                           "what": "mean of 4 warm builds of mesh A from pinned host arrays (gi_mesh_build_ms: "
+                                   "CUDA events around validation + build, the mid-build host round trip included)",
                            "alg_bytes_per_mesh": build_bytes, "peak_source": peak_src,
                            "note": "24V + 12T (mesh) + 64T (32-bit key sort) + 32(2T-1) + 4T (nodes, ids) + "
                                    "32(2T-1) (refit read) over the device time of validation + build kernels"},

@@ -123,7 +123,11 @@ struct Counters {
     unsigned pad8[31];
     unsigned bar_gen;    // grid barrier: barriers completed
     unsigned bstop;      // decision of the last completed barrier: 1 = the traversal is over
-    unsigned pad9[30];
+    unsigned cand_total; // candidates made by the completed levels (written by the barriers' last arrivers)
+    unsigned pad9[29];
+    unsigned cand_ready; // candidates published to the candidate blocks (all written)
+    unsigned cand_final; // 1: no candidate will be published after cand_ready
+    unsigned pad10[30];
     unsigned long long t_start;                 // globaltimer at the launch's start (ns)
     unsigned long long level_ns[kLevelTimes];   // globaltimer when level l ended (its barrier completed)
 };
@@ -151,6 +155,8 @@ struct Bufs {
     int two_frame;    // also test child boxes in B's own frame (fewer pairs, more work per pair)
     int deep_seed;    // seed from the depth-4 cuts (single-pair calls) instead of the depth-3 cuts
     unsigned quad_below;  // level-synchronous traversal: levels of at most this many node pairs use the quad form
+    unsigned cand_blocks; // level-synchronous traversal: blocks that only filter candidates (0: every block
+                          // expands node pairs and filters the previous level's candidates)
 };
 
 }  // namespace gi

@@ -1644,9 +1644,12 @@ __device__ __forceinline__ unsigned long long globaltimer_ns()
     return t;
 }
 
-// Grid barrier ending level `lev` of the level-synchronous traversal.  Returns
-// false when the block's wait ran out (the block must leave the kernel).
-__device__ __forceinline__ bool level_barrier(const Bufs& B, unsigned& gen, unsigned lev)
+// Grid barrier ending level `lev` of the level-synchronous traversal, among
+// the `nblocks` blocks that expand node pairs.  Returns false when the block's
+// wait ran out (the block must leave the kernel).  The last block to arrive
+// also publishes the level's candidates to the candidate blocks (split form):
+// they are all written once every node block has arrived.
+__device__ __forceinline__ bool level_barrier(const Bufs& B, unsigned& gen, unsigned lev, unsigned nblocks)
 {
     __shared__ unsigned s_ok;
     Counters* C = B.cnt;
@@ -1655,15 +1658,28 @@ __device__ __forceinline__ bool level_barrier(const Bufs& B, unsigned& gen, unsi
         s_ok = 1u;
         __threadfence();
         const unsigned arrived = atomicAdd(&C->bar_count, 1u) + 1u;
-        if (arrived == gridDim.x) {
-            // every block has arrived: the counts of this level are final
+        if (arrived == nblocks) {
+            // every node block has arrived: the counts of this level are final
             C->bar_count = 0u;
             const unsigned long long v = __ldcg(&C->lvl[lev % 3u]);
             const unsigned ab = ld_vol(&C->abort_);
-            C->bstop = (ab != 0u || v == 0ull) ? 1u : 0u;
+            // the split form stops when no node pair is left (its candidates go
+            // to the candidate blocks); the other when the level made nothing
+            const bool stop = ab != 0u || (B.cand_blocks ? (unsigned)v == 0u : v == 0ull);
+            C->bstop = stop ? 1u : 0u;
             C->lvl[(lev + 2u) % 3u] = 0ull;
             atomicMax(&C->q_tail, 2u * (unsigned)v);  // both halves of the queue buffer must hold the widest level
             if (lev < (unsigned)kLevelTimes) C->level_ns[lev] = globaltimer_ns();
+            const unsigned tot = C->cand_total + (unsigned)(v >> 32);
+            C->cand_total = tot;
+            if (B.cand_blocks) {
+                __threadfence();
+                atomicExch(&C->cand_ready, tot);
+                if (stop) {
+                    __threadfence();
+                    atomicExch(&C->cand_final, 1u);
+                }
+            }
             __threadfence();
             atomicExch(&C->bar_gen, gen + 1u);
         } else {
@@ -1779,13 +1795,62 @@ __device__ __forceinline__ void level_reserve(const Bufs& B, unsigned lev, unsig
     c = snap + (unsigned)(old >> 32) + incc - nc;
 }
 
+// Candidate blocks of the split form: warps take chunks of 32 candidates with
+// one atomic and filter them once the node blocks have published them (every
+// level's candidates are published by the barrier that ends it).  A warp
+// leaves when its chunk starts at or beyond the final count.
+template <bool F64>
+__device__ __forceinline__ void filter_published(const Bufs& B, unsigned long long& decided,
+                                                 unsigned long long& tested)
+{
+    Counters* C = B.cnt;
+    const unsigned lane = threadIdx.x & 31;
+    for (;;) {
+        unsigned base = 0, ready = 0, gone = 0;
+        if (lane == 0) {
+            base = atomicAdd(&C->c_head, 32u);
+            unsigned spins = 0;
+            for (;;) {
+                ready = ld_acq(&C->cand_ready);
+                if (ready >= base + 32u) break;
+                if (ld_acq(&C->cand_final)) {  // cand_ready was written before the final flag
+                    ready = ld_acq(&C->cand_ready);
+                    break;
+                }
+                if (ld_vol(&C->abort_)) {
+                    gone = 1u;
+                    break;
+                }
+                if (++spins > kIdleSpins) {
+                    atomicOr(&C->err, kErrTimeout);
+                    atomicExch(&C->abort_, 1u);
+                    gone = 1u;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        base = __shfl_sync(0xffffffffu, base, 0);
+        ready = __shfl_sync(0xffffffffu, ready, 0);
+        gone = __shfl_sync(0xffffffffu, gone, 0);
+        if (gone || base >= ready) return;
+        const unsigned i = base + lane;
+        const bool have = i < min(ready, B.cap_cand);
+        const uint4 cnd = have ? __ldcg(B.cand + i) : make_uint4(0u, 0u, 0u, 0u);
+        filter_candidates<F64>(B, have, cnd, decided, tested);
+    }
+}
+
 template <bool F64>
 __global__ void __launch_bounds__(kTravThreads, 2) k_traverse_levels(Bufs B)
 {
     Counters* C = B.cnt;
     const unsigned lane = threadIdx.x & 31;
+    // blocks [0, nblocks) expand node pairs; in the split form the others filter candidates
+    const unsigned nblocks = gridDim.x - B.cand_blocks;
+    const bool node_block = blockIdx.x < nblocks;
     const unsigned gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const unsigned nw = (gridDim.x * blockDim.x) >> 5;
+    const unsigned nw = (nblocks * blockDim.x) >> 5;
     const uint32_t capL = B.cap_queue / 2u;
     uint4* const front0 = B.queue;
     uint4* const front1 = B.queue + capL;
@@ -1793,9 +1858,10 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse_levels(Bufs B)
     unsigned long long visited = 0, decided = 0, tested = 0;
     unsigned gen = 0, snap = 0, lev = 0;
     bool ovf_f = false, ovf_c = false;
-    seed_levels<F64>(B, gw, nw, front0, capL);
-    for (;;) {
-        if (!level_barrier(B, gen, lev)) return;
+    if (node_block) seed_levels<F64>(B, gw, nw, front0, capL);
+    else filter_published<F64>(B, decided, tested);
+    for (; node_block;) {
+        if (!level_barrier(B, gen, lev, nblocks)) return;
         if (__ldcg(&C->bstop)) break;
         // the pairs made by level `lev`, expanded and filtered by level lev + 1
         const unsigned long long v = __ldcg(&C->lvl[lev % 3u]);
@@ -1808,7 +1874,9 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse_levels(Bufs B)
         const bool quad = n <= B.quad_below;
         const unsigned per = quad ? 8u : 32u;
         const unsigned node_chunks = (n + per - 1u) / per;
-        const unsigned chunks = node_chunks + (cend > cbase ? (cend - cbase + 31u) / 32u : 0u);
+        // the split form leaves the candidates to the candidate blocks
+        const unsigned chunks =
+            node_chunks + (!B.cand_blocks && cend > cbase ? (cend - cbase + 31u) / 32u : 0u);
         for (unsigned k = gw; k < chunks; k += nw) {
             if (k < node_chunks) {
                 if (quad) {
@@ -2529,10 +2597,13 @@ cudaError_t launch_traverse(const Bufs& b, const LaunchCfg& cfg, int precision, 
     note_launches(1);
     const int f64 = precision == 1 ? 1 : 0, q = shape.quad ? 1 : 0;
     if (shape.levels) {
-        // cooperative: the grid barriers need every block resident
-        const int grid = (shape.one_per_sm ? 1 : cfg.levels_per_sm[f64]) * cfg.sms;
+        // cooperative: the grid barriers need every block resident.  Bit 0 of the
+        // shape selects the split form: half the blocks filter candidates while
+        // the other half expand the levels' node pairs
+        const int grid = cfg.levels_per_sm[f64] * cfg.sms;
         Bufs bb = b;
-        bb.quad_below = shape.quad ? (unsigned)(grid * (kTravThreads / 32) * 8) : 0u;
+        bb.cand_blocks = shape.one_per_sm ? (unsigned)(grid / 2) : 0u;
+        bb.quad_below = shape.quad ? (unsigned)((grid - (int)bb.cand_blocks) * (kTravThreads / 32) * 8) : 0u;
         void* args[] = {&bb};
         return cudaLaunchCooperativeKernel(f64 ? (const void*)k_traverse_levels<true> : (const void*)k_traverse_levels<false>,
                                            dim3(grid), dim3(kTravThreads), args, 0, st);

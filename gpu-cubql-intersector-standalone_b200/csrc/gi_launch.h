@@ -56,7 +56,9 @@ struct LaunchCfg {
 // Traversal shapes the tuner chooses from: the work-queue traversal or the
 // level-synchronous one (bit 2); expansion form (bit 1: one node pair per quad
 // of lanes; for the level-synchronous traversal, the quad form on levels of at
-// most 8 node pairs per warp) x blocks per SM (bit 0: one, else all resident).
+// most 8 node pairs per warp); bit 0: the work-queue traversal with one block
+// per SM (else all resident), the level-synchronous one in its split form
+// (half the blocks only filter candidates).
 struct TravShape {
     bool quad = false;
     bool one_per_sm = false;
