@@ -1947,6 +1947,9 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse_levels(Bufs B)
             ovf_f = ovf_c = false;
         }
     }
+    // split form: the node blocks are done (the last barrier published every
+    // candidate and the final flag) and join the candidate blocks on what is left
+    if (node_block && B.cand_blocks) filter_published<F64>(B, decided, tested);
     for (int o = 16; o > 0; o >>= 1) {
         visited += __shfl_xor_sync(0xffffffffu, visited, o);
         decided += __shfl_xor_sync(0xffffffffu, decided, o);
