@@ -709,6 +709,7 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         b.deep_seed = nj == 1 ? 1 : 0;
         b.quad_below = 0u;   // set by the launcher of the level-synchronous traversal
         b.cand_blocks = 0u;
+        b.publish = 0u;
         CK(c, cudaMemsetAsync(c->d_cnt, 0, sizeof(Counters), c->st), "counters");
         CK(c, cudaEventRecord(c->ev[0], c->st), "event");
         CK(c, launch_traverse(b, c->cfg, prec, trav_shape(shape), c->st), "traverse");

@@ -155,8 +155,9 @@ struct Bufs {
     int two_frame;    // also test child boxes in B's own frame (fewer pairs, more work per pair)
     int deep_seed;    // seed from the depth-4 cuts (single-pair calls) instead of the depth-3 cuts
     unsigned quad_below;  // level-synchronous traversal: levels of at most this many node pairs use the quad form
-    unsigned cand_blocks; // level-synchronous traversal: blocks that only filter candidates (0: every block
-                          // expands node pairs and filters the previous level's candidates)
+    unsigned cand_blocks; // level-synchronous traversal: blocks that only filter candidates
+    unsigned publish;     // level-synchronous traversal: 1 = each level's candidates are published to the
+                          // candidate blocks (0: they are filtered by every warp in the next level)
 };
 
 }  // namespace gi

@@ -1644,11 +1644,24 @@ __device__ __forceinline__ unsigned long long globaltimer_ns()
     return t;
 }
 
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed_u32(unsigned* p, unsigned v)
+{
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // Grid barrier ending level `lev` of the level-synchronous traversal, among
-// the `nblocks` blocks that expand node pairs.  Returns false when the block's
-// wait ran out (the block must leave the kernel).  The last block to arrive
-// also publishes the level's candidates to the candidate blocks (split form):
-// they are all written once every node block has arrived.
+// `nblocks` blocks.  Returns false when the block's wait ran out (the block must
+// leave the kernel).  The last block to arrive decides for every block whether
+// the traversal is over, clears the counter slot that level lev + 2 will use,
+// stamps the level's end time and publishes the level's candidates to the
+// candidate blocks (split form); they are all written once every node block has
+// arrived.  Its loads go out together and its stores are released by one
+// release store of the generation word, so the barrier costs few round trips
+// to L2 on its critical path.
 __device__ __forceinline__ bool level_barrier(const Bufs& B, unsigned& gen, unsigned lev, unsigned nblocks)
 {
     __shared__ unsigned s_ok;
@@ -1656,32 +1669,33 @@ __device__ __forceinline__ bool level_barrier(const Bufs& B, unsigned& gen, unsi
     __syncthreads();
     if (threadIdx.x == 0) {
         s_ok = 1u;
-        __threadfence();
+        __threadfence();  // this block's writes of the level before its arrival
         const unsigned arrived = atomicAdd(&C->bar_count, 1u) + 1u;
         if (arrived == nblocks) {
-            // every node block has arrived: the counts of this level are final
-            C->bar_count = 0u;
+            // every block has arrived: the counts of this level are final (read
+            // through L2, where every block's fenced writes are; the acquire
+            // fence has no store of this thread to wait for)
+            fence_acq_rel();
             const unsigned long long v = __ldcg(&C->lvl[lev % 3u]);
-            const unsigned ab = ld_vol(&C->abort_);
-            // the split form stops when no node pair is left (its candidates go
-            // to the candidate blocks); the other when the level made nothing
-            const bool stop = ab != 0u || (B.cand_blocks ? (unsigned)v == 0u : v == 0ull);
+            const unsigned ab = __ldcg(&C->abort_);
+            const unsigned prev = __ldcg(&C->cand_total);
+            // with published candidates the levels stop when no node pair is left
+            // (the filtering warps finish the candidates); otherwise when the
+            // level made nothing
+            const bool stop = ab != 0u || (B.publish ? (unsigned)v == 0u : v == 0ull);
+            const unsigned tot = prev + (unsigned)(v >> 32);
+            C->bar_count = 0u;
             C->bstop = stop ? 1u : 0u;
             C->lvl[(lev + 2u) % 3u] = 0ull;
+            C->cand_total = tot;
             atomicMax(&C->q_tail, 2u * (unsigned)v);  // both halves of the queue buffer must hold the widest level
             if (lev < (unsigned)kLevelTimes) C->level_ns[lev] = globaltimer_ns();
-            const unsigned tot = C->cand_total + (unsigned)(v >> 32);
-            C->cand_total = tot;
-            if (B.cand_blocks) {
-                __threadfence();
-                atomicExch(&C->cand_ready, tot);
-                if (stop) {
-                    __threadfence();
-                    atomicExch(&C->cand_final, 1u);
-                }
+            if (B.publish) {
+                st_relaxed_u32(&C->cand_ready, tot);
+                // cand_ready is visible before the final flag
+                if (stop) st_release_u32(&C->cand_final, 1u);
             }
-            __threadfence();
-            atomicExch(&C->bar_gen, gen + 1u);
+            st_release_u32(&C->bar_gen, gen + 1u);  // releases every store above
         } else {
             unsigned spins = 0;
             while (ld_acq(&C->bar_gen) == gen) {
@@ -1858,6 +1872,7 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse_levels(Bufs B)
     unsigned long long visited = 0, decided = 0, tested = 0;
     unsigned gen = 0, snap = 0, lev = 0;
     bool ovf_f = false, ovf_c = false;
+    // the node blocks seed; the candidate blocks filter from the start
     if (node_block) seed_levels<F64>(B, gw, nw, front0, capL);
     else filter_published<F64>(B, decided, tested);
     for (; node_block;) {
@@ -1874,9 +1889,8 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse_levels(Bufs B)
         const bool quad = n <= B.quad_below;
         const unsigned per = quad ? 8u : 32u;
         const unsigned node_chunks = (n + per - 1u) / per;
-        // the split form leaves the candidates to the candidate blocks
-        const unsigned chunks =
-            node_chunks + (!B.cand_blocks && cend > cbase ? (cend - cbase + 31u) / 32u : 0u);
+        // published candidates are left to the filtering warps
+        const unsigned chunks = node_chunks + (!B.publish && cend > cbase ? (cend - cbase + 31u) / 32u : 0u);
         for (unsigned k = gw; k < chunks; k += nw) {
             if (k < node_chunks) {
                 if (quad) {
@@ -1947,9 +1961,9 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse_levels(Bufs B)
             ovf_f = ovf_c = false;
         }
     }
-    // split form: the node blocks are done (the last barrier published every
-    // candidate and the final flag) and join the candidate blocks on what is left
-    if (node_block && B.cand_blocks) filter_published<F64>(B, decided, tested);
+    // published candidates: the node blocks are done (the last barrier published
+    // every candidate and the final flag) and filter what is left
+    if (node_block && B.publish) filter_published<F64>(B, decided, tested);
     for (int o = 16; o > 0; o >>= 1) {
         visited += __shfl_xor_sync(0xffffffffu, visited, o);
         decided += __shfl_xor_sync(0xffffffffu, decided, o);
@@ -2605,7 +2619,8 @@ cudaError_t launch_traverse(const Bufs& b, const LaunchCfg& cfg, int precision, 
         // the other half expand the levels' node pairs
         const int grid = cfg.levels_per_sm[f64] * cfg.sms;
         Bufs bb = b;
-        bb.cand_blocks = shape.one_per_sm ? (unsigned)(grid / 2) : 0u;
+        bb.cand_blocks = shape.one_per_sm ? (unsigned)(grid / 3) : 0u;
+        bb.publish = shape.one_per_sm ? 1u : 0u;
         bb.quad_below = shape.quad ? (unsigned)((grid - (int)bb.cand_blocks) * (kTravThreads / 32) * 8) : 0u;
         void* args[] = {&bb};
         return cudaLaunchCooperativeKernel(f64 ? (const void*)k_traverse_levels<true> : (const void*)k_traverse_levels<false>,
