@@ -1809,49 +1809,125 @@ __device__ __forceinline__ void level_reserve(const Bufs& B, unsigned lev, unsig
     c = snap + (unsigned)(old >> 32) + incc - nc;
 }
 
-// Candidate blocks of the split form: warps take chunks of 32 candidates with
-// one atomic and filter them once the node blocks have published them (every
-// level's candidates are published by the barrier that ends it).  A warp
-// leaves when its chunk starts at or beyond the final count.
+// Published candidates (split form).  A warp takes chunks of 32 candidates
+// with one atomic and filters each once the node blocks have published it
+// (every level's candidates are published by the barrier that ends it).  The
+// loop is software-pipelined: the next chunk is claimed before the current one
+// is filtered, and when it is already published, its candidate records and
+// triangle records are loaded before the current chunk's vertices, so these
+// two dependent round trips overlap the current chunk's work.  A warp leaves
+// when its chunk starts at or beyond the final count.
+constexpr unsigned kGone = 0xffffffffu;
+
+// Lane 0 waits (bounded) until the chunk at `base` is published in full or no
+// more candidates will come; returns the published count, or kGone.
+__device__ __forceinline__ unsigned wait_published(Counters* C, unsigned base)
+{
+    unsigned ready = 0, spins = 0;
+    for (;;) {
+        ready = ld_acq(&C->cand_ready);
+        if (ready >= base + 32u) return ready;
+        if (ld_acq(&C->cand_final)) return ld_acq(&C->cand_ready);  // written before the final flag
+        if (ld_vol(&C->abort_)) return kGone;
+        if (++spins > kIdleSpins) {
+            atomicOr(&C->err, kErrTimeout);
+            atomicExch(&C->abort_, 1u);
+            return kGone;
+        }
+        __nanosleep(64);
+    }
+}
+
+struct PubChunk {
+    uint4 c;       // candidate: job, leaf position in A, leaf position in B
+    uint4 ta, tb;  // the two leaves' records: vertex indices and original triangle id
+    bool have;
+};
+
+__device__ __forceinline__ PubChunk load_published(const Bufs& B, unsigned base, unsigned ready)
+{
+    PubChunk k;
+    const unsigned i = base + (threadIdx.x & 31u);
+    k.have = i < min(ready, B.cap_cand);
+    k.c = k.have ? __ldcg(B.cand + i) : make_uint4(0u, 0u, 0u, 0u);
+    k.ta = k.tb = make_uint4(0u, 0u, 0u, 0u);
+    if (k.have) {
+        const JobDev& J = B.jobs[k.c.x];
+        k.ta = __ldg(J.A.leafTri + k.c.y);
+        k.tb = __ldg(J.B.leafTri + k.c.z);
+    }
+    return k;
+}
+
+template <bool F64>
+__device__ __forceinline__ void filter_loaded(const Bufs& B, const PubChunk& k, unsigned long long& decided,
+                                              unsigned long long& tested)
+{
+    Counters* C = B.cnt;
+    int dec = DEC_NO;
+    if (k.have) {
+        tested++;
+        const JobDev& J = B.jobs[k.c.x];
+        double3 P[3], Q[3];
+        P[0] = world_vertex(J.A.verts, k.ta.x, J.pa);
+        P[1] = world_vertex(J.A.verts, k.ta.y, J.pa);
+        P[2] = world_vertex(J.A.verts, k.ta.z, J.pa);
+        Q[0] = world_vertex(J.B.verts, k.tb.x, J.pb);
+        Q[1] = world_vertex(J.B.verts, k.tb.y, J.pb);
+        Q[2] = world_vertex(J.B.verts, k.tb.z, J.pb);
+        if constexpr (F64) dec = classify_fast<double>(P, Q);
+        else dec = classify_fast<float>(P, Q);
+        decided += (dec != DEC_ESC);
+    }
+    const bool yes = k.have && dec == DEC_YES;
+    const bool esc = k.have && dec == DEC_ESC;
+    const unsigned pr = warp_append(yes, &C->res);
+    if (yes) {
+        if (pr < B.cap_res) B.res[pr] = make_uint4(k.c.x, k.ta.w, k.tb.w, 0u);
+        else atomicOr(&C->overflow, kOvfRes);
+    }
+    const unsigned pe = warp_append(esc, &C->esc);
+    if (esc) {
+        if (pe < B.cap_esc) B.esc[pe] = make_uint4(k.c.x, k.c.y, k.c.z, 0u);
+        else atomicOr(&C->overflow, kOvfEsc);
+    }
+}
+
 template <bool F64>
 __device__ __forceinline__ void filter_published(const Bufs& B, unsigned long long& decided,
                                                  unsigned long long& tested)
 {
     Counters* C = B.cnt;
     const unsigned lane = threadIdx.x & 31;
+    unsigned base = 0, ready = 0;
+    if (lane == 0) {
+        base = atomicAdd(&C->c_head, 32u);
+        ready = wait_published(C, base);
+    }
+    base = __shfl_sync(0xffffffffu, base, 0);
+    ready = __shfl_sync(0xffffffffu, ready, 0);
+    if (ready == kGone || base >= ready) return;
+    PubChunk cur = load_published(B, base, ready);
     for (;;) {
-        unsigned base = 0, ready = 0, gone = 0;
+        // the next chunk: claimed now, its records loaded now if it is published
+        unsigned nbase = 0, nready = 0;
         if (lane == 0) {
-            base = atomicAdd(&C->c_head, 32u);
-            unsigned spins = 0;
-            for (;;) {
-                ready = ld_acq(&C->cand_ready);
-                if (ready >= base + 32u) break;
-                if (ld_acq(&C->cand_final)) {  // cand_ready was written before the final flag
-                    ready = ld_acq(&C->cand_ready);
-                    break;
-                }
-                if (ld_vol(&C->abort_)) {
-                    gone = 1u;
-                    break;
-                }
-                if (++spins > kIdleSpins) {
-                    atomicOr(&C->err, kErrTimeout);
-                    atomicExch(&C->abort_, 1u);
-                    gone = 1u;
-                    break;
-                }
-                __nanosleep(64);
-            }
+            nbase = atomicAdd(&C->c_head, 32u);
+            nready = ld_acq(&C->cand_ready);
         }
-        base = __shfl_sync(0xffffffffu, base, 0);
-        ready = __shfl_sync(0xffffffffu, ready, 0);
-        gone = __shfl_sync(0xffffffffu, gone, 0);
-        if (gone || base >= ready) return;
-        const unsigned i = base + lane;
-        const bool have = i < min(ready, B.cap_cand);
-        const uint4 cnd = have ? __ldcg(B.cand + i) : make_uint4(0u, 0u, 0u, 0u);
-        filter_candidates<F64>(B, have, cnd, decided, tested);
+        nbase = __shfl_sync(0xffffffffu, nbase, 0);
+        nready = __shfl_sync(0xffffffffu, nready, 0);
+        const bool early = nready >= nbase + 32u;
+        PubChunk nxt;
+        if (early) nxt = load_published(B, nbase, nready);
+        filter_loaded<F64>(B, cur, decided, tested);
+        if (!early) {
+            if (lane == 0) nready = wait_published(C, nbase);
+            nready = __shfl_sync(0xffffffffu, nready, 0);
+            if (nready == kGone || nbase >= nready) return;
+            nxt = load_published(B, nbase, nready);
+        }
+        cur = nxt;
     }
 }
 
