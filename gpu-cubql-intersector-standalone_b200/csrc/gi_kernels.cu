@@ -2691,8 +2691,8 @@ cudaError_t launch_traverse(const Bufs& b, const LaunchCfg& cfg, int precision, 
     const int f64 = precision == 1 ? 1 : 0, q = shape.quad ? 1 : 0;
     if (shape.levels) {
         // cooperative: the grid barriers need every block resident.  Bit 0 of the
-        // shape selects the split form: half the blocks filter candidates while
-        // the other half expand the levels' node pairs
+        // shape selects the split form: a third of the blocks filter candidates
+        // while the other two thirds expand the levels' node pairs
         const int grid = cfg.levels_per_sm[f64] * cfg.sms;
         Bufs bb = b;
         bb.cand_blocks = shape.one_per_sm ? (unsigned)(grid / 3) : 0u;

@@ -93,8 +93,8 @@ typedef struct gi_server gi_server;
  * traversal (grid barriers between the levels) over the work-queue one; bit 1
  * the quad form (one node pair per quad of lanes; level-synchronous: on levels
  * of at most 8 node pairs per warp); bit 0 one block per SM instead of all
- * resident blocks (work queue) or the split form, in which half the blocks
- * only filter candidates as the levels publish them (level-synchronous). */
+ * resident blocks (work queue) or the split form, in which a third of the
+ * blocks only filter candidates as the levels publish them (level-synchronous). */
 #define GI_FLAG_FIXED_SHAPE 0x100u
 #define GI_FLAG_SHAPE(k) ((((uint32_t)(k)) & 7u) << 9)
 
