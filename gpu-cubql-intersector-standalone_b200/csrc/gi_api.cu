@@ -640,6 +640,14 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
     // the result will be small (the kernel refuses, and this loop reruns on the
     // radix path, if it is not)
     bool small_order = ba + bb + bj <= 63 && c->pred_pairs <= kOrderSmallMax - kOrderSmallMax / 4;
+    // everything after the traversal in one launch: sorted output of a result
+    // the previous call's count says is small enough (the kernel refuses, and
+    // this loop reruns on the general path, if it is not, or if its keys crowd
+    // into one partition; a refusal keeps the next calls off this path a while)
+    bool fin = sort && ba + bb + bj <= 63 && c->pred_pairs <= kFinMax - kFinMax / 4 && c->fin_backoff == 0;
+    if (c->fin_backoff) c->fin_backoff--;
+    const int kbits = ba + bb + bj;
+    const int fin_shift = kbits > kFinPartBits ? kbits - kFinPartBits : 0;
     const uint32_t tune_key = TravTuner::key(prec, nj, sumT);
     const int shape = c->fixed_shape >= 0 ? c->fixed_shape : c->tuner.pick(tune_key);
     for (;;) {
@@ -714,32 +722,45 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         CK(c, cudaEventRecord(c->ev[0], c->st), "event");
         CK(c, launch_traverse(b, c->cfg, prec, trav_shape(shape), c->st), "traverse");
         CK(c, cudaEventRecord(c->ev[1], c->st), "event");
-        CK(c, launch_exact(b, c->cfg, c->st), "exact stage");
-        CK(c, cudaEventRecord(c->ev[2], c->st), "event");
-        if (small_order && want_segs && sort) {
-            // the segments are built on the second stream while the ordering
-            // ranks the results; only the placing launch waits for them
-            CK(c, cudaStreamWaitEvent(c->st2, c->ev[2], 0), "event");
-            CK(c, launch_segments(b, c->segs, c->nseg, c->cfg, c->st2), "segments");
-            CK(c, cudaEventRecord(c->ev[3], c->st2), "event");
-            CK(c, launch_order_small_phases(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
-                                            c->segpair_out, want_segs, kOrderRank, c->st),
-               "ordering");
-            CK(c, cudaStreamWaitEvent(c->st, c->ev[3], 0), "event");
-            CK(c, launch_order_small_phases(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
-                                            c->segpair_out, want_segs, kOrderPlace, c->st),
-               "ordering");
+        if (fin) {
+            FinArgs F;
+            F.segs = c->segs;
+            F.pairs_out = c->pairs_out;
+            F.job_out = c->job_out;
+            F.segs_out = c->segs_out;
+            F.segpair_out = c->segpair_out;
+            F.cap = cap;
+            F.want_segments = want_segs ? 1 : 0;
+            F.shift = fin_shift;
+            CK(c, launch_finish(b, O, F, c->cfg, c->st), "exact stage, segments and ordering");
         } else {
-            if (want_segs) CK(c, launch_segments(b, c->segs, c->nseg, c->cfg, c->st), "segments");
-            CK(c, cudaEventRecord(c->ev[3], c->st), "event");
-            if (small_order)
-                CK(c, launch_order_small(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
-                                         c->segpair_out, want_segs, c->st),
+            CK(c, launch_exact(b, c->cfg, c->st), "exact stage");
+            CK(c, cudaEventRecord(c->ev[2], c->st), "event");
+            if (small_order && want_segs && sort) {
+                // the segments are built on the second stream while the ordering
+                // ranks the results; only the placing launch waits for them
+                CK(c, cudaStreamWaitEvent(c->st2, c->ev[2], 0), "event");
+                CK(c, launch_segments(b, c->segs, c->nseg, c->cfg, c->st2), "segments");
+                CK(c, cudaEventRecord(c->ev[3], c->st2), "event");
+                CK(c, launch_order_small_phases(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
+                                                c->segpair_out, want_segs, kOrderRank, c->st),
                    "ordering");
-            else
-                CK(c, launch_order_gather(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
-                                          c->segpair_out, want_segs, c->cfg, c->st),
+                CK(c, cudaStreamWaitEvent(c->st, c->ev[3], 0), "event");
+                CK(c, launch_order_small_phases(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
+                                                c->segpair_out, want_segs, kOrderPlace, c->st),
                    "ordering");
+            } else {
+                if (want_segs) CK(c, launch_segments(b, c->segs, c->nseg, c->cfg, c->st), "segments");
+                CK(c, cudaEventRecord(c->ev[3], c->st), "event");
+                if (small_order)
+                    CK(c, launch_order_small(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
+                                             c->segpair_out, want_segs, c->st),
+                       "ordering");
+                else
+                    CK(c, launch_order_gather(b, O, sort, c->segs, c->nseg, c->pairs_out, c->job_out, c->segs_out,
+                                              c->segpair_out, want_segs, c->cfg, c->st),
+                       "ordering");
+            }
         }
         CK(c, cudaEventRecord(c->ev[4], c->st), "event");
         // speculative copy at the previous call's size
@@ -766,7 +787,11 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
                "copy segments");
         }
         CK(c, cudaStreamSynchronize(c->st), "sync");
-        if (H.err & kErrTimeout) return set_err(c, GI_ERR_TIMEOUT, "a bounded device wait ran out");
+        if (H.err & kErrTimeout) {
+            // a finish launch that gave up may leave partition counts behind
+            if (fin) cudaMemsetAsync(O.fin, 0, sizeof(uint32_t) * 2 * kFinParts, c->st);
+            return set_err(c, GI_ERR_TIMEOUT, "a bounded device wait ran out");
+        }
         if (H.err & kErrExactCapacity) return set_err(c, GI_ERR_RANGE, "exact arithmetic capacity exceeded");
         if (H.overflow) {
             if (retries >= 12) return set_err(c, GI_ERR_CAPACITY, "intersection buffers stayed too small");
@@ -782,6 +807,14 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
             continue;
         }
         if (H.order_redo) {
+            if (fin) {
+                // a refusal after the counting leaves the partition counts behind
+                CK(c, cudaMemsetAsync(O.fin, 0, sizeof(uint32_t) * 2 * kFinParts, c->st), "finish counts");
+                fin = false;
+                if (H.order_redo == kRedoCrowded) c->fin_backoff = 64;
+                if (H.res > kOrderSmallMax) small_order = false;
+                continue;
+            }
             if (!small_order) return set_err(c, GI_ERR_CAPACITY, "ordering path refused twice");
             small_order = false;
             continue;
@@ -817,10 +850,20 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
     c->pred_segs = nsegs;
     float ms_trav = 0, ms_exact = 0, ms_seg = 0, ms_sort = 0, ms_total = 0;
     cudaEventElapsedTime(&ms_trav, c->ev[0], c->ev[1]);
-    cudaEventElapsedTime(&ms_exact, c->ev[1], c->ev[2]);
-    cudaEventElapsedTime(&ms_seg, c->ev[2], c->ev[3]);
-    cudaEventElapsedTime(&ms_sort, c->ev[3], c->ev[4]);
     cudaEventElapsedTime(&ms_total, c->ev[0], c->ev[4]);
+    if (fin) {
+        // one launch after the traversal: its phases from its own timestamps,
+        // the ordering takes the rest (launch included)
+        if (H.fin_ns[1] >= H.fin_ns[0] && H.fin_ns[2] >= H.fin_ns[1]) {
+            ms_exact = (float)(1e-6 * double(H.fin_ns[1] - H.fin_ns[0]));
+            ms_seg = (float)(1e-6 * double(H.fin_ns[2] - H.fin_ns[1]));
+        }
+        ms_sort = std::max(0.0f, ms_total - ms_trav - ms_exact - ms_seg);
+    } else {
+        cudaEventElapsedTime(&ms_exact, c->ev[1], c->ev[2]);
+        cudaEventElapsedTime(&ms_seg, c->ev[2], c->ev[3]);
+        cudaEventElapsedTime(&ms_sort, c->ev[3], c->ev[4]);
+    }
     if (c->fixed_shape < 0) c->tuner.report(tune_key, shape, ms_trav);
     // split per job (sorted by job first)
     std::vector<uint32_t> job_start(nj + 1, 0);
@@ -889,6 +932,11 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         s2.ms_sort = ms_sort;
         s2.ms_total = ms_total;
         static_assert(sizeof(s2.level_end_ms) / sizeof(double) == (size_t)kLevelTimes, "level time slots");
+        if (fin && H.fin_ns[0] && H.fin_ns[4] >= H.fin_ns[0]) {
+            for (int k = 0; k < 4; k++)
+                s2.finish_ms[k] = H.fin_ns[k + 1] >= H.fin_ns[0] ? 1e-6 * double(H.fin_ns[k + 1] - H.fin_ns[0]) : 0.0;
+            s2.finish_phases = 4;
+        }
         if (trav_shape(shape).levels && H.t_start) {
             const uint32_t nl = std::min<uint32_t>(H.levels + 1u, (uint32_t)kLevelTimes);
             for (uint32_t l = 0; l < nl && H.level_ns[l] >= H.t_start; l++) {

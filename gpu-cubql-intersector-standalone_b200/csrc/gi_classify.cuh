@@ -166,10 +166,25 @@ __device__ __forceinline__ int lone_index(const int s[3])
     return 2;
 }
 
+// Endpoint pattern of a pair that the first stage found intersecting: in
+// general position the intersection is the segment between two of the four
+// edge-plane crossings X0, X1 (P's edges from its lone vertex o1, in vertex
+// order, through plane(Q)) and Y0, Y1 (Q's edges from o2 through plane(P));
+// xin / yin mark the crossings that lie inside the other interval.  The exact
+// classification gives the same points in the same order (X's, then Y's), so a
+// consumer can construct them without evaluating any sign again.
+//   bit 0 valid, bits 1-2 o1, bits 3-4 o2, bits 5-6 xin, bits 7-8 yin
+constexpr unsigned kPatValid = 1u;
+__device__ __forceinline__ unsigned make_pattern(int o1, int o2, unsigned xin, unsigned yin)
+{
+    return kPatValid | ((unsigned)o1 << 1) | ((unsigned)o2 << 3) | (xin << 5) | (yin << 7);
+}
+
 // First stage: decides the general-position case (every vertex strictly off the
-// other triangle's plane) with filtered signs; everything else escalates.
+// other triangle's plane) with filtered signs; everything else escalates.  For
+// an intersecting pair, *pat receives its endpoint pattern (make_pattern).
 template <class T>
-static __device__ int classify_fast(const double3* P, const double3* Q)
+static __device__ int classify_fast(const double3* P, const double3* Q, unsigned* pat = nullptr)
 {
     Plane<T> pp = make_plane<T>(vdiff<T>(P[1], P[0]), vdiff<T>(P[2], P[0]));
     if (!pp.proper) return DEC_ESC;
@@ -208,9 +223,11 @@ static __device__ int classify_fast(const double3* P, const double3* Q)
             c[i][j] = filt_o3<T>(xn[i], xp[i], yn[j], yp[j]);
             if (c[i][j] == kUnsure) return DEC_ESC;
         }
-    bool hit = (c[0][0] * c[0][1] < 0) || (c[1][0] * c[1][1] < 0) || (c[0][0] * c[1][0] < 0) ||
-               (c[0][1] * c[1][1] < 0);
-    return hit ? DEC_YES : DEC_NO;
+    const unsigned xin = (c[0][0] * c[0][1] < 0 ? 1u : 0u) | (c[1][0] * c[1][1] < 0 ? 2u : 0u);
+    const unsigned yin = (c[0][0] * c[1][0] < 0 ? 1u : 0u) | (c[0][1] * c[1][1] < 0 ? 2u : 0u);
+    if (!(xin | yin)) return DEC_NO;
+    if (pat) *pat = make_pattern(o1, o2, xin, yin);
+    return DEC_YES;
 }
 
 // ---------------------------------------------------------------------------
@@ -845,7 +862,8 @@ __device__ __forceinline__ dd dd_div(dd x, dd y)  // DWDivDW2, rel. err <= 15u^2
 
 // orient3d(p,q,r,x) = det[p-x; q-x; r-x] in double-double; *perm receives the
 // permanent.  |error| <= 21u^2 perm (4u^2 products, 3u^2 sums); callers use 64u^2.
-static __device__ __noinline__ dd o3_dd(const double3& p, const double3& q, const double3& r, const double3& x, double* perm)
+__device__ __forceinline__ dd o3_dd_f(const double3& p, const double3& q, const double3& r, const double3& x,
+                                     double* perm)
 {
     dd adx = two_diff_dd(p.x, x.x), ady = two_diff_dd(p.y, x.y), adz = two_diff_dd(p.z, x.z);
     dd bdx = two_diff_dd(q.x, x.x), bdy = two_diff_dd(q.y, x.y), bdz = two_diff_dd(q.z, x.z);
@@ -858,6 +876,10 @@ static __device__ __noinline__ dd o3_dd(const double3& p, const double3& q, cons
     *perm = (fabs(p1.hi) + fabs(p2.hi)) * fabs(adz.hi) + (fabs(p3.hi) + fabs(p4.hi)) * fabs(bdz.hi) +
             (fabs(p5.hi) + fabs(p6.hi)) * fabs(cdz.hi);
     return det;
+}
+static __device__ __noinline__ dd o3_dd(const double3& p, const double3& q, const double3& r, const double3& x, double* perm)
+{
+    return o3_dd_f(p, q, r, x, perm);
 }
 // orient2d(p,q,x) on the projection dropping `drop`; |error| <= 15u^2 perm
 static __device__ __noinline__ dd o2_dd(const double3& p, const double3& q, const double3& x, int drop, double* perm)
@@ -933,6 +955,51 @@ static __device__ __noinline__ bool construct_exact(const double3* pts, const Sy
     return ok;
 }
 
+// Fast path of a constructed point from its two side values sa, sb (with error
+// bounds Ea, Eb): true when every coordinate passed the rounding test.
+__device__ __forceinline__ bool construct_fast(const double3& a, const double3& b, dd sa, dd sb, double Ea, double Eb,
+                                               double3& out)
+{
+    const double u2 = 0x1p-106;
+    dd D = dd_add(sa, dd_neg(sb));
+    double aD = fabs(D.hi);
+    bool fast = aD > 8.0 * (Ea + Eb) && aD > 0x1p-900;
+    double res[3];
+    if (fast) {
+        dd t = dd_div(sa, D);
+        double err_t = 2.0 * (Ea + Eb) / aD * 1.01 + 32.0 * u2;
+        const double* A = &a.x;
+        const double* B = &b.x;
+        for (int k = 0; k < 3 && fast; k++) {
+            dd df = two_diff_dd(B[k], A[k]);
+            dd pr = dd_mul(t, df);
+            dd X = dd_add({A[k], 0.0}, pr);
+            double ad = fabs(df.hi);
+            double err = err_t * ad * 1.01 + 16.0 * u2 * (fabs(A[k]) + ad + fabs(X.hi));
+            if (B[k] == A[k]) {
+                res[k] = A[k];
+                continue;
+            }
+            fast = ziv_round(X, err, &res[k]);
+        }
+    }
+    if (fast) out = make_double3(res[0], res[1], res[2]);
+    return fast;
+}
+
+// The crossing of edge (a, b) with plane(p, q, r), fast path only, on values in
+// registers (inlined): false when the rounding test failed (construct_point
+// then decides exactly).
+__device__ __forceinline__ bool construct_plane_fast(const double3& p, const double3& q, const double3& r,
+                                                     const double3& a, const double3& b, double3& out)
+{
+    const double u2 = 0x1p-106;
+    double pa, pb;
+    const dd sa = o3_dd_f(p, q, r, a, &pa);
+    const dd sb = o3_dd_f(p, q, r, b, &pb);
+    return construct_fast(a, b, sa, sb, 64.0 * u2 * pa, 64.0 * u2 * pb, out);
+}
+
 // returns false only on exact-arithmetic capacity failure
 static __device__ __noinline__ bool construct_point(const double3* pts, const SymPt& s, double3& out, unsigned long long* nexact)
 {
@@ -957,34 +1024,31 @@ static __device__ __noinline__ bool construct_point(const double3* pts, const Sy
         Ea = 32.0 * u2 * pa;
         Eb = 32.0 * u2 * pb;
     }
-    dd D = dd_add(sa, dd_neg(sb));
-    double aD = fabs(D.hi);
-    bool fast = aD > 8.0 * (Ea + Eb) && aD > 0x1p-900;
-    double res[3];
-    if (fast) {
-        dd t = dd_div(sa, D);
-        double err_t = 2.0 * (Ea + Eb) / aD * 1.01 + 32.0 * u2;
-        const double* A = &a.x;
-        const double* B = &b.x;
-        for (int k = 0; k < 3 && fast; k++) {
-            dd df = two_diff_dd(B[k], A[k]);
-            dd pr = dd_mul(t, df);
-            dd X = dd_add({A[k], 0.0}, pr);
-            double ad = fabs(df.hi);
-            double err = err_t * ad * 1.01 + 16.0 * u2 * (fabs(A[k]) + ad + fabs(X.hi));
-            if (B[k] == A[k]) {
-                res[k] = A[k];
-                continue;
-            }
-            fast = ziv_round(X, err, &res[k]);
-        }
-    }
-    if (fast) {
-        out = make_double3(res[0], res[1], res[2]);
-        return true;
-    }
+    if (construct_fast(a, b, sa, sb, Ea, Eb, out)) return true;
     atomicAdd(nexact, 1ull);
     return construct_exact(pts, s, out);
+}
+
+// Symbolic result of a pair from its endpoint pattern (make_pattern): the same
+// points, in the same order, as classify_exact gives for it.
+__device__ __forceinline__ void pattern_result(unsigned pat, TTRes& r)
+{
+    const int o1 = (pat >> 1) & 3, o2 = (pat >> 3) & 3;
+    const unsigned xin = (pat >> 5) & 3, yin = (pat >> 7) & 3;
+    r.n = 0;
+    int k = 0;
+    for (int i = 0; i < 3; i++) {
+        if (i == o1) continue;
+        if ((xin >> k) & 1u) r.pt[r.n++] = sp_plane(o1, i, 3, 4, 5);
+        k++;
+    }
+    k = 0;
+    for (int j = 0; j < 3; j++) {
+        if (j == o2) continue;
+        if ((yin >> k) & 1u) r.pt[r.n++] = sp_plane(3 + o2, 3 + j, 0, 1, 2);
+        k++;
+    }
+    r.kind = r.n == 1 ? KIND_POINT : KIND_SEGMENT;
 }
 
 }  // namespace gi

@@ -357,6 +357,7 @@ struct gi_ctx {
     int32_t* segpair_out = nullptr;
     uint32_t cap_out = 0;
     uint64_t pred_pairs = 0, pred_segs = 0;  // result sizes of the previous call
+    uint32_t fin_backoff = 0;  // calls left before the one-launch finish is tried again after a refusal
     void* order_scratch = nullptr;
     size_t order_scratch_bytes = 0;
     // pinned blocks the results are copied into

@@ -130,10 +130,24 @@ struct Counters {
     unsigned pad10[30];
     unsigned long long t_start;                 // globaltimer at the launch's start (ns)
     unsigned long long level_ns[kLevelTimes];   // globaltimer when level l ended (its barrier completed)
+    // post-traversal launch (k_finish): globaltimer at its start, after the exact
+    // stage, when the last block ended its key phase, after the count scan's
+    // release, and when its last block ended
+    unsigned long long fin_ns[5];
+    unsigned fin_done;  // blocks of k_finish that have ended
+    unsigned pad11[31];
+    unsigned fbar;      // k_finish: blocks arrived at the barrier after its key phase
+    unsigned pad12[31];
+    unsigned frel;      // k_finish: the last block's release (1), or its refusal (2)
+    unsigned fin_over;  // k_finish: keys put on the overflow list (may exceed its capacity)
+    unsigned pad13[30];
 };
 
 constexpr unsigned kOvfFrontier = 1u, kOvfCand = 2u, kOvfRes = 4u, kOvfEsc = 8u;
 constexpr unsigned kErrTimeout = 1u, kErrExactCapacity = 2u;
+// Counters::order_redo: the small-count ordering or the one-launch finish
+// refused; kRedoCrowded: the finish found a key partition over its limit
+constexpr unsigned kRedoCount = 1u, kRedoCrowded = 2u;
 
 // Per-call buffers handed to the kernels.
 struct Bufs {

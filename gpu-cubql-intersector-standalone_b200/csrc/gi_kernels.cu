@@ -1355,21 +1355,22 @@ __device__ __forceinline__ void filter_candidates(const Bufs& B, bool have, cons
     Counters* C = B.cnt;
     int dec = DEC_NO;
     uint32_t ta = 0, tb = 0;
+    unsigned pat = 0;
     if (have) {
         tested++;
         const JobDev& J = B.jobs[c.x];
         double3 P[3], Q[3];
         load_tri<F64>(J.A, J.pa, c.y, P, &ta);
         load_tri<F64>(J.B, J.pb, c.z, Q, &tb);
-        if constexpr (F64) dec = classify_fast<double>(P, Q);
-        else dec = classify_fast<float>(P, Q);
+        if constexpr (F64) dec = classify_fast<double>(P, Q, &pat);
+        else dec = classify_fast<float>(P, Q, &pat);
         decided += (dec != DEC_ESC);
     }
     const bool yes = have && dec == DEC_YES;
     const bool esc = have && dec == DEC_ESC;
     const unsigned pr = warp_append(yes, &C->res);
     if (yes) {
-        if (pr < B.cap_res) B.res[pr] = make_uint4(c.x, ta, tb, 0u);
+        if (pr < B.cap_res) B.res[pr] = make_uint4(c.x, ta, tb, pat);
         else atomicOr(&C->overflow, kOvfRes);
     }
     const unsigned pe = warp_append(esc, &C->esc);
@@ -1865,6 +1866,7 @@ __device__ __forceinline__ void filter_loaded(const Bufs& B, const PubChunk& k, 
 {
     Counters* C = B.cnt;
     int dec = DEC_NO;
+    unsigned pat = 0;
     if (k.have) {
         tested++;
         const JobDev& J = B.jobs[k.c.x];
@@ -1875,15 +1877,15 @@ __device__ __forceinline__ void filter_loaded(const Bufs& B, const PubChunk& k, 
         Q[0] = world_vertex(J.B.verts, k.tb.x, J.pb);
         Q[1] = world_vertex(J.B.verts, k.tb.y, J.pb);
         Q[2] = world_vertex(J.B.verts, k.tb.z, J.pb);
-        if constexpr (F64) dec = classify_fast<double>(P, Q);
-        else dec = classify_fast<float>(P, Q);
+        if constexpr (F64) dec = classify_fast<double>(P, Q, &pat);
+        else dec = classify_fast<float>(P, Q, &pat);
         decided += (dec != DEC_ESC);
     }
     const bool yes = k.have && dec == DEC_YES;
     const bool esc = k.have && dec == DEC_ESC;
     const unsigned pr = warp_append(yes, &C->res);
     if (yes) {
-        if (pr < B.cap_res) B.res[pr] = make_uint4(k.c.x, k.ta.w, k.tb.w, 0u);
+        if (pr < B.cap_res) B.res[pr] = make_uint4(k.c.x, k.ta.w, k.tb.w, pat);
         else atomicOr(&C->overflow, kOvfRes);
     }
     const unsigned pe = warp_append(esc, &C->esc);
@@ -2059,12 +2061,12 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse_levels(Bufs B)
 // ===========================================================================
 // Exact stage and segments
 // ===========================================================================
-__global__ void __launch_bounds__(128) k_exact(Bufs B)
+// Exact stage over the escalated pairs, grid-stride over the threads of the
+// launch (nth a multiple of 32): intersecting pairs are appended to the results.
+__device__ __forceinline__ void exact_stage(const Bufs& B, unsigned gtid, unsigned nth)
 {
     Counters* C = B.cnt;
     const unsigned lane = threadIdx.x & 31;
-    const unsigned gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const unsigned nth = gridDim.x * blockDim.x;
     unsigned ne = ld_cg_u32(&C->esc);
     if (ne > B.cap_esc) ne = B.cap_esc;
     unsigned long long nexact = 0;
@@ -2096,12 +2098,97 @@ __global__ void __launch_bounds__(128) k_exact(Bufs B)
     if (lane == 0 && nexact) atomicAdd(&C->exact_signs, nexact);
 }
 
+__global__ void __launch_bounds__(128) k_exact(Bufs B)
+{
+    exact_stage(B, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
 __device__ __forceinline__ void load_tri_orig(const MeshDev& M, const DevPose& P, uint32_t tri, double3* out)
 {
     const uint32_t* t = M.tris + 3 * (size_t)tri;
     out[0] = world_vertex(M.verts, __ldg(t), P);
     out[1] = world_vertex(M.verts, __ldg(t + 1), P);
     out[2] = world_vertex(M.verts, __ldg(t + 2), P);
+}
+
+// One endpoint of a general-position segment: crossing `sel` of the pattern
+// (0, 1: P's edges from its lone vertex through plane(Q); 2, 3: Q's edges from
+// its lone vertex through plane(P)), fast path on values in registers, the
+// exact construction when the rounding test fails.
+__device__ __forceinline__ bool pattern_point(const double3* pts, int o1, int o2, int sel, double3& q,
+                                              unsigned long long* exact_points)
+{
+    const double3 P0 = pts[0], P1 = pts[1], P2 = pts[2], Q0 = pts[3], Q1 = pts[4], Q2 = pts[5];
+    const bool onP = sel < 2;
+    const int lone = onP ? o1 : o2;
+    // the lone vertex and the other end of the edge (the non-lone vertices in order)
+    const double3 T0 = onP ? P0 : Q0, T1 = onP ? P1 : Q1, T2 = onP ? P2 : Q2;
+    const double3 L = lone == 0 ? T0 : (lone == 1 ? T1 : T2);
+    const int first = (sel & 1) == 0;
+    const double3 E = first ? (lone == 0 ? T1 : T0) : (lone == 2 ? T1 : T2);
+    const double3 U0 = onP ? Q0 : P0, U1 = onP ? Q1 : P1, U2 = onP ? Q2 : P2;
+    if (construct_plane_fast(U0, U1, U2, L, E, q)) return true;
+    const int other = first ? (lone == 0 ? 1 : 0) : (lone == 2 ? 1 : 2);
+    const SymPt sp = onP ? sp_plane(o1, other, 3, 4, 5) : sp_plane(3 + o2, 3 + other, 0, 1, 2);
+    return construct_point(pts, sp, q, exact_points);
+}
+
+// Segments of one result (up to 3, 6 doubles each, at o): their count.  A
+// result that carries an endpoint pattern (decided by the first filter in
+// general position) only needs its two crossings constructed; `per` threads
+// (1 or 2, adjacent lanes) share it, thread `half` constructing endpoints
+// half, half + per, ..  A result without a pattern is classified exactly by
+// its thread with half = 0 alone (the others return 0).
+__device__ __forceinline__ uint32_t result_segments(const Bufs& B, const uint4& rr, double* o, unsigned half = 0u,
+                                                    unsigned per = 1u)
+{
+    Counters* C = B.cnt;
+    const JobDev& J = B.jobs[B.njobs == 1 ? 0u : rr.x];  // one job: its loads need not wait for rr
+    double3 pts[6];
+    load_tri_orig(J.A, J.pa, rr.y, pts);
+    load_tri_orig(J.B, J.pb, rr.z, pts + 3);
+    if (rr.w & kPatValid) {
+        const int o1 = (rr.w >> 1) & 3, o2 = (rr.w >> 3) & 3;
+        unsigned m = ((rr.w >> 5) & 3u) | (((rr.w >> 7) & 3u) << 2);
+        const int s0 = __ffs(m) - 1;
+        m &= m - 1u;
+        const int s1 = m ? __ffs(m) - 1 : s0;
+        for (unsigned k = half; k < 2u; k += per) {
+            double3 q;
+            if (!pattern_point(pts, o1, o2, k ? s1 : s0, q, &C->exact_points)) atomicOr(&C->err, kErrExactCapacity);
+            o[3 * k] = q.x;
+            o[3 * k + 1] = q.y;
+            o[3 * k + 2] = q.z;
+        }
+        return 1;
+    }
+    if (half) return 0;
+    ExactSigns S{&C->err, 0ull};
+    TTRes r;
+    classify_exact(pts, r, S);
+    double3 q[3];
+    if (r.kind == KIND_POINT || r.kind == KIND_SEGMENT || r.kind == KIND_TRIANGLE) {
+        for (int k = 0; k < r.n && k < 3; k++)
+            if (!construct_point(pts, r.pt[k], q[k], &C->exact_points)) atomicOr(&C->err, kErrExactCapacity);
+        if (r.kind == KIND_POINT) {
+            double v[6] = {q[0].x, q[0].y, q[0].z, q[0].x, q[0].y, q[0].z};
+            for (int k = 0; k < 6; k++) o[k] = v[k];
+            return 1;
+        }
+        if (r.kind == KIND_SEGMENT) {
+            double v[6] = {q[0].x, q[0].y, q[0].z, q[1].x, q[1].y, q[1].z};
+            for (int k = 0; k < 6; k++) o[k] = v[k];
+            return 1;
+        }
+        for (int e = 0; e < 3; e++) {
+            const double3& u = q[e];
+            const double3& w = q[(e + 1) % 3];
+            double v[6] = {u.x, u.y, u.z, w.x, w.y, w.z};
+            for (int k = 0; k < 6; k++) o[6 * e + k] = v[k];
+        }
+        return 3;
+    }
+    return 0;
 }
 
 __global__ void __launch_bounds__(128) k_segments(Bufs B, double* __restrict__ segs, uint32_t* __restrict__ nseg)
@@ -2112,41 +2199,7 @@ __global__ void __launch_bounds__(128) k_segments(Bufs B, double* __restrict__ s
     if (ld_cg_u32(&C->overflow)) return;
     unsigned nres = ld_cg_u32(&C->res);
     if (nres > B.cap_res) nres = B.cap_res;
-    for (unsigned i = gtid; i < nres; i += nth) {
-        uint4 rr = __ldcg(B.res + i);
-        const JobDev& J = B.jobs[rr.x];
-        double3 pts[6];
-        load_tri_orig(J.A, J.pa, rr.y, pts);
-        load_tri_orig(J.B, J.pb, rr.z, pts + 3);
-        ExactSigns S{&C->err, 0ull};
-        TTRes r;
-        classify_exact(pts, r, S);
-        double3 q[3];
-        uint32_t ns = 0;
-        if (r.kind == KIND_POINT || r.kind == KIND_SEGMENT || r.kind == KIND_TRIANGLE) {
-            for (int k = 0; k < r.n && k < 3; k++)
-                if (!construct_point(pts, r.pt[k], q[k], &C->exact_points)) atomicOr(&C->err, kErrExactCapacity);
-            double* o = segs + 18 * (size_t)i;
-            if (r.kind == KIND_POINT) {
-                double v[6] = {q[0].x, q[0].y, q[0].z, q[0].x, q[0].y, q[0].z};
-                for (int k = 0; k < 6; k++) o[k] = v[k];
-                ns = 1;
-            } else if (r.kind == KIND_SEGMENT) {
-                double v[6] = {q[0].x, q[0].y, q[0].z, q[1].x, q[1].y, q[1].z};
-                for (int k = 0; k < 6; k++) o[k] = v[k];
-                ns = 1;
-            } else {
-                for (int e = 0; e < 3; e++) {
-                    const double3& u = q[e];
-                    const double3& w = q[(e + 1) % 3];
-                    double v[6] = {u.x, u.y, u.z, w.x, w.y, w.z};
-                    for (int k = 0; k < 6; k++) o[6 * e + k] = v[k];
-                }
-                ns = 3;
-            }
-        }
-        nseg[i] = ns;
-    }
+    for (unsigned i = gtid; i < nres; i += nth) nseg[i] = result_segments(B, __ldcg(B.res + i), segs + 18 * (size_t)i);
 }
 
 // ===========================================================================
@@ -2340,8 +2393,8 @@ size_t order_scratch_bytes(uint32_t cap, int passes)
     size_t ntiles = (cap + kOsTile - 1) / kOsTile;
     return 2 * sizeof(unsigned long long) * (size_t)cap + 2 * sizeof(uint32_t) * (size_t)cap +
            sizeof(uint32_t) * ((size_t)(passes + 1) * ntiles * 256 + 2 * kOsMaxPasses * 256 + kOsMaxPasses + 2 +
-                               (size_t)cap / kOsGatherTile + 1 + kOrderSmallBlocks) +
-           8192;
+                               (size_t)cap / kOsGatherTile + 1 + kOrderSmallBlocks + 5 * kFinParts + 2) +
+           (sizeof(unsigned long long) + sizeof(uint32_t)) * ((size_t)kFinParts * kFinBucket + kFinOverflow) + 8192;
 }
 
 OrderBufs make_order_bufs(void* scratch, uint32_t cap, int bits_a, int bits_b, int bits_job)
@@ -2369,6 +2422,12 @@ OrderBufs make_order_bufs(void* scratch, uint32_t cap, int bits_a, int bits_b, i
     O.base = (uint32_t*)take(sizeof(uint32_t) * kOsMaxPasses * 256);
     O.tile_ctr = (uint32_t*)take(sizeof(uint32_t) * (kOsMaxPasses + 2));
     O.tile_tot = (uint32_t*)take(sizeof(uint32_t) * kOrderSmallBlocks);
+    O.fin = (uint32_t*)take(sizeof(uint32_t) * 2 * kFinParts);
+    O.fin_off = (uint32_t*)take(sizeof(uint32_t) * (3 * kFinParts + 2));
+    O.fin_bkey = (unsigned long long*)take(sizeof(unsigned long long) * kFinParts * kFinBucket);
+    O.fin_bval = (uint32_t*)take(sizeof(uint32_t) * kFinParts * kFinBucket);
+    O.fin_okey = (unsigned long long*)take(sizeof(unsigned long long) * kFinOverflow);
+    O.fin_oval = (uint32_t*)take(sizeof(uint32_t) * kFinOverflow);
     return O;
 }
 
@@ -2450,7 +2509,7 @@ __global__ void __launch_bounds__(kOrderSmallThreads, 1)
     Counters* C = B.cnt;
     const unsigned n = res_count(B);
     if (n > kOrderSmallMax) {  // same decision in every block: no barrier is reached
-        if (blockIdx.x == 0 && threadIdx.x == 0) C->order_redo = 1u;
+        if (blockIdx.x == 0 && threadIdx.x == 0) C->order_redo = kRedoCount;
         return;
     }
     if (threadIdx.x == 0) s_ok = 1u;
@@ -2660,6 +2719,411 @@ cudaError_t launch_order_small_phases(const Bufs& b, const OrderBufs& O, bool so
 }
 
 // ===========================================================================
+// Post-traversal work of a call in one cooperative launch (sorted output, up to
+// kFinMax results, keys of at most 63 bits):
+//   phase 0  the exact stage on the escalated pairs (only when there are any:
+//            the count is final at launch, so every block decides alike);
+//   phase 1  one result per thread (results spread over all blocks): its key
+//            goes into its partition (the key's top kFinPartBits bits) at the
+//            slot one atomic on the partition's count returns, in a fixed
+//            bucket of kFinBucket slots or, beyond it, one overflow list; then
+//            its segments, whose count the partition's segment count gains;
+//   barrier  the block that arrives last scans the partition counts into key
+//            and segment offsets and lists the partitions over kFinBucket keys
+//            before it releases the others;
+//   phase 2  in a partition of up to kFinBucket keys, each result's thread
+//            ranks its key against the bucket (the keys are unique, so the rank
+//            is the number of smaller keys) and writes its pair, job and
+//            segments at their final positions; a larger partition is one
+//            block's (its bucket and its overflow entries, bitonic sort in
+//            shared memory).
+// Every wait is bounded.  Over kFinMax results (or more results than threads),
+// a partition over kFinBig keys or a full overflow list make the kernel refuse
+// (Counters::order_redo, decided alike in every block).
+// ===========================================================================
+constexpr int kFinThreads = 256;
+constexpr int kFinWarps = kFinThreads / 32;
+// dynamic shared memory: a big partition's keys and values, or (in the last
+// block of the key phase) the partition counts
+constexpr size_t kFinDyn = (sizeof(unsigned long long) + sizeof(uint32_t)) * kFinBig > 2 * sizeof(uint32_t) * kFinParts
+                               ? (sizeof(unsigned long long) + sizeof(uint32_t)) * kFinBig
+                               : 2 * sizeof(uint32_t) * kFinParts;
+static_assert(kFinParts % (32 * kFinWarps) == 0, "whole rows of 32 partitions per warp");
+static_assert(kFinBucket % 8 == 0, "a bucket is read 8 keys at a time");
+static_assert(kFinMax <= (1u << 30), "a bucket value holds the result index below bit 30");
+
+// One result at its final position: pair and job from the key, its segments
+// copied from the scratch, each segment's pair index set.
+__device__ __forceinline__ void fin_place(const OrderBufs& O, const FinArgs& F, unsigned long long key, unsigned idx,
+                                          unsigned pos, unsigned ns, unsigned so)
+{
+    // (positions stay inside the arrays even after a spent barrier wait)
+    if (pos >= F.cap || (size_t)so + ns > 3 * (size_t)F.cap) return;
+    const unsigned long long ma = (1ull << O.bits_a) - 1ull, mb = (1ull << O.bits_b) - 1ull;
+    F.pairs_out[2 * (size_t)pos] = (int32_t)((key >> O.bits_b) & ma);
+    F.pairs_out[2 * (size_t)pos + 1] = (int32_t)(key & mb);
+    F.job_out[pos] = (uint32_t)(key >> (O.bits_a + O.bits_b));
+    for (unsigned e = 0; e < ns; e++) {
+        const double2* sp = reinterpret_cast<const double2*>(F.segs + 18 * (size_t)idx + 6 * e);
+        double2* dp = reinterpret_cast<double2*>(F.segs_out + 6 * (size_t)(so + e));
+        dp[0] = __ldcg(sp);
+        dp[1] = __ldcg(sp + 1);
+        dp[2] = __ldcg(sp + 2);
+        F.segpair_out[so + e] = (int32_t)pos;
+    }
+}
+
+__device__ __forceinline__ void fin_stamp(Counters* C, int k)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) C->fin_ns[k] = globaltimer_ns();
+}
+
+// Block end: the last block to end stamps the launch's end.
+__device__ __forceinline__ void fin_end(Counters* C)
+{
+    __syncthreads();
+    if (threadIdx.x == 0 && atomicAdd(&C->fin_done, 1u) == gridDim.x - 1u) C->fin_ns[4] = globaltimer_ns();
+}
+
+// Layout of O.fin_off: key offsets (kFinParts + 1), segment offsets (kFinParts),
+// the number of big partitions, then their ids.
+constexpr int kFinSoff = kFinParts + 1;
+constexpr int kFinNbig = 2 * kFinParts + 1;
+constexpr int kFinBigIds = 2 * kFinParts + 2;
+
+// Run by the block that arrives last at the phase-1 barrier: the exclusive
+// scans of the partition key and segment counts into O.fin_off (one warp per
+// 512 partitions, 32 at a time, coalesced), the list of partitions over
+// kFinBucket keys, the counts cleared for the next call, and the refusal
+// decided.  Returns the refusal code (0: none).
+__device__ __forceinline__ unsigned fin_scan_counts(const OrderBufs& O, Counters* C, uint32_t* sw, unsigned* s_nbig,
+                                                    uint32_t* sk)
+{
+    constexpr int kSeg = kFinParts / kFinWarps;  // partitions per warp
+    constexpr int kIt = kSeg / 32;
+    const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    uint32_t* const kcount = O.fin;
+    uint32_t* const scount = O.fin + kFinParts;
+    uint32_t* const koff = O.fin_off;
+    uint32_t* const soff = O.fin_off + kFinSoff;
+    const unsigned over = ld_cg_u32(&C->fin_over);
+    // all counts into shared memory first (every load in flight at once), then
+    // the scan reads them there
+    uint32_t* const ss = sk + kFinParts;
+#pragma unroll
+    for (int it = 0; it < kFinParts / kFinThreads; it++) {
+        const unsigned q = it * kFinThreads + tid;
+        sk[q] = __ldcg(kcount + q);
+        ss[q] = __ldcg(scount + q);
+    }
+    __syncthreads();
+    const unsigned w0 = warp * kSeg;
+    uint32_t kc[kIt], sc[kIt];
+#pragma unroll
+    for (int it = 0; it < kIt; it++) {
+        kc[it] = sk[w0 + 32 * it + lane];
+        sc[it] = ss[w0 + 32 * it + lane];
+    }
+    uint32_t tk = 0, ts = 0;
+    bool too_big = false;
+#pragma unroll
+    for (int it = 0; it < kIt; it++) {
+        tk += kc[it];
+        ts += sc[it];
+        too_big |= kc[it] > (uint32_t)kFinBig;
+    }
+    tk = __reduce_add_sync(0xffffffffu, tk);
+    ts = __reduce_add_sync(0xffffffffu, ts);
+    const bool any_big = __any_sync(0xffffffffu, too_big);
+    if (lane == 0) {
+        sw[warp] = tk;
+        sw[kFinWarps + warp] = ts;
+        sw[2 * kFinWarps + warp] = any_big ? 1u : 0u;
+    }
+    __syncthreads();
+    unsigned kb = 0, sb = 0, ktot = 0, stot = 0, refuse = 0;
+#pragma unroll
+    for (int w = 0; w < kFinWarps; w++) {
+        const unsigned a = sw[w], b = sw[kFinWarps + w];
+        if ((unsigned)w < warp) {
+            kb += a;
+            sb += b;
+        }
+        ktot += a;
+        stot += b;
+        refuse |= sw[2 * kFinWarps + w];
+    }
+#pragma unroll
+    for (int it = 0; it < kIt; it++) {
+        const unsigned p = w0 + 32 * it + lane;
+        unsigned xk = kc[it], xs = sc[it];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned yk = __shfl_up_sync(0xffffffffu, xk, o), ys = __shfl_up_sync(0xffffffffu, xs, o);
+            if (lane >= (unsigned)o) {
+                xk += yk;
+                xs += ys;
+            }
+        }
+        koff[p] = kb + xk - kc[it];
+        soff[p] = sb + xs - sc[it];
+        kb += __shfl_sync(0xffffffffu, xk, 31);
+        sb += __shfl_sync(0xffffffffu, xs, 31);
+        kcount[p] = 0u;
+        scount[p] = 0u;
+        if (kc[it] > (uint32_t)kFinBucket) {
+            const unsigned at = atomicAdd(s_nbig, 1u);
+            if (at < (unsigned)kFinParts) O.fin_off[kFinBigIds + at] = p;
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        koff[kFinParts] = ktot;
+        O.fin_off[kFinNbig] = *s_nbig;
+        C->nseg = stot;
+    }
+    if (refuse || over > (unsigned)kFinOverflow) return kRedoCrowded;
+    return 0u;
+}
+
+__global__ void __launch_bounds__(kFinThreads, 2) k_finish(Bufs B, OrderBufs O, FinArgs F)
+{
+    extern __shared__ unsigned long long fin_dyn[];  // a big partition: kFinBig keys, then kFinBig values
+    __shared__ uint32_t sw[33];
+    __shared__ unsigned s_ok, s_last, s_redo, s_fill, s_nbig;
+    Counters* C = B.cnt;
+    const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const unsigned gtid = blockIdx.x * kFinThreads + tid, nth = gridDim.x * kFinThreads;
+    if (tid == 0) {
+        s_ok = 1u;
+        s_nbig = 0u;
+    }
+    fin_stamp(C, 0);
+    if (ld_cg_u32(&C->overflow)) {  // final at launch: the call reruns with larger buffers
+        fin_end(C);
+        return;
+    }
+    // ---- phase 0: exact stage ----
+    if (ld_cg_u32(&C->esc)) {
+        exact_stage(B, gtid, nth);
+        grid_barrier(&C->obar, 1u, &C->err, &s_ok);
+        if (ld_cg_u32(&C->overflow)) {  // read after the barrier: alike in every block
+            fin_end(C);
+            return;
+        }
+    }
+    fin_stamp(C, 1);
+    const unsigned n = ld_cg_u32(&C->res);
+    if (n > kFinMax || n > nth) {  // one result per thread at most
+        if (blockIdx.x == 0 && tid == 0) C->order_redo = kRedoCount;
+        fin_end(C);
+        return;
+    }
+    // ---- phase 1: this thread's result: its key into its partition, its segments ----
+    // thread slots go to the warps of different blocks first (warp w of block b
+    // holds slots 32 (b + w G) ..), so that a small result spreads over every
+    // SM; when there are slots enough, two adjacent slots share a result (its
+    // two endpoints, FP64 work that one warp per SM sub-partition would issue
+    // too slowly), the first of them owning its key
+    const unsigned g = 32u * (blockIdx.x + gridDim.x * warp) + lane;
+    const unsigned per = 2u * n <= nth ? 2u : 1u;
+    const unsigned i = g / per, half = g % per;
+    const bool mine = i < n && half == 0u;
+    unsigned long long key = 0;
+    unsigned p = 0, ns = 0, slot = 0;
+    if (i < n) {
+        const uint4 rr = __ldcg(B.res + i);
+        if (mine) {
+            key = order_key(rr, O);
+            p = (unsigned)(key >> F.shift);
+            slot = atomicAdd(O.fin + p, 1u);  // waited for after the segments
+        }
+        if (F.want_segments) ns = result_segments(B, rr, F.segs + 18 * (size_t)i, half, per);
+    }
+    if (mine) {
+        if (ns) atomicAdd(O.fin + kFinParts + p, ns);
+        const uint32_t v = i | (ns << 30);
+        if (slot < (unsigned)kFinBucket) {
+            O.fin_bkey[p * kFinBucket + slot] = key;
+            O.fin_bval[p * kFinBucket + slot] = v;
+        } else {
+            const unsigned o = atomicAdd(&C->fin_over, 1u);
+            if (o < (unsigned)kFinOverflow) {
+                O.fin_okey[o] = key;
+                O.fin_oval[o] = v;
+            }
+        }
+    }
+    // ---- barrier: the last block to arrive scans the counts, then releases ----
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        s_last = atomicAdd(&C->fbar, 1u) == gridDim.x - 1u ? 1u : 0u;
+        __threadfence();
+    }
+    __syncthreads();
+    if (s_last) {
+        if (tid == 0) C->fin_ns[2] = globaltimer_ns();
+        const unsigned r = fin_scan_counts(O, C, sw, &s_nbig, reinterpret_cast<uint32_t*>(fin_dyn));
+        if (tid == 0) {
+            if (r) C->order_redo = r;
+            s_redo = r;
+            __threadfence();
+            st_release_u32(&C->frel, r ? 2u : 1u);
+        }
+    } else if (tid == 0) {
+        unsigned v = ld_acq(&C->frel);
+        unsigned long long spins = 0;
+        while (v == 0u) {
+            if (++spins > kLookbackSpins) {
+                atomicOr(&C->err, kErrTimeout);
+                v = 2u;
+                break;
+            }
+            __nanosleep(32);
+            v = ld_acq(&C->frel);
+        }
+        s_redo = v == 2u ? 1u : 0u;
+    }
+    __syncthreads();
+    if (s_redo) {
+        fin_end(C);
+        return;
+    }
+    fin_stamp(C, 3);
+    // ---- phase 2: each result ranks itself in its partition's bucket ----
+    const uint32_t* const koff = O.fin_off;
+    const uint32_t* const soff = O.fin_off + kFinSoff;
+    if (mine) {
+        // the offsets, the bucket's first 8 keys and the segments, all at once
+        const unsigned base = __ldcg(koff + p), end = __ldcg(koff + p + 1), so = __ldcg(soff + p);
+        const ulonglong2* bk2 = reinterpret_cast<const ulonglong2*>(O.fin_bkey + p * kFinBucket);
+        const uint4* bv4 = reinterpret_cast<const uint4*>(O.fin_bval + p * kFinBucket);
+        ulonglong2 k2[4];
+        uint4 v4[2];
+#pragma unroll
+        for (int q = 0; q < 4; q++) k2[q] = __ldcg(bk2 + q);
+        v4[0] = __ldcg(bv4);
+        v4[1] = __ldcg(bv4 + 1);
+        double2 sg[9];
+#pragma unroll
+        for (int e = 0; e < 9; e++)
+            if (e < 3 * (int)ns) sg[e] = __ldcg(reinterpret_cast<const double2*>(F.segs + 18 * (size_t)i) + e);
+        const unsigned m = end - base;
+        if (m <= (unsigned)kFinBucket) {
+            unsigned rank = 0, pre = 0;
+            const unsigned long long kk[8] = {k2[0].x, k2[0].y, k2[1].x, k2[1].y, k2[2].x, k2[2].y, k2[3].x, k2[3].y};
+            const uint32_t vv[8] = {v4[0].x, v4[0].y, v4[0].z, v4[0].w, v4[1].x, v4[1].y, v4[1].z, v4[1].w};
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+                if ((unsigned)j < m && kk[j] < key) {
+                    rank++;
+                    pre += vv[j] >> 30;
+                }
+            for (unsigned j = 8; j < m; j++) {
+                const unsigned long long kj = __ldcg(O.fin_bkey + p * kFinBucket + j);
+                if (kj < key) {
+                    rank++;
+                    pre += __ldcg(O.fin_bval + p * kFinBucket + j) >> 30;
+                }
+            }
+            const unsigned pos = base + rank, s0 = so + pre;
+            if (pos < F.cap && (size_t)s0 + ns <= 3 * (size_t)F.cap) {
+                const unsigned long long ma = (1ull << O.bits_a) - 1ull, mb = (1ull << O.bits_b) - 1ull;
+                F.pairs_out[2 * (size_t)pos] = (int32_t)((key >> O.bits_b) & ma);
+                F.pairs_out[2 * (size_t)pos + 1] = (int32_t)(key & mb);
+                F.job_out[pos] = (uint32_t)(key >> (O.bits_a + O.bits_b));
+                double2* dp = reinterpret_cast<double2*>(F.segs_out + 6 * (size_t)s0);
+#pragma unroll
+                for (int e = 0; e < 9; e++)
+                    if (e < 3 * (int)ns) dp[e] = sg[e];
+                for (unsigned e = 0; e < ns; e++) F.segpair_out[s0 + e] = (int32_t)pos;
+            }
+        }
+    }
+    // partitions over kFinBucket keys (listed by the scan): one block each,
+    // whose threads gather its bucket and its overflow entries into shared
+    // memory and sort them there (bitonic)
+    const unsigned nbig = min(__ldcg(O.fin_off + kFinNbig), (unsigned)kFinParts);
+    unsigned long long* bk = fin_dyn;
+    uint32_t* bv = reinterpret_cast<uint32_t*>(fin_dyn + kFinBig);
+    for (unsigned q = blockIdx.x; q < nbig; q += gridDim.x) {
+        const unsigned pb = __ldcg(O.fin_off + kFinBigIds + q);
+        if (pb >= (unsigned)kFinParts) continue;  // block-uniform
+        const unsigned base = __ldcg(koff + pb), m = __ldcg(koff + pb + 1) - base;
+        if (m <= (unsigned)kFinBucket || m > (unsigned)kFinBig) continue;
+        unsigned mp = 2u * kFinBucket;
+        while (mp < m) mp <<= 1;
+        __syncthreads();  // the previous partition's reads are done
+        for (unsigned t = tid; t < mp; t += kFinThreads) {
+            bk[t] = ~0ull;  // padding sorts last
+            bv[t] = 0u;
+        }
+        if (tid == 0) s_fill = kFinBucket;
+        __syncthreads();
+        if (tid < (unsigned)kFinBucket) {
+            bk[tid] = __ldcg(O.fin_bkey + pb * kFinBucket + tid);
+            bv[tid] = __ldcg(O.fin_bval + pb * kFinBucket + tid);
+        }
+        const unsigned nover = min(ld_cg_u32(&C->fin_over), (unsigned)kFinOverflow);
+        for (unsigned t = tid; t < nover; t += kFinThreads) {
+            const unsigned long long kt = __ldcg(O.fin_okey + t);
+            if ((unsigned)(kt >> F.shift) == pb) {
+                const unsigned at = atomicAdd(&s_fill, 1u);
+                if (at < mp) {
+                    bk[at] = kt;
+                    bv[at] = __ldcg(O.fin_oval + t);
+                }
+            }
+        }
+        __syncthreads();
+        for (unsigned k = 2; k <= mp; k <<= 1)
+            for (unsigned j = k >> 1; j > 0; j >>= 1) {
+                for (unsigned t = tid; t < mp; t += kFinThreads) {
+                    const unsigned u = t ^ j;
+                    if (u > t) {
+                        const unsigned long long x = bk[t], y = bk[u];
+                        if ((x > y) == ((t & k) == 0u)) {
+                            bk[t] = y;
+                            bk[u] = x;
+                            const uint32_t w = bv[t];
+                            bv[t] = bv[u];
+                            bv[u] = w;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        unsigned run = __ldcg(soff + pb);
+        for (unsigned c0 = 0; c0 < m; c0 += kFinThreads) {
+            const unsigned k = c0 + tid;
+            const bool have = k < m;
+            const uint32_t v = have ? bv[k] : 0u;
+            const unsigned nsk = v >> 30;
+            unsigned idx = v & ((1u << 30) - 1u);
+            if (idx >= n) idx = 0u;
+            unsigned tot;
+            const unsigned ex = block_exclusive_scan(nsk, sw, &tot);
+            if (have) fin_place(O, F, bk[k], idx, base + k, nsk, run + ex);
+            run += tot;
+        }
+    }
+    fin_end(C);
+}
+
+cudaError_t launch_finish(const Bufs& b, const OrderBufs& O, const FinArgs& F, const LaunchCfg& cfg, cudaStream_t st)
+{
+    Bufs bb = b;
+    OrderBufs oo = O;
+    FinArgs ff = F;
+    void* args[] = {&bb, &oo, &ff};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_finish, dim3(cfg.fin_per_sm * cfg.sms),
+                                                dim3(kFinThreads), args, kFinDyn, st);
+    note_launches(1);
+    return e;
+}
+
+// ===========================================================================
 // Launchers
 // ===========================================================================
 
@@ -2672,6 +3136,9 @@ cudaError_t query_launch(int device, LaunchCfg* cfg)
     GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nl[0], k_traverse_levels<false>, kTravThreads, 0));
     GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nl[1], k_traverse_levels<true>, kTravThreads, 0));
     for (int a = 0; a < 2; a++) cfg->levels_per_sm[a] = nl[a] < 1 ? 1 : (nl[a] > 2 ? 2 : nl[a]);
+    int nf = 0;
+    GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nf, k_finish, kFinThreads, kFinDyn));
+    cfg->fin_per_sm = nf < 1 ? 1 : (nf > 2 ? 2 : nf);
     GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n[0][0], k_traverse<false, false>, kTravThreads, 0));
     GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n[0][1], k_traverse<false, true>, kTravThreads, 0));
     GI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n[1][0], k_traverse<true, false>, kTravThreads, 0));

@@ -50,6 +50,7 @@ struct LaunchCfg {
     int sms = 0;
     int trav_per_sm[2][2] = {};  // resident traversal blocks per SM, [FP64][quad form]
     int levels_per_sm[2] = {};   // resident blocks of the level-synchronous traversal (at most 2), [FP64]
+    int fin_per_sm = 1;          // resident blocks of the post-traversal launch (at most 2)
     int trav_threads = 256;
 };
 
@@ -94,6 +95,14 @@ struct OrderBufs {
     uint32_t* base;      // kOsMaxPasses x 256
     uint32_t* tile_ctr;  // kOsMaxPasses + 2 (per pass, the gather, the histogram blocks)
     uint32_t* tile_tot;  // kOrderSmallBlocks: segment totals per run (small-count path)
+    // one-launch finish (k_finish)
+    uint32_t* fin;       // 2 x kFinParts: keys and segments per partition (zero between calls)
+    uint32_t* fin_off;   // kFinParts + 1 key offsets, kFinParts segment offsets, the number of
+                         // partitions over kFinBucket keys, their ids (kFinParts at most)
+    unsigned long long* fin_bkey;  // kFinParts x kFinBucket: each partition's first keys
+    uint32_t* fin_bval;            // ... and their result index | segment count << 30
+    unsigned long long* fin_okey;  // kFinOverflow: the keys beyond a bucket
+    uint32_t* fin_oval;
     uint32_t ntiles_cap;
     int passes;
     int bits_a, bits_b;
@@ -121,6 +130,31 @@ constexpr unsigned kOrderRank = 1u, kOrderPlace = 2u;
 cudaError_t launch_order_small_phases(const Bufs& b, const OrderBufs& O, bool sort, const double* segs,
                                       const uint32_t* nseg, int32_t* pairs_out, uint32_t* job_out, double* segs_out,
                                       int32_t* segpair_out, bool want_segments, unsigned phases, cudaStream_t st);
+// Everything after the traversal in one cooperative launch, for sorted output
+// of up to kFinMax results with keys of at most 63 bits: the exact stage (when
+// pairs were escalated), the segments, and the ordering by partitions of the
+// key's top kFinPartBits bits (one warp ranks a partition of up to kFinBucket
+// keys, one block a larger one, up to kFinBig).  A call over those limits
+// makes the kernel set only Counters::order_redo; the caller then reruns on
+// the general path (launch_exact, launch_segments, launch_order_gather).
+constexpr int kFinPartBits = 12;
+constexpr int kFinParts = 1 << kFinPartBits;
+constexpr int kFinBucket = 32;
+constexpr int kFinOverflow = 1 << 14;
+constexpr int kFinBig = 2048;
+constexpr uint32_t kFinMax = 1u << 16;
+struct FinArgs {
+    double* segs;       // per result: up to 3 segments (scratch)
+    int32_t* pairs_out;
+    uint32_t* job_out;
+    double* segs_out;
+    int32_t* segpair_out;
+    uint32_t cap;       // results the output arrays hold (segments: 3 per result)
+    int want_segments;
+    int shift;          // partition of a key = key >> shift
+};
+cudaError_t launch_finish(const Bufs& b, const OrderBufs& O, const FinArgs& F, const LaunchCfg& cfg, cudaStream_t st);
+
 // Number of kernels launched by the launchers of this library (monotonic).
 unsigned long long launch_count();
 void note_launches(unsigned n);

@@ -99,11 +99,15 @@ class Stats(ctypes.Structure):
                 ("ms_traverse", ctypes.c_double), ("ms_exact", ctypes.c_double), ("ms_segments", ctypes.c_double),
                 ("ms_sort", ctypes.c_double), ("ms_total", ctypes.c_double),
                 ("level_times", ctypes.c_uint32), ("reserved2", ctypes.c_uint32),
-                ("level_end_ms", ctypes.c_double * 32)]
+                ("level_end_ms", ctypes.c_double * 32),
+                ("finish_phases", ctypes.c_uint32), ("reserved3", ctypes.c_uint32),
+                ("finish_ms", ctypes.c_double * 4)]
 
     def as_dict(self):
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("level_end_ms", "reserved2")}
+        d = {k: getattr(self, k) for k, _ in self._fields_
+             if k not in ("level_end_ms", "reserved2", "finish_ms", "reserved3")}
         d["level_end_ms"] = [self.level_end_ms[i] for i in range(min(self.level_times, 32))]
+        d["finish_ms"] = [self.finish_ms[i] for i in range(min(self.finish_phases, 4))]
         return d
 
 

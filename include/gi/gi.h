@@ -144,7 +144,10 @@ typedef struct {
     double ms_exact;                  /* device time: FP64 / exact stage */
     double ms_segments;               /* device time: segment construction */
     double ms_sort;                   /* device time: output ordering (the part after segment construction
-                                         ends; ranking overlaps the segments) */
+                                         ends; ranking overlaps the segments).  With the one-launch
+                                         finish (finish_phases = 4), ms_exact and ms_segments are its
+                                         phases' own spans and ms_sort the rest of the call after the
+                                         traversal, launch included */
     double ms_total;                  /* device time of the whole call */
     /* level-synchronous traversal only (else level_times = 0): level_end_ms[l]
      * is the time from the traversal's start to the end of level l (level 0:
@@ -153,6 +156,14 @@ typedef struct {
     uint32_t level_times;
     uint32_t reserved2;
     double level_end_ms[32];
+    /* one-launch finish after the traversal (sorted output of a small result;
+     * else finish_phases = 0): finish_ms[k] is the time from the launch's start
+     * to the end of its exact phase (k = 0), of its key and segment phase (1:
+     * the last block's arrival), of the count scan (2: the release of the
+     * others), and of its last block (3) */
+    uint32_t finish_phases;
+    uint32_t reserved3;
+    double finish_ms[4];
 } gi_stats;
 
 /* Batched job: one mesh pair with its poses. */

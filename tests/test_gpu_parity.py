@@ -169,6 +169,45 @@ def test_ordering_paths_and_redo(gi, oc):
         B.release()
 
 
+def _crowded_pair(n_grid, corner):
+    """A: 2,048 triangles, the first a large triangle in the plane z = 0, the
+    others tiny and far away; B: an n_grid x n_grid unit grid at z = 0.  Every
+    result has a = 0, so the keys crowd into the partitions of the first a."""
+    big = [[0.25, 0.25, 0.0], [corner + 0.25, 0.25, 0.0], [0.25, corner + 0.25, 0.0]]
+    tiny = []
+    for k in range(2047):
+        x = 1000.0 + 3.0 * k
+        tiny += [[x, 0.0, 500.0], [x + 1.0, 0.0, 500.0], [x, 1.0, 500.0]]
+    vA = np.array(big + tiny, dtype=np.float64)
+    tA = np.arange(vA.shape[0], dtype=np.uint32).reshape(-1, 3)
+    from gpuintersector import meshgen as mg
+
+    vB, tB = mg.grid_mesh(n=n_grid, cell=1.0)
+    return dict(vA=vA, tA=tA, vB=vB, tB=tB, poseA=None, poseB=None)
+
+
+def test_finish_block_partitions_and_crowded_refusal(gi, oc):
+    """The one-launch finish with partitions above 32 keys (sorted by a whole
+    block), with escalated coplanar pairs (its exact phase), and with a
+    partition above its limit (refused, rerun on the general path, kept off the
+    finish for the next calls).  All equal the oracle, segments included."""
+    with gi.Context(0) as c:
+        mid = _crowded_pair(64, 18.0)       # a few hundred keys per partition
+        r, ref = run_cfg(c, gi, oc, mid)
+        assert 64 < len(ref["pairs"]) < 4096
+        assert r.stats["escalated"] > 0
+        assert r.stats["launches"] == 2      # traversal + the finish
+        assert_same(r, ref)
+        crowded = _crowded_pair(128, 88.0)  # ~15 k keys, most in one partition
+        r, ref = run_cfg(c, gi, oc, crowded)
+        assert 4096 < len(ref["pairs"]) < 24000
+        assert r.stats["launches"] > 2       # refused, rerun on the general path
+        assert_same(r, ref)
+        r, ref = run_cfg(c, gi, oc, mid)     # the next call stays off the finish
+        assert r.stats["launches"] > 2
+        assert_same(r, ref)
+
+
 @pytest.mark.parametrize("shape", list(range(8)))
 def test_every_traversal_shape(gi, oc, shape):
     """Each traversal shape the autotuner may pick (work queue or level-synchronous
