@@ -183,48 +183,61 @@ __device__ __forceinline__ unsigned make_pattern(int o1, int o2, unsigned xin, u
 // First stage: decides the general-position case (every vertex strictly off the
 // other triangle's plane) with filtered signs; everything else escalates.  For
 // an intersecting pair, *pat receives its endpoint pattern (make_pattern).
-template <class T>
-static __device__ int classify_fast(const double3* P, const double3* Q, unsigned* pat = nullptr)
+// The vertex of three that `i` names (0, 1, 2), by selects (no indexed array).
+__device__ __forceinline__ double3 sel3(int i, const double3& a, const double3& b, const double3& c)
 {
-    Plane<T> pp = make_plane<T>(vdiff<T>(P[1], P[0]), vdiff<T>(P[2], P[0]));
+    return i == 0 ? a : (i == 1 ? b : c);
+}
+
+// Index of the vertex whose sign differs from the other two (signs not all equal).
+__device__ __forceinline__ int lone3(int s0, int s1, int s2)
+{
+    if (s0 != s1 && s0 != s2) return 0;
+    if (s1 != s0 && s1 != s2) return 1;
+    return 2;
+}
+
+// First stage: decides the general-position case (every vertex strictly off the
+// other triangle's plane) with filtered signs; everything else escalates.  For
+// an intersecting pair, *pat receives its endpoint pattern (make_pattern).
+// Inlined, on values only (the vertex choices are selects), so that nothing of
+// it lives in local memory.
+template <class T>
+__device__ __forceinline__ int classify_fast(const double3* P, const double3* Q, unsigned* pat = nullptr)
+{
+    const double3 P0 = P[0], P1 = P[1], P2 = P[2], Q0 = Q[0], Q1 = Q[1], Q2 = Q[2];
+    const Plane<T> pp = make_plane<T>(vdiff<T>(P1, P0), vdiff<T>(P2, P0));
     if (!pp.proper) return DEC_ESC;
-    int s2[3];
     // orient3d(P0,P1,P2,X) = (P0 - X) . nP
-    for (int j = 0; j < 3; j++) s2[j] = filt_dot<T>(pp, vdiff<T>(P[0], Q[j]));
-    if ((s2[0] == 1 && s2[1] == 1 && s2[2] == 1) || (s2[0] == -1 && s2[1] == -1 && s2[2] == -1)) return DEC_NO;
-    Plane<T> pq = make_plane<T>(vdiff<T>(Q[1], Q[0]), vdiff<T>(Q[2], Q[0]));
+    const int s20 = filt_dot<T>(pp, vdiff<T>(P0, Q0)), s21 = filt_dot<T>(pp, vdiff<T>(P0, Q1)),
+              s22 = filt_dot<T>(pp, vdiff<T>(P0, Q2));
+    if ((s20 == 1 && s21 == 1 && s22 == 1) || (s20 == -1 && s21 == -1 && s22 == -1)) return DEC_NO;
+    const Plane<T> pq = make_plane<T>(vdiff<T>(Q1, Q0), vdiff<T>(Q2, Q0));
     if (!pq.proper) return DEC_ESC;
-    int s1[3];
-    for (int i = 0; i < 3; i++) s1[i] = filt_dot<T>(pq, vdiff<T>(Q[0], P[i]));
-    if ((s1[0] == 1 && s1[1] == 1 && s1[2] == 1) || (s1[0] == -1 && s1[1] == -1 && s1[2] == -1)) return DEC_NO;
-    if (s1[0] == kUnsure || s1[1] == kUnsure || s1[2] == kUnsure || s2[0] == kUnsure || s2[1] == kUnsure ||
-        s2[2] == kUnsure)
+    const int s10 = filt_dot<T>(pq, vdiff<T>(Q0, P0)), s11 = filt_dot<T>(pq, vdiff<T>(Q0, P1)),
+              s12 = filt_dot<T>(pq, vdiff<T>(Q0, P2));
+    if ((s10 == 1 && s11 == 1 && s12 == 1) || (s10 == -1 && s11 == -1 && s12 == -1)) return DEC_NO;
+    if (s10 == kUnsure || s11 == kUnsure || s12 == kUnsure || s20 == kUnsure || s21 == kUnsure || s22 == kUnsure)
         return DEC_ESC;
-    // both intervals consist of two edge crossings from the lone vertex
-    int o1 = lone_index(s1), o2 = lone_index(s2);
-    double3 xn[2], xp[2], yn[2], yp[2];
-    int k = 0;
-    for (int i = 0; i < 3; i++) {
-        if (i == o1) continue;
-        xn[k] = s1[o1] < 0 ? P[o1] : P[i];
-        xp[k] = s1[o1] < 0 ? P[i] : P[o1];
-        k++;
-    }
-    k = 0;
-    for (int j = 0; j < 3; j++) {
-        if (j == o2) continue;
-        yn[k] = s2[o2] < 0 ? Q[o2] : Q[j];
-        yp[k] = s2[o2] < 0 ? Q[j] : Q[o2];
-        k++;
-    }
-    int c[2][2];
-    for (int i = 0; i < 2; i++)
-        for (int j = 0; j < 2; j++) {
-            c[i][j] = filt_o3<T>(xn[i], xp[i], yn[j], yp[j]);
-            if (c[i][j] == kUnsure) return DEC_ESC;
-        }
-    const unsigned xin = (c[0][0] * c[0][1] < 0 ? 1u : 0u) | (c[1][0] * c[1][1] < 0 ? 2u : 0u);
-    const unsigned yin = (c[0][0] * c[1][0] < 0 ? 1u : 0u) | (c[0][1] * c[1][1] < 0 ? 2u : 0u);
+    // both intervals consist of two edge crossings from the lone vertex; the
+    // edges in vertex order of their other end, each from its negative end
+    const int o1 = lone3(s10, s11, s12), o2 = lone3(s20, s21, s22);
+    const bool neg1 = (o1 == 0 ? s10 : (o1 == 1 ? s11 : s12)) < 0;
+    const bool neg2 = (o2 == 0 ? s20 : (o2 == 1 ? s21 : s22)) < 0;
+    const double3 L1 = sel3(o1, P0, P1, P2), A1 = o1 == 0 ? P1 : P0, B1 = o1 == 2 ? P1 : P2;
+    const double3 L2 = sel3(o2, Q0, Q1, Q2), A2 = o2 == 0 ? Q1 : Q0, B2 = o2 == 2 ? Q1 : Q2;
+    const double3 xn0 = neg1 ? L1 : A1, xp0 = neg1 ? A1 : L1, xn1 = neg1 ? L1 : B1, xp1 = neg1 ? B1 : L1;
+    const double3 yn0 = neg2 ? L2 : A2, yp0 = neg2 ? A2 : L2, yn1 = neg2 ? L2 : B2, yp1 = neg2 ? B2 : L2;
+    const int c00 = filt_o3<T>(xn0, xp0, yn0, yp0);
+    if (c00 == kUnsure) return DEC_ESC;
+    const int c01 = filt_o3<T>(xn0, xp0, yn1, yp1);
+    if (c01 == kUnsure) return DEC_ESC;
+    const int c10 = filt_o3<T>(xn1, xp1, yn0, yp0);
+    if (c10 == kUnsure) return DEC_ESC;
+    const int c11 = filt_o3<T>(xn1, xp1, yn1, yp1);
+    if (c11 == kUnsure) return DEC_ESC;
+    const unsigned xin = (c00 * c01 < 0 ? 1u : 0u) | (c10 * c11 < 0 ? 2u : 0u);
+    const unsigned yin = (c00 * c10 < 0 ? 1u : 0u) | (c01 * c11 < 0 ? 2u : 0u);
     if (!(xin | yin)) return DEC_NO;
     if (pat) *pat = make_pattern(o1, o2, xin, yin);
     return DEC_YES;
