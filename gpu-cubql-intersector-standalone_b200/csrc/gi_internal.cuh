@@ -122,7 +122,7 @@ struct Counters {
     unsigned bar_count;  // grid barrier: blocks arrived
     unsigned pad8[31];
     unsigned bar_gen;    // grid barrier: barriers completed
-    unsigned bstop;      // decision of the last completed barrier: 1 = the traversal is over
+    unsigned bstop;      // decision of the last completed barrier: 1 = the traversal is over (kept for the host)
     unsigned cand_total; // candidates made by the completed levels (written by the barriers' last arrivers)
     unsigned pad9[29];
     unsigned cand_ready; // candidates published to the candidate blocks (all written)
@@ -134,6 +134,9 @@ struct Counters {
     // stage, when the last block ended its key phase, after the count scan's
     // release, and when its last block ended
     unsigned long long fin_ns[5];
+    // level-synchronous traversal: the last completed barrier's level counts
+    // (lvl of the finished level) and stop decision, read by each block in one load
+    alignas(16) unsigned long long bpub[2];
     unsigned fin_done;  // blocks of k_finish that have ended
     unsigned pad11[31];
     unsigned fbar;      // k_finish: blocks arrived at the barrier after its key phase

@@ -1663,20 +1663,21 @@ __device__ __forceinline__ void st_relaxed_u32(unsigned* p, unsigned v)
 // arrived.  Its loads go out together and its stores are released by one
 // release store of the generation word, so the barrier costs few round trips
 // to L2 on its critical path.
-__device__ __forceinline__ bool level_barrier(const Bufs& B, unsigned& gen, unsigned lev, unsigned nblocks)
+__device__ __forceinline__ bool level_barrier(const Bufs& B, unsigned& gen, unsigned lev, unsigned nblocks,
+                                              unsigned long long& v_out, bool& stop_out)
 {
-    __shared__ unsigned s_ok;
+    __shared__ unsigned s_ok, s_stop;
+    __shared__ unsigned long long s_v;
     Counters* C = B.cnt;
     __syncthreads();
     if (threadIdx.x == 0) {
         s_ok = 1u;
-        __threadfence();  // this block's writes of the level before its arrival
-        const unsigned arrived = atomicAdd(&C->bar_count, 1u) + 1u;
+        // the arrival is an acquire-release atomic: it releases this block's
+        // writes of the level (ordered before it by the block barrier) and, for
+        // the last arriver, acquires every other block's
+        const unsigned arrived = arrive_acq_rel(&C->bar_count) + 1u;
         if (arrived == nblocks) {
-            // every block has arrived: the counts of this level are final (read
-            // through L2, where every block's fenced writes are; the acquire
-            // fence has no store of this thread to wait for)
-            fence_acq_rel();
+            // every block has arrived: the counts of this level are final
             const unsigned long long v = __ldcg(&C->lvl[lev % 3u]);
             const unsigned ab = __ldcg(&C->abort_);
             const unsigned prev = __ldcg(&C->cand_total);
@@ -1687,6 +1688,10 @@ __device__ __forceinline__ bool level_barrier(const Bufs& B, unsigned& gen, unsi
             const unsigned tot = prev + (unsigned)(v >> 32);
             C->bar_count = 0u;
             C->bstop = stop ? 1u : 0u;
+            C->bpub[0] = v;
+            C->bpub[1] = stop ? 1ull : 0ull;
+            s_v = v;
+            s_stop = stop ? 1u : 0u;
             C->lvl[(lev + 2u) % 3u] = 0ull;
             C->cand_total = tot;
             atomicMax(&C->q_tail, 2u * (unsigned)v);  // both halves of the queue buffer must hold the widest level
@@ -1708,10 +1713,16 @@ __device__ __forceinline__ bool level_barrier(const Bufs& B, unsigned& gen, unsi
                 }
                 __nanosleep(32);
             }
+            // the level's counts and the decision, published before the release
+            const ulonglong2 pub = __ldcg(reinterpret_cast<const ulonglong2*>(C->bpub));
+            s_v = pub.x;
+            s_stop = pub.y != 0ull ? 1u : 0u;
         }
         gen++;
     }
     __syncthreads();
+    v_out = s_v;
+    stop_out = s_stop != 0u;
     return s_ok != 0u;
 }
 
@@ -1954,10 +1965,11 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse_levels(Bufs B)
     if (node_block) seed_levels<F64>(B, gw, nw, front0, capL);
     else filter_published<F64>(B, decided, tested);
     for (; node_block;) {
-        if (!level_barrier(B, gen, lev, nblocks)) return;
-        if (__ldcg(&C->bstop)) break;
-        // the pairs made by level `lev`, expanded and filtered by level lev + 1
-        const unsigned long long v = __ldcg(&C->lvl[lev % 3u]);
+        unsigned long long v;
+        bool stop;
+        if (!level_barrier(B, gen, lev, nblocks, v, stop)) return;
+        if (stop) break;
+        // v: the pairs made by level `lev`, expanded and filtered by level lev + 1
         const unsigned n = min((unsigned)v, capL);
         const unsigned cbase = snap, cend = min(snap + (unsigned)(v >> 32), B.cap_cand);
         snap += (unsigned)(v >> 32);
@@ -2956,11 +2968,7 @@ __global__ void __launch_bounds__(kFinThreads, 2) k_finish(Bufs B, OrderBufs O, 
     }
     // ---- barrier: the last block to arrive scans the counts, then releases ----
     __syncthreads();
-    if (tid == 0) {
-        __threadfence();
-        s_last = atomicAdd(&C->fbar, 1u) == gridDim.x - 1u ? 1u : 0u;
-        __threadfence();
-    }
+    if (tid == 0) s_last = arrive_acq_rel(&C->fbar) == gridDim.x - 1u ? 1u : 0u;
     __syncthreads();
     if (s_last) {
         if (tid == 0) C->fin_ns[2] = globaltimer_ns();
