@@ -1380,6 +1380,41 @@ __device__ __forceinline__ void filter_candidates(const Bufs& B, bool have, cons
     }
 }
 
+// A traversal block's counts at its end: summed over its warps in shared
+// memory, then one atomic per counter for the block (every warp's own atomics
+// on the same three words queued up at the end of the launch).  Every thread
+// of the block must call it.
+__device__ __forceinline__ void block_stats(Counters* C, unsigned long long visited, unsigned long long decided,
+                                            unsigned long long tested, unsigned levels = 0u)
+{
+    __shared__ unsigned long long s_stats[4][kTravWarps];
+    for (int o = 16; o > 0; o >>= 1) {
+        visited += __shfl_xor_sync(0xffffffffu, visited, o);
+        decided += __shfl_xor_sync(0xffffffffu, decided, o);
+        tested += __shfl_xor_sync(0xffffffffu, tested, o);
+        levels = max(levels, __shfl_xor_sync(0xffffffffu, levels, o));
+    }
+    const unsigned warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31u) == 0u) {
+        s_stats[0][warp] = visited;
+        s_stats[1][warp] = decided;
+        s_stats[2][warp] = tested;
+        s_stats[3][warp] = levels;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4u) {
+        unsigned long long t = 0;
+#pragma unroll
+        for (int w = 0; w < kTravWarps; w++)
+            t = threadIdx.x == 3u ? max(t, s_stats[3][w]) : t + s_stats[threadIdx.x][w];
+        if (threadIdx.x == 3u) {
+            if (t) atomicMax(&C->levels, (unsigned)t);
+        } else if (t) {
+            atomicAdd(threadIdx.x == 0u ? &C->node_pairs : (threadIdx.x == 1u ? &C->filter_decided : &C->tested), t);
+        }
+    }
+}
+
 // QUAD selects the expansion form: one node pair per lane (32 per warp
 // iteration, the form for work-bound launches) or one per quad (8 per
 // iteration with a quarter of the dependent chain, the form for launches bound
@@ -1599,18 +1634,7 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
         __nanosleep(backoff);
         backoff = min(backoff * 2u, 256u);
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        visited += __shfl_xor_sync(0xffffffffu, visited, o);
-        decided += __shfl_xor_sync(0xffffffffu, decided, o);
-        tested += __shfl_xor_sync(0xffffffffu, tested, o);
-        maxlev = max(maxlev, __shfl_xor_sync(0xffffffffu, maxlev, o));
-    }
-    if (lane == 0) {
-        if (visited) atomicAdd(&C->node_pairs, visited);
-        if (decided) atomicAdd(&C->filter_decided, decided);
-        if (tested) atomicAdd(&C->tested, tested);
-        atomicMax(&C->levels, maxlev + 1u);
-    }
+    block_stats(C, visited, decided, tested, maxlev + 1u);
 }
 
 // ---------------------------------------------------------------------------
@@ -2054,16 +2078,7 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse_levels(Bufs B)
     // published candidates: the node blocks are done (the last barrier published
     // every candidate and the final flag) and filter what is left
     if (node_block && B.publish) filter_published<F64>(B, decided, tested);
-    for (int o = 16; o > 0; o >>= 1) {
-        visited += __shfl_xor_sync(0xffffffffu, visited, o);
-        decided += __shfl_xor_sync(0xffffffffu, decided, o);
-        tested += __shfl_xor_sync(0xffffffffu, tested, o);
-    }
-    if (lane == 0) {
-        if (visited) atomicAdd(&C->node_pairs, visited);
-        if (decided) atomicAdd(&C->filter_decided, decided);
-        if (tested) atomicAdd(&C->tested, tested);
-    }
+    block_stats(C, visited, decided, tested);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         C->levels = lev;
         C->work_cand = (unsigned long long)snap << 32;  // candidates made, for the host's retry sizing
