@@ -44,7 +44,7 @@ METRIC = "ms/intersect at 2×1.3M tris & tri-pair tests/s; pose-update p50/p99 v
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one traversal
 # launch on the level-8 pose workload with L2 flushed, from the ncu captures
 # summarised in profiles/k_traverse_config2.md, per traversal shape captured
-TRAVERSE_DRAM_BYTES = {0: 19.51e6 + 4.05e6, 6: 19.46e6 + 4.23e6, 7: 16.84e6 + 1.67e6}
+TRAVERSE_DRAM_BYTES = {0: 11.373824e6 + 512.0, 7: 13.247232e6 + 768.0}
 
 
 def parse():
