@@ -721,7 +721,9 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
         CK(c, cudaMemsetAsync(c->d_cnt, 0, sizeof(Counters), c->st), "counters");
         CK(c, cudaEventRecord(c->ev[0], c->st), "event");
         CK(c, launch_traverse(b, c->cfg, prec, trav_shape(shape), c->st), "traverse");
-        CK(c, cudaEventRecord(c->ev[1], c->st), "event");
+        // the finish follows the traversal directly (programmatic dependent
+        // launch): no event between them; the general path keeps its events
+        if (!fin) CK(c, cudaEventRecord(c->ev[1], c->st), "event");
         if (fin) {
             FinArgs F;
             F.segs = c->segs;
@@ -732,7 +734,7 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
             F.cap = cap;
             F.want_segments = want_segs ? 1 : 0;
             F.shift = fin_shift;
-            CK(c, launch_finish(b, O, F, c->cfg, c->st), "exact stage, segments and ordering");
+            CK(c, launch_finish(b, O, F, c->cfg, c->st, true), "exact stage, segments and ordering");
         } else {
             CK(c, launch_exact(b, c->cfg, c->st), "exact stage");
             CK(c, cudaEventRecord(c->ev[2], c->st), "event");
@@ -849,17 +851,20 @@ static gi_status run_jobs(gi_ctx* c, const std::vector<JobDev>& jobs, const gi_i
     c->pred_pairs = nres;
     c->pred_segs = nsegs;
     float ms_trav = 0, ms_exact = 0, ms_seg = 0, ms_sort = 0, ms_total = 0;
-    cudaEventElapsedTime(&ms_trav, c->ev[0], c->ev[1]);
     cudaEventElapsedTime(&ms_total, c->ev[0], c->ev[4]);
     if (fin) {
-        // one launch after the traversal: its phases from its own timestamps,
-        // the ordering takes the rest (launch included)
+        // the finish follows the traversal with no event between them: its span
+        // and phases from its own timestamps (taken after it waited for the
+        // traversal), the traversal the rest of the call
+        const double span = H.fin_ns[4] >= H.fin_ns[0] ? 1e-6 * double(H.fin_ns[4] - H.fin_ns[0]) : 0.0;
         if (H.fin_ns[1] >= H.fin_ns[0] && H.fin_ns[2] >= H.fin_ns[1]) {
             ms_exact = (float)(1e-6 * double(H.fin_ns[1] - H.fin_ns[0]));
             ms_seg = (float)(1e-6 * double(H.fin_ns[2] - H.fin_ns[1]));
         }
-        ms_sort = std::max(0.0f, ms_total - ms_trav - ms_exact - ms_seg);
+        ms_trav = std::max(0.0f, ms_total - (float)span);
+        ms_sort = std::max(0.0f, (float)span - ms_exact - ms_seg);
     } else {
+        cudaEventElapsedTime(&ms_trav, c->ev[0], c->ev[1]);
         cudaEventElapsedTime(&ms_exact, c->ev[1], c->ev[2]);
         cudaEventElapsedTime(&ms_seg, c->ev[2], c->ev[3]);
         cudaEventElapsedTime(&ms_sort, c->ev[3], c->ev[4]);

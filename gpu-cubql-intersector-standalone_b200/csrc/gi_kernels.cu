@@ -1245,6 +1245,20 @@ __device__ __forceinline__ unsigned ld_acq(const unsigned* p)
     return v;
 }
 
+// Programmatic dependent launch: the launch that follows on the stream (the
+// call's finish) may be scheduled now; it waits for this grid's completion and
+// memory before it reads anything (wait_prior_grid).  Without such a launch
+// both are no-ops.
+__device__ __forceinline__ void allow_dependent_launch()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+__device__ __forceinline__ void wait_prior_grid()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 __device__ __forceinline__ void fence_acq_rel()
 {
     asm volatile("fence.acq_rel.gpu;" ::: "memory");
@@ -1425,6 +1439,7 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse(Bufs B)
     constexpr unsigned kSlots = QUAD ? 8u : 32u;  // node-queue slots per ticket: one per work unit
     constexpr unsigned kStack = QUAD ? 8u : 32u;  // node pairs kept for the next iteration
     __shared__ uint4 stk[kTravWarps][kWarpStack];
+    allow_dependent_launch();
     Counters* C = B.cnt;
     const unsigned lane = threadIdx.x & 31;
     uint4* S = stk[threadIdx.x >> 5];
@@ -1981,6 +1996,7 @@ __global__ void __launch_bounds__(kTravThreads, 2) k_traverse_levels(Bufs B)
     const uint32_t capL = B.cap_queue / 2u;
     uint4* const front0 = B.queue;
     uint4* const front1 = B.queue + capL;
+    allow_dependent_launch();
     if (blockIdx.x == 0 && threadIdx.x == 0) C->t_start = globaltimer_ns();
     unsigned long long visited = 0, decided = 0, tested = 0;
     unsigned gen = 0, snap = 0, lev = 0;
@@ -2915,6 +2931,7 @@ __device__ __forceinline__ unsigned fin_scan_counts(const OrderBufs& O, Counters
 
 __global__ void __launch_bounds__(kFinThreads, 2) k_finish(Bufs B, OrderBufs O, FinArgs F)
 {
+    wait_prior_grid();  // the traversal's results are complete and visible
     extern __shared__ unsigned long long fin_dyn[];  // a big partition: kFinBig keys, then kFinBig values
     __shared__ uint32_t sw[33];
     __shared__ unsigned s_ok, s_last, s_redo, s_fill, s_nbig;
@@ -3134,16 +3151,35 @@ __global__ void __launch_bounds__(kFinThreads, 2) k_finish(Bufs B, OrderBufs O, 
     fin_end(C);
 }
 
-cudaError_t launch_finish(const Bufs& b, const OrderBufs& O, const FinArgs& F, const LaunchCfg& cfg, cudaStream_t st)
+cudaError_t launch_finish(const Bufs& b, const OrderBufs& O, const FinArgs& F, const LaunchCfg& cfg, cudaStream_t st,
+                          bool dependent)
 {
     Bufs bb = b;
     OrderBufs oo = O;
     FinArgs ff = F;
-    void* args[] = {&bb, &oo, &ff};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_finish, dim3(cfg.fin_per_sm * cfg.sms),
-                                                dim3(kFinThreads), args, kFinDyn, st);
     note_launches(1);
-    return e;
+    if (dependent) {
+        // cooperative, and a programmatic dependent of the traversal launched
+        // just before it on the stream: its launch overlaps the traversal's end
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(cfg.fin_per_sm * cfg.sms);
+        lc.blockDim = dim3(kFinThreads);
+        lc.dynamicSmemBytes = kFinDyn;
+        lc.stream = st;
+        cudaLaunchAttribute at[2];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[1].val.programmaticStreamSerializationAllowed = 1;
+        lc.attrs = at;
+        lc.numAttrs = 2;
+        const cudaError_t e = cudaLaunchKernelEx(&lc, k_finish, bb, oo, ff);
+        if (e == cudaSuccess) return e;
+        (void)cudaGetLastError();  // refused: launch it the plain cooperative way
+    }
+    void* args[] = {&bb, &oo, &ff};
+    return cudaLaunchCooperativeKernel((const void*)k_finish, dim3(cfg.fin_per_sm * cfg.sms), dim3(kFinThreads), args,
+                                      kFinDyn, st);
 }
 
 // ===========================================================================

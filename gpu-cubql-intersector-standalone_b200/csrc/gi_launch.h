@@ -153,7 +153,10 @@ struct FinArgs {
     int want_segments;
     int shift;          // partition of a key = key >> shift
 };
-cudaError_t launch_finish(const Bufs& b, const OrderBufs& O, const FinArgs& F, const LaunchCfg& cfg, cudaStream_t st);
+// dependent: launched right after the traversal on the same stream, with no
+// other stream work between them (programmatic dependent launch)
+cudaError_t launch_finish(const Bufs& b, const OrderBufs& O, const FinArgs& F, const LaunchCfg& cfg, cudaStream_t st,
+                          bool dependent = false);
 
 // Number of kernels launched by the launchers of this library (monotonic).
 unsigned long long launch_count();

@@ -145,9 +145,9 @@ typedef struct {
     double ms_segments;               /* device time: segment construction */
     double ms_sort;                   /* device time: output ordering (the part after segment construction
                                          ends; ranking overlaps the segments).  With the one-launch
-                                         finish (finish_phases = 4), ms_exact and ms_segments are its
-                                         phases' own spans and ms_sort the rest of the call after the
-                                         traversal, launch included */
+                                         finish (finish_phases = 4), ms_exact, ms_segments and ms_sort
+                                         are its phases' own spans (its timestamps) and ms_traverse the
+                                         rest of the call, the hand-off between the launches included */
     double ms_total;                  /* device time of the whole call */
     /* level-synchronous traversal only (else level_times = 0): level_end_ms[l]
      * is the time from the traversal's start to the end of level l (level 0:
