@@ -20,7 +20,9 @@
 //    back to its start is closed; vertices of degree 0 (isolated points) are
 //    one-vertex curves, and branch vertices (degree >= 3) end chains.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "gi_host.h"
@@ -30,6 +32,7 @@ struct gi_curves {
     std::vector<uint64_t> offsets;     // curve c: vertex ids idx[offsets[c] .. offsets[c+1])
     std::vector<uint32_t> idx;
     std::vector<uint8_t> closed;       // 1: the curve closes (its last vertex joins its first)
+    std::vector<uint64_t> job_curves;  // batch: job j owns curves [job_curves[j], job_curves[j + 1])
 };
 
 namespace {
@@ -56,19 +59,21 @@ inline uint64_t hash_pt(const PtKey& k)
 
 // Open-addressing hash table (linear probing, power-of-two capacity of at
 // least twice the number of keys it will hold): one flat allocation instead of
-// a node per entry.
+// a node per entry, kept between calls (reset clears only the flags).
 template <class K, class V>
 struct FlatMap {
     std::vector<K> keys;
     std::vector<V> vals;
     std::vector<uint8_t> used;
     size_t mask = 0;
-    explicit FlatMap(size_t max_keys)
+    void reset(size_t max_keys)
     {
         size_t cap = 16;
         while (cap < 2 * max_keys + 1) cap <<= 1;
-        keys.resize(cap);
-        vals.resize(cap);
+        if (keys.size() < cap) {
+            keys.resize(cap);
+            vals.resize(cap);
+        }
         used.assign(cap, 0);
         mask = cap - 1;
     }
@@ -98,30 +103,62 @@ inline PtKey key_of(const double* p)
     return k;
 }
 
+struct EdgeInfo {
+    uint32_t coplanar = 0, other = 0;
+};
+
+// Working tables of one thread, kept between calls: a call on a result of
+// similar size allocates nothing but its own output (fresh allocations and
+// their first-touch page faults cost more than the hashing itself).
+struct CurveScratch {
+    std::vector<uint32_t> per_pair;
+    std::vector<uint64_t> vslot;
+    std::vector<PtKey> vkeys;
+    FlatMap<uint64_t, EdgeInfo> edges;
+    std::vector<uint64_t> edge_keys;
+    std::vector<std::pair<uint32_t, uint32_t>> el;
+    std::vector<uint32_t> deg, nbr, nedge;
+    std::vector<uint64_t> start, fill;
+    std::vector<uint8_t> used;
+};
+
+CurveScratch& scratch()
+{
+    thread_local CurveScratch sc;
+    return sc;
+}
+
 }  // namespace
 
-extern "C" gi_status gi_curves_build(const double* seg6, const int32_t* seg_pair, uint64_t nsegs, uint64_t npairs,
-                                     int32_t drop_coplanar_interior, gi_curves** out)
+// The curves of one result (or one job of a batch): segments seg6[0 .. nsegs),
+// segment s of pair seg_pair[s] - pair_base in [0, npairs).
+template <class PairIndex>
+static void build_curves(const double* seg6, const PairIndex* seg_pair, int64_t pair_base, uint64_t nsegs,
+                         uint64_t npairs, int32_t drop_coplanar_interior, gi_curves* cv)
 {
-    if (!out || (nsegs && (!seg6 || !seg_pair))) return GI_ERR_INVALID_ARG;
-    *out = nullptr;
-    gi_curves* cv = new (std::nothrow) gi_curves();
-    if (!cv) return GI_ERR_OOM;
-    struct {
+    struct View {
         const double* segs;
-        const int32_t* seg_pair;
+        const PairIndex* sp;
+        int64_t base;
         uint64_t nsegs, npairs;
-    } rr{seg6, seg_pair, nsegs, npairs}, *r = &rr;
+        int64_t seg_pair_at(uint64_t s) const { return (int64_t)sp[s] - base; }
+    } rr{seg6, seg_pair, pair_base, nsegs, npairs}, *r = &rr;
     const uint64_t ns = r->nsegs;
+    CurveScratch& sc = scratch();
     // segments per pair: three mark a coplanar overlap triangle
-    std::vector<uint32_t> per_pair(r->npairs, 0);
-    for (uint64_t s = 0; s < ns; s++)
-        if (r->seg_pair[s] >= 0 && (uint64_t)r->seg_pair[s] < r->npairs) per_pair[r->seg_pair[s]]++;
+    std::vector<uint32_t>& per_pair = sc.per_pair;
+    per_pair.assign(r->npairs, 0);
+    for (uint64_t s = 0; s < ns; s++) {
+        const int64_t q = r->seg_pair_at(s);
+        if (q >= 0 && (uint64_t)q < r->npairs) per_pair[q]++;
+    }
     // vertex table: 8-byte slots (hash tag, vertex id + 1) over keys stored once in vertex order
     size_t vcap = 16;
     while (vcap < 4 * ns + 1) vcap <<= 1;
-    std::vector<uint64_t> vslot(vcap, 0);
-    std::vector<PtKey> vkeys;
+    std::vector<uint64_t>& vslot = sc.vslot;
+    vslot.assign(vcap, 0);
+    std::vector<PtKey>& vkeys = sc.vkeys;
+    vkeys.clear();
     vkeys.reserve(2 * ns);
     cv->verts.reserve(6 * ns);
     auto vertex = [&](const double* p) {
@@ -142,18 +179,18 @@ extern "C" gi_status gi_curves_build(const double* seg6, const int32_t* seg_pair
         cv->verts.insert(cv->verts.end(), p, p + 3);
         return id;
     };
-    struct EdgeInfo {
-        uint32_t coplanar = 0, other = 0;
-    };
-    FlatMap<uint64_t, EdgeInfo> edges(ns);
-    std::vector<uint64_t> edge_keys;  // distinct edges in first-seen order
+    FlatMap<uint64_t, EdgeInfo>& edges = sc.edges;
+    edges.reset(ns);
+    std::vector<uint64_t>& edge_keys = sc.edge_keys;  // distinct edges in first-seen order
+    edge_keys.clear();
     edge_keys.reserve(ns);
     for (uint64_t s = 0; s < ns; s++) {
         const double* a = r->segs + 6 * s;
         const uint32_t u = vertex(a), v = vertex(a + 3);
         if (u == v) continue;  // touching point: an isolated vertex unless an edge reaches it
         const uint64_t k = u < v ? ((uint64_t)u << 32) | v : ((uint64_t)v << 32) | u;
-        const bool cop = r->seg_pair[s] >= 0 && (uint64_t)r->seg_pair[s] < r->npairs && per_pair[r->seg_pair[s]] == 3;
+        const int64_t q = r->seg_pair_at(s);
+        const bool cop = q >= 0 && (uint64_t)q < r->npairs && per_pair[q] == 3;
         auto it = edges.emplace(k, EdgeInfo{}, mix64);
         if (it.second) edge_keys.push_back(k);
         EdgeInfo& e = *it.first;
@@ -161,7 +198,8 @@ extern "C" gi_status gi_curves_build(const double* seg6, const int32_t* seg_pair
         else e.other++;
     }
     const uint32_t nv = (uint32_t)(cv->verts.size() / 3);
-    std::vector<std::pair<uint32_t, uint32_t>> el;
+    std::vector<std::pair<uint32_t, uint32_t>>& el = sc.el;
+    el.clear();
     el.reserve(edge_keys.size());
     for (uint64_t k : edge_keys) {
         const EdgeInfo& e = *edges.emplace(k, EdgeInfo{}, mix64).first;
@@ -170,15 +208,21 @@ extern "C" gi_status gi_curves_build(const double* seg6, const int32_t* seg_pair
     }
     // edges in first-seen order: the curve order follows the segment order (deterministic)
     // adjacency (CSR)
-    std::vector<uint32_t> deg(nv + 1, 0);
+    std::vector<uint32_t>& deg = sc.deg;
+    deg.assign(nv + 1, 0);
     for (auto& e : el) {
         deg[e.first]++;
         deg[e.second]++;
     }
-    std::vector<uint64_t> start(nv + 1, 0);
+    std::vector<uint64_t>& start = sc.start;
+    start.assign(nv + 1, 0);
     for (uint32_t v = 0; v < nv; v++) start[v + 1] = start[v] + deg[v];
-    std::vector<uint32_t> nbr(2 * el.size()), nedge(2 * el.size());
-    std::vector<uint64_t> fill(start.begin(), start.end() - 1);
+    std::vector<uint32_t>& nbr = sc.nbr;
+    std::vector<uint32_t>& nedge = sc.nedge;
+    nbr.resize(2 * el.size());
+    nedge.resize(2 * el.size());
+    std::vector<uint64_t>& fill = sc.fill;
+    fill.assign(start.begin(), start.end() - 1);
     for (uint32_t i = 0; i < (uint32_t)el.size(); i++) {
         const uint32_t a = el[i].first, b = el[i].second;
         nbr[fill[a]] = b;
@@ -186,7 +230,8 @@ extern "C" gi_status gi_curves_build(const double* seg6, const int32_t* seg_pair
         nbr[fill[b]] = a;
         nedge[fill[b]++] = i;
     }
-    std::vector<uint8_t> used(el.size(), 0);
+    std::vector<uint8_t>& used = sc.used;
+    used.assign(el.size(), 0);
     cv->offsets.push_back(0);
     auto walk = [&](uint32_t v0, uint64_t slot) {
         // follow unused edges from v0 through vertices of degree 2
@@ -231,7 +276,118 @@ extern "C" gi_status gi_curves_build(const double* seg6, const int32_t* seg_pair
     for (uint32_t v = 0; v < nv; v++)
         for (uint64_t s = start[v]; s < start[v + 1]; s++)
             if (!used[nedge[s]]) walk(v, s);
+}
+
+extern "C" gi_status gi_curves_build(const double* seg6, const int32_t* seg_pair, uint64_t nsegs, uint64_t npairs,
+                                     int32_t drop_coplanar_interior, gi_curves** out)
+{
+    if (!out || (nsegs && (!seg6 || !seg_pair))) return GI_ERR_INVALID_ARG;
+    *out = nullptr;
+    gi_curves* cv = new (std::nothrow) gi_curves();
+    if (!cv) return GI_ERR_OOM;
+    try {
+        build_curves(seg6, seg_pair, 0, nsegs, npairs, drop_coplanar_interior, cv);
+    } catch (const std::bad_alloc&) {
+        delete cv;
+        return GI_ERR_OOM;
+    }
     *out = cv;
+    return GI_OK;
+}
+
+extern "C" gi_status gi_curves_build_jobs(const double* seg6, const int64_t* seg_pair, uint64_t nsegs,
+                                          const int64_t* pair_offsets, uint32_t njobs, int32_t drop_coplanar_interior,
+                                          gi_curves** out)
+{
+    if (!out || !pair_offsets || (nsegs && (!seg6 || !seg_pair))) return GI_ERR_INVALID_ARG;
+    *out = nullptr;
+    for (uint32_t j = 0; j < njobs; j++)
+        if (pair_offsets[j + 1] < pair_offsets[j]) return GI_ERR_INVALID_ARG;
+    for (uint64_t s = 1; s < nsegs; s++)
+        if (seg_pair[s] < seg_pair[s - 1]) return GI_ERR_INVALID_ARG;  // segments ordered by pair
+    // each job's segment range (the segments are ordered by pair, the pairs by job)
+    std::vector<uint64_t> sfirst(njobs + 1, 0);
+    uint64_t s = 0;
+    for (uint32_t j = 0; j < njobs; j++) {
+        while (s < nsegs && seg_pair[s] < pair_offsets[j]) s++;
+        sfirst[j] = s;
+    }
+    sfirst[njobs] = nsegs;
+    gi_curves* cv = new (std::nothrow) gi_curves();
+    if (!cv) return GI_ERR_OOM;
+    std::vector<gi_curves> part(njobs);
+    std::atomic<uint32_t> next{0};
+    std::atomic<bool> oom{false};
+    auto work = [&]() {
+        for (;;) {
+            const uint32_t j = next.fetch_add(1);
+            if (j >= njobs) return;
+            try {
+                build_curves(seg6 + 6 * sfirst[j], seg_pair + sfirst[j], pair_offsets[j], sfirst[j + 1] - sfirst[j],
+                             (uint64_t)(pair_offsets[j + 1] - pair_offsets[j]), drop_coplanar_interior, &part[j]);
+            } catch (const std::bad_alloc&) {
+                oom = true;
+                return;
+            }
+        }
+    };
+    // the jobs are independent: host threads take them one at a time
+    const unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), std::max(1u, njobs / 4u)));
+    auto run = [&](auto&& body) {
+        std::vector<std::thread> pool;
+        for (unsigned t = 1; t < nt; t++) pool.emplace_back(body);
+        body();
+        for (auto& t : pool) t.join();
+    };
+    run(work);
+    if (oom) {
+        delete cv;
+        return GI_ERR_OOM;
+    }
+    // concatenated in job order, vertex ids and curve offsets rebased: prefix
+    // counts first, then each thread copies its jobs into place
+    std::vector<uint64_t> vb(njobs + 1, 0), ib(njobs + 1, 0), cb(njobs + 1, 0);
+    for (uint32_t j = 0; j < njobs; j++) {
+        vb[j + 1] = vb[j] + part[j].verts.size() / 3;
+        ib[j + 1] = ib[j] + part[j].idx.size();
+        cb[j + 1] = cb[j] + part[j].closed.size();
+    }
+    try {
+        cv->verts.resize(3 * vb[njobs]);
+        cv->idx.resize(ib[njobs]);
+        cv->closed.resize(cb[njobs]);
+        cv->offsets.resize(cb[njobs] + 1);
+        cv->job_curves.assign(cb.begin(), cb.end());
+    } catch (const std::bad_alloc&) {
+        delete cv;
+        return GI_ERR_OOM;
+    }
+    cv->offsets[0] = 0;
+    next = 0;
+    run([&]() {
+        for (;;) {
+            const uint32_t j = next.fetch_add(1);
+            if (j >= njobs) return;
+            const gi_curves& p = part[j];
+            std::copy(p.verts.begin(), p.verts.end(), cv->verts.begin() + 3 * vb[j]);
+            const uint32_t v0 = (uint32_t)vb[j];
+            for (size_t k = 0; k < p.idx.size(); k++) cv->idx[ib[j] + k] = v0 + p.idx[k];
+            for (size_t c = 0; c < p.closed.size(); c++) {
+                cv->closed[cb[j] + c] = p.closed[c];
+                cv->offsets[cb[j] + c + 1] = ib[j] + p.offsets[c + 1];
+            }
+            gi_curves().verts.swap(const_cast<gi_curves&>(p).verts);  // release the part as it is copied
+        }
+    });
+    *out = cv;
+    return GI_OK;
+}
+
+extern "C" gi_status gi_curves_job_offsets(const gi_curves* c, const uint64_t** job_curves, uint64_t* njobs)
+{
+    if (!c || !job_curves || !njobs) return GI_ERR_INVALID_ARG;
+    *job_curves = c->job_curves.data();
+    *njobs = c->job_curves.empty() ? 0 : c->job_curves.size() - 1;
     return GI_OK;
 }
 

@@ -513,6 +513,64 @@ class Result:
         return curves(self.segments, self.seg_pair, self.npairs, drop_coplanar_interior)
 
 
+class _CurvesOwner:
+    """Keeps a gi_curves alive while views of its arrays exist."""
+
+    __slots__ = ("handle",)
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    def __del__(self):
+        if self.handle:
+            lib().gi_curves_free(self.handle)
+            self.handle = None
+
+
+def curves_of_jobs(segments, seg_pair, pair_offsets, drop_coplanar_interior=True):
+    """The curves of every job of a batch in one call (gi_curves_build_jobs):
+    segments (M, 6) ordered by pair, seg_pair (M,) batch-wide pair indices,
+    pair_offsets (njobs + 1,).  Returns flat arrays: vertices (V, 3), curve
+    offsets (C + 1,) into idx, idx (vertex ids), closed (C,) flags and
+    job_curves (njobs + 1,): job j owns curves job_curves[j] .. job_curves[j + 1].
+    The arrays are views of the library's (no copy), released with the last of them."""
+    L = lib()
+    seg = np.ascontiguousarray(segments, dtype=np.float64).reshape(-1, 6)
+    sp = np.ascontiguousarray(seg_pair, dtype=np.int64).reshape(-1)
+    po = np.ascontiguousarray(pair_offsets, dtype=np.int64).reshape(-1)
+    h = ctypes.c_void_p()
+    rc = L.gi_curves_build_jobs(seg.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                sp.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), seg.shape[0],
+                                po.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), max(po.shape[0] - 1, 0),
+                                1 if drop_coplanar_interior else 0, ctypes.byref(h))
+    if rc:
+        raise GIError(rc, "gi_curves_build_jobs")
+    owner = _CurvesOwner(h)
+    addr = lambda ptr: ctypes.cast(ptr, ctypes.c_void_p).value or 0
+
+    def view(ptr, shape, dtype):
+        if int(np.prod(shape)) == 0:
+            return np.zeros(shape, dtype=dtype)
+        return np.asarray(_View(owner, addr(ptr), shape, dtype))
+
+    vp = ctypes.POINTER(ctypes.c_double)()
+    nv = ctypes.c_uint64()
+    L.gi_curves_vertices(h, ctypes.byref(vp), ctypes.byref(nv))
+    off = ctypes.POINTER(ctypes.c_uint64)()
+    idx = ctypes.POINTER(ctypes.c_uint32)()
+    cl = ctypes.POINTER(ctypes.c_uint8)()
+    nc = ctypes.c_uint64()
+    L.gi_curves_polylines(h, ctypes.byref(off), ctypes.byref(idx), ctypes.byref(cl), ctypes.byref(nc))
+    jo = ctypes.POINTER(ctypes.c_uint64)()
+    nj = ctypes.c_uint64()
+    L.gi_curves_job_offsets(h, ctypes.byref(jo), ctypes.byref(nj))
+    o = view(off, (nc.value + 1,), np.uint64)
+    return dict(vertices=view(vp, (nv.value, 3), np.float64), offsets=o,
+                idx=view(idx, (int(o[-1]),), np.uint32),
+                closed=view(cl, (nc.value,), np.uint8).view(np.bool_),
+                job_curves=view(jo, (nj.value + 1,), np.uint64))
+
+
 class _BatchOwner:
     """Keeps every result handle of a batch alive while views of their shared block exist."""
 
@@ -569,6 +627,10 @@ class BatchResult:
         local = whole(qa, nsegs, soff, 1, np.int32)  # per job, relative to the job's first pair
         self.seg_pair = local.astype(np.int64) + np.repeat(self.offsets[:-1], nsegs)
         self.job = np.repeat(np.arange(n, dtype=np.uint32), npairs)
+
+    def curves(self, drop_coplanar_interior=True):
+        """Every job's curves in one call (see curves_of_jobs)."""
+        return curves_of_jobs(self.segments, self.seg_pair, self.offsets, drop_coplanar_interior)
 
 
 class Server:

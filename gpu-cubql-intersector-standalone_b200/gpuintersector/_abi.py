@@ -46,6 +46,7 @@ EXPORTED = [
     "gi_classify_pairs", "gi_classify_pairs_noalloc", "gi_predicate_signs",
     "gi_off_load", "gi_off_arrays", "gi_off_free", "gi_scene_load", "gi_mesh_download",
     "gi_curves_build", "gi_result_curves", "gi_curves_vertices", "gi_curves_polylines", "gi_curves_free",
+    "gi_curves_build_jobs", "gi_curves_job_offsets",
     "gi_records_write_csv", "gi_pairs_diff", "gi_sweep_poses",
     "gi_result_pairs", "gi_result_segments", "gi_result_stats", "gi_result_free",
     "gi_server_start", "gi_server_submit", "gi_server_poll", "gi_server_wait", "gi_server_stop",
@@ -179,6 +180,10 @@ def load(path=None):
         "gi_curves_polylines": ([vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_uint64)), ctypes.POINTER(up),
                                  ctypes.POINTER(ctypes.POINTER(ctypes.c_uint8)), ctypes.POINTER(ctypes.c_uint64)], st),
         "gi_curves_free": ([vp], st),
+        "gi_curves_build_jobs": ([dp, ctypes.POINTER(ctypes.c_int64), ctypes.c_uint64, ctypes.POINTER(ctypes.c_int64),
+                                  ctypes.c_uint32, ctypes.c_int32, ctypes.POINTER(vp)], st),
+        "gi_curves_job_offsets": ([vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_uint64)), ctypes.POINTER(ctypes.c_uint64)],
+                                  st),
         "gi_records_write_csv": ([ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_char_p,
                                   ctypes.POINTER(RecordMesh), ctypes.POINTER(RecordMesh),
                                   ctypes.POINTER(ctypes.c_int32), ctypes.c_uint64, ctypes.c_uint32], st),

@@ -350,6 +350,18 @@ gi_status gi_curves_vertices(const gi_curves* c, const double** xyz, uint64_t* n
 gi_status gi_curves_polylines(const gi_curves* c, const uint64_t** offsets, const uint32_t** verts,
                               const uint8_t** closed, uint64_t* ncurves);
 gi_status gi_curves_free(gi_curves* c);
+/* The curves of every job of a batch in one call (the flat batch arrays of
+ * gi_intersect_batch results): segments seg6[0 .. nsegs) ordered by their
+ * pair, seg_pair[s] a batch-wide pair index, job j owning pairs
+ * [pair_offsets[j], pair_offsets[j + 1]).  Each job's curves are those
+ * gi_curves_build gives for the job alone; the jobs are assembled on host
+ * threads and concatenated in job order (vertex ids across the batch), and
+ * gi_curves_job_offsets gives each job's range of curves. */
+gi_status gi_curves_build_jobs(const double* seg6, const int64_t* seg_pair, uint64_t nsegs,
+                               const int64_t* pair_offsets, uint32_t njobs, int32_t drop_coplanar_interior,
+                               gi_curves** out);
+/* job j: curves [job_curves[j], job_curves[j + 1]) */
+gi_status gi_curves_job_offsets(const gi_curves* c, const uint64_t** job_curves, uint64_t* njobs);
 
 /* ---- run records: CSV export and run diffs (tooling around the path) ------ */
 /* The reference's IntersectionHistory (src/CPU/IntersectionHistory.h:12-232)

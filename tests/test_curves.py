@@ -129,6 +129,35 @@ def test_curves_match_reference(gi, seed, drop):
     assert n_closed == (3 if drop else 2)  # two loops, plus the coplanar region's boundary when interiors drop
 
 
+@pytest.mark.parametrize("drop", [True, False])
+def test_curves_of_jobs_equal_per_job(gi, drop):
+    """gi_curves_build_jobs on a batch of soups (some jobs empty) gives, per
+    job, exactly what gi_curves_build gives for the job alone."""
+    rng = np.random.default_rng(11)
+    segs, gpair, offsets, jobs = [], [], [0], []
+    for j in range(40):
+        if j % 7 == 3:  # a job without segments, and one with pairs but no segments
+            jobs.append((np.zeros((0, 6)), np.zeros(0, np.int32), 2 if j % 2 else 0))
+        else:
+            seg, sp, npairs = _soup(rng)
+            order = np.argsort(sp, kind="stable")  # a result's segments are ordered by pair
+            jobs.append((seg[order], sp[order], npairs))
+        seg, sp, npairs = jobs[-1]
+        segs.append(seg)
+        gpair.append(sp.astype(np.int64) + offsets[-1])
+        offsets.append(offsets[-1] + npairs)
+    out = gi.curves_of_jobs(np.concatenate(segs), np.concatenate(gpair), np.array(offsets), drop)
+    assert len(out["job_curves"]) == len(jobs) + 1
+    for j, (seg, sp, npairs) in enumerate(jobs):
+        v, cv = gi.curves(seg, sp, npairs, drop_coplanar_interior=drop)
+        c0, c1 = int(out["job_curves"][j]), int(out["job_curves"][j + 1])
+        assert c1 - c0 == len(cv)
+        for k, (ids, closed) in enumerate(cv):
+            a, b = int(out["offsets"][c0 + k]), int(out["offsets"][c0 + k + 1])
+            assert bool(out["closed"][c0 + k]) == closed
+            assert np.array_equal(out["vertices"][out["idx"][a:b]], v[ids])
+
+
 def test_curves_empty_and_points(gi):
     v, cv = gi.curves(np.zeros((0, 6)), np.zeros(0, np.int32), 0)
     assert v.shape == (0, 3) and cv == []
