@@ -2766,11 +2766,13 @@ cudaError_t launch_order_small_phases(const Bufs& b, const OrderBufs& O, bool so
 // kFinMax results, keys of at most 63 bits):
 //   phase 0  the exact stage on the escalated pairs (only when there are any:
 //            the count is final at launch, so every block decides alike);
-//   phase 1  one result per thread (results spread over all blocks): its key
-//            goes into its partition (the key's top kFinPartBits bits) at the
-//            slot one atomic on the partition's count returns, in a fixed
-//            bucket of kFinBucket slots or, beyond it, one overflow list; then
-//            its segments, whose count the partition's segment count gains;
+//   phase 1  one result per thread, or per two adjacent threads when the grid
+//            has threads enough (each then builds one of the two endpoints),
+//            results spread over all blocks: its key goes into its partition
+//            (the key's top kFinPartBits bits) at the slot one atomic on the
+//            partition's count returns, in a fixed bucket of kFinBucket slots
+//            or, beyond it, one overflow list; then its segments, whose count
+//            the partition's segment count gains;
 //   barrier  the block that arrives last scans the partition counts into key
 //            and segment offsets and lists the partitions over kFinBucket keys
 //            before it releases the others;
@@ -2782,7 +2784,9 @@ cudaError_t launch_order_small_phases(const Bufs& b, const OrderBufs& O, bool so
 //            shared memory).
 // Every wait is bounded.  Over kFinMax results (or more results than threads),
 // a partition over kFinBig keys or a full overflow list make the kernel refuse
-// (Counters::order_redo, decided alike in every block).
+// (Counters::order_redo, decided alike in every block).  Launched as a
+// programmatic dependent of the traversal: it waits for the traversal's grid
+// (griddepcontrol.wait) before anything else.
 // ===========================================================================
 constexpr int kFinThreads = 256;
 constexpr int kFinWarps = kFinThreads / 32;
