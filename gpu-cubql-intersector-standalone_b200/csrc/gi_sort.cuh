@@ -14,6 +14,42 @@ namespace gi {
 // counts kernel launches made by this library (for gi_stats.launches)
 void note_launches(unsigned n);
 
+// Programmatic dependent launch of the build's kernels.  A kernel launched by
+// launch_dep may be scheduled while the kernel before it in the stream is still
+// finishing; at its first statement (pdl_enter) it waits for that kernel's
+// completion and memory (griddepcontrol.wait), then lets its own successor be
+// scheduled (griddepcontrol.launch_dependents).  Because the wait comes first
+// in every such kernel, each one starts its work after all earlier kernels of
+// the stream have completed, as in a plain launch; only the launch latency of
+// the next kernel overlaps the tail of the current one.  In a plain launch both
+// instructions are no-ops.
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Launches k(args...) with programmatic stream serialisation; a launch the
+// driver refuses is repeated as a plain launch.
+template <class... KArgs, class... Args>
+inline void launch_dep(void (*k)(KArgs...), unsigned grid, unsigned block, cudaStream_t st, Args... args)
+{
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(grid);
+    lc.blockDim = dim3(block);
+    lc.dynamicSmemBytes = 0;
+    lc.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    if (cudaLaunchKernelEx(&lc, k, args...) != cudaSuccess) {
+        (void)cudaGetLastError();
+        k<<<grid, block, 0, st>>>(args...);
+    }
+}
+
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;
@@ -50,6 +86,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
 
 __global__ void k_scan_tiles(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tile_sums)
 {
+    pdl_enter();
     __shared__ uint32_t sw[33];
     uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
@@ -71,6 +108,7 @@ __global__ void k_scan_tiles(const uint32_t* in, uint32_t* out, uint32_t n, uint
 
 __global__ void k_scan_add(uint32_t* out, uint32_t n, const uint32_t* tile_offsets)
 {
+    pdl_enter();
     uint32_t add = tile_offsets[blockIdx.x];
     uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
 #pragma unroll
@@ -93,14 +131,14 @@ inline void scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, uint32
     if (n == 0) return;
     uint32_t tiles = (n + kScanTile - 1) / kScanTile;
     if (tiles == 1) {
-        k_scan_tiles<<<1, kScanThreads, 0, st>>>(in, out, n, nullptr);
+        launch_dep(k_scan_tiles, 1, kScanThreads, st, in, out, n, (uint32_t*)nullptr);
         note_launches(1);
         return;
     }
     uint32_t* sums = temp;
-    k_scan_tiles<<<tiles, kScanThreads, 0, st>>>(in, out, n, sums);
+    launch_dep(k_scan_tiles, tiles, kScanThreads, st, in, out, n, sums);
     scan_exclusive(sums, sums, tiles, temp + tiles + 1, st);
-    k_scan_add<<<tiles, kScanThreads, 0, st>>>(out, n, sums);
+    launch_dep(k_scan_add, tiles, kScanThreads, st, out, n, (const uint32_t*)sums);
     note_launches(2);
 }
 
@@ -114,7 +152,7 @@ inline void scan_exclusive_split(const uint32_t* in, uint32_t* out, uint32_t n, 
     *sums = nullptr;
     if (n == 0) return;
     uint32_t tiles = (n + kScanTile - 1) / kScanTile;
-    k_scan_tiles<<<tiles, kScanThreads, 0, st>>>(in, out, n, tiles > 1 ? temp : nullptr);
+    launch_dep(k_scan_tiles, tiles, kScanThreads, st, in, out, n, tiles > 1 ? temp : (uint32_t*)nullptr);
     note_launches(1);
     if (tiles > 1) {
         scan_exclusive(temp, temp, tiles, temp + tiles + 1, st);
@@ -176,6 +214,7 @@ template <class K, int BITS>
 __global__ void __launch_bounds__(kRsThreads) k_rs_hist(const K* __restrict__ keys, uint32_t n, int shift,
                                                         uint32_t* __restrict__ counts, uint32_t ntiles)
 {
+    pdl_enter();
     constexpr uint32_t kDig = 1u << BITS;
     __shared__ uint32_t h[kDig];
     for (uint32_t d = threadIdx.x; d < kDig; d += kRsThreads) h[d] = 0;
@@ -196,6 +235,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K* __restrict__
                                                            int shift, const uint32_t* __restrict__ offsets,
                                                            const uint32_t* __restrict__ tile_sums, uint32_t ntiles)
 {
+    pdl_enter();
     constexpr uint32_t kDig = 1u << BITS;
     __shared__ uint32_t wc[kRsWarps][kDig];
     __shared__ uint32_t tile_off[kDig];
@@ -267,10 +307,11 @@ void radix_sort(K*& k0, uint32_t*& v0, K*& k1, uint32_t*& v1, uint32_t n, int bi
     K* kd = k1;
     uint32_t* vd = v1;
     for (int p = 0; p < passes; p++) {
-        k_rs_hist<K, BITS><<<ntiles, kRsThreads, 0, st>>>(ks, n, BITS * p, counts, ntiles);
+        launch_dep(k_rs_hist<K, BITS>, ntiles, kRsThreads, st, (const K*)ks, n, BITS * p, counts, ntiles);
         const uint32_t* sums = nullptr;
         scan_exclusive_split(counts, counts, (1u << BITS) * ntiles, temp, &sums, st);
-        k_rs_scatter<K, BITS><<<ntiles, kRsThreads, 0, st>>>(ks, vs, kd, vd, n, BITS * p, counts, sums, ntiles);
+        launch_dep(k_rs_scatter<K, BITS>, ntiles, kRsThreads, st, (const K*)ks, (const uint32_t*)vs, kd, vd, n,
+                   BITS * p, (const uint32_t*)counts, sums, ntiles);
         note_launches(2);
         K* tk = ks;
         ks = kd;
