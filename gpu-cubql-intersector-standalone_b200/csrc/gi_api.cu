@@ -234,7 +234,9 @@ static gi_status mesh_alloc(gi_ctx* c, uint32_t nv, uint32_t nt, gi_mesh** pm, c
     m->ctx = c;
     m->b.nv = nv;
     m->b.nt = nt;
-    size_t vb = sizeof(double) * 3 * (size_t)(nv ? nv : 1), tb = sizeof(uint32_t) * 3 * (size_t)(nt ? nt : 1);
+    // 16 bytes past the last vertex: the kernels read a vertex as the two
+    // aligned 16-byte vectors that hold it (load_vertex)
+    size_t vb = sizeof(double) * 3 * (size_t)(nv ? nv : 1) + 16, tb = sizeof(uint32_t) * 3 * (size_t)(nt ? nt : 1);
     if (c->budget && c->mesh_bytes + vb + tb > c->budget) {
         delete m;
         return sk.fail(GI_ERR_OOM, "HBM budget exceeded by mesh upload");

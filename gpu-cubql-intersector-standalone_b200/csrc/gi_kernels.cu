@@ -3,7 +3,7 @@
 // Build (once per mesh, replaces the reference's level-cut / forest builders,
 // include/third-party/cubql/level_cut_builder.h:278-364 and forest_builder.h:405-517,
 // which loop on the host with a device sync per tree level):
-//   k_validate -> k_tri_boxes -> k_morton -> radix sort -> k_karras_leaves (leaves + binary tree)
+//   k_validate -> k_tri_boxes -> k_morton_hist -> radix sort -> k_karras_leaves (leaves + binary tree)
 //   -> k_state_tables -> k_wide_flags -> scan -> k_collapse (size-greedy 4-wide nodes,
 //   topology) -> k_refit_wide (bottom-up over the wide tree, atomic arrival counters)
 // One host round trip, for the wide-node count (the node array's size).
@@ -117,9 +117,12 @@ __global__ void __launch_bounds__(kTriBoxThreads, 4) k_tri_boxes(const double* _
 #pragma unroll
         for (int q = 0; q < 2; q++)
 #pragma unroll
-            for (int j = 0; j < 3; j++)
-#pragma unroll
-                for (int k = 0; k < 3; k++) v[q][3 * j + k] = V[3 * (size_t)ix[q][j] + k];
+            for (int j = 0; j < 3; j++) {
+                const double3 p = load_vertex(V, ix[q][j]);
+                v[q][3 * j] = p.x;
+                v[q][3 * j + 1] = p.y;
+                v[q][3 * j + 2] = p.z;
+            }
 #pragma unroll
         for (int q = 0; q < 2; q++) {
             if (q == 1 && tt[1] == t) break;
@@ -177,30 +180,63 @@ __device__ __forceinline__ uint32_t spread10(uint32_t x)
     return x;
 }
 
-// 30-bit Morton key of triangle t: its box centre quantised to 10 bits per
-// axis over the centroid bounds cb (ordered-float min x, y, z, max x, y, z)
-__device__ __forceinline__ uint32_t morton_key(const float* __restrict__ box, uint32_t t, const unsigned* __restrict__ cb)
+// Box centre coordinate c quantised to 10 bits over [lo, lo + ext].
+__device__ __forceinline__ uint32_t morton_axis(float c, float lo, float ext)
 {
-    uint32_t q[3];
-    for (int k = 0; k < 3; k++) {
-        float lo = ord2f(cb[k]), hi = ord2f(cb[3 + k]);
-        float c = 0.5f * box[6 * (size_t)t + k] + 0.5f * box[6 * (size_t)t + 3 + k];
-        float ext = hi - lo;
-        float f = ext > 0.0f ? (c - lo) / ext : 0.0f;
-        f = fminf(fmaxf(f, 0.0f), 1.0f);
-        q[k] = (uint32_t)fminf(f * 1024.0f, 1023.0f);
-    }
-    return (spread10(q[0]) << 2) | (spread10(q[1]) << 1) | spread10(q[2]);
+    float f = ext > 0.0f ? (c - lo) / ext : 0.0f;
+    f = fminf(fmaxf(f, 0.0f), 1.0f);
+    return (uint32_t)fminf(f * 1024.0f, 1023.0f);
 }
 
-__global__ void k_morton(const float* __restrict__ box, uint32_t nt, const unsigned* __restrict__ cb,
-                         uint32_t* __restrict__ keys, uint32_t* __restrict__ vals)
+// 30-bit Morton keys of the triangles (their box centres quantised to 10 bits
+// per axis over the centroid bounds cb: ordered-float min x, y, z, max x, y,
+// z) with identity values, kRsTile triangles per block, and each block's counts
+// of the first radix digit in the layout of k_rs_hist (digit-major, one column
+// per block), so the sort's first pass needs no histogram launch.  All of a
+// thread's box loads are issued before its first shared-memory atomic.
+template <int BITS>
+__global__ void __launch_bounds__(kRsThreads) k_morton_hist(const float* __restrict__ box, uint32_t nt,
+                                                            const unsigned* __restrict__ cb,
+                                                            uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                                                            uint32_t* __restrict__ counts, uint32_t ntiles)
 {
     pdl_enter();
-    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nt) return;
-    keys[t] = morton_key(box, t, cb);
-    vals[t] = t;
+    constexpr uint32_t kDig = 1u << BITS;
+    __shared__ uint32_t h[kDig];
+    for (uint32_t d = threadIdx.x; d < kDig; d += kRsThreads) h[d] = 0;
+    float lo[3], ext[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        lo[k] = ord2f(cb[k]);
+        ext[k] = ord2f(cb[3 + k]) - lo[k];
+    }
+    const uint32_t base = blockIdx.x * kRsTile;
+    uint32_t kk[kRsItems];
+#pragma unroll
+    for (int it = 0; it < kRsItems; it++) {
+        const uint32_t t = base + it * kRsThreads + threadIdx.x;
+        kk[it] = 0;
+        if (t < nt) {
+            const float2* b2 = reinterpret_cast<const float2*>(box + 6 * (size_t)t);
+            const float2 a = b2[0], b = b2[1], c = b2[2];  // lo x, y | lo z, hi x | hi y, z
+            const uint32_t qx = morton_axis(0.5f * a.x + 0.5f * b.y, lo[0], ext[0]);
+            const uint32_t qy = morton_axis(0.5f * a.y + 0.5f * c.x, lo[1], ext[1]);
+            const uint32_t qz = morton_axis(0.5f * b.x + 0.5f * c.y, lo[2], ext[2]);
+            kk[it] = (spread10(qx) << 2) | (spread10(qy) << 1) | spread10(qz);
+        }
+    }
+    __syncthreads();  // the histogram is cleared
+#pragma unroll
+    for (int it = 0; it < kRsItems; it++) {
+        const uint32_t t = base + it * kRsThreads + threadIdx.x;
+        if (t < nt) {
+            keys[t] = kk[it];
+            vals[t] = t;
+            atomicAdd(&h[kk[it] & (kDig - 1u)], 1u);
+        }
+    }
+    __syncthreads();
+    for (uint32_t d = threadIdx.x; d < kDig; d += kRsThreads) counts[d * ntiles + blockIdx.x] = h[d];
 }
 
 __device__ __forceinline__ int kdelta(const uint32_t* __restrict__ keys, int n, int i, int j)
@@ -649,8 +685,10 @@ cudaError_t build_bvh(MeshBuffers& m, bool fp64, unsigned* d_err, cudaMemPool_t 
     // four resident blocks per SM, each looping: the centroid bounds take one set of atomics per block
     const int gboxes = (int)((n + 2 * kTriBoxThreads - 1) / (2 * kTriBoxThreads));
     k_tri_boxes<<<gboxes < 592 ? gboxes : 592, kTriBoxThreads, 0, st>>>(m.verts, m.nv, m.tris, n, box, box64, cb);
-    launch_dep(k_morton, gb, tb, st, (const float*)box, n, (const unsigned*)cb, k0, v0);
-    radix_sort<uint32_t, kMortonDigit>(k0, v0, k1, v1, n, 30, counts, stemp, st);
+    const uint32_t ntiles = (n + kRsTile - 1) / kRsTile;
+    launch_dep(k_morton_hist<kMortonDigit>, ntiles, kRsThreads, st, (const float*)box, n, (const unsigned*)cb, k0, v0,
+               counts, ntiles);
+    radix_sort<uint32_t, kMortonDigit>(k0, v0, k1, v1, n, 30, counts, stemp, st, true);
     if (n > 1) {
         GI_TRY(pool_alloc(&child, sizeof(uint4) * (n - 1), pool, st));
         GI_TRY(pool_alloc(&parent, sizeof(int) * (n - 1), pool, st));

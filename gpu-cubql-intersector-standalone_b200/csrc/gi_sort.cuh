@@ -219,11 +219,19 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_hist(const K* __restrict__ ke
     __shared__ uint32_t h[kDig];
     for (uint32_t d = threadIdx.x; d < kDig; d += kRsThreads) h[d] = 0;
     __syncthreads();
+    // every load of the tile is issued before the first shared-memory atomic
+    // (one round trip to memory per thread instead of one per few keys)
     uint32_t base = blockIdx.x * kRsTile;
-#pragma unroll 4
+    K kk[kRsItems];
+#pragma unroll
     for (int k = 0; k < kRsItems; k++) {
-        uint32_t i = base + k * kRsThreads + threadIdx.x;
-        if (i < n) atomicAdd(&h[(uint32_t)(keys[i] >> shift) & (kDig - 1u)], 1u);
+        const uint32_t i = base + k * kRsThreads + threadIdx.x;
+        kk[k] = i < n ? keys[i] : (K)0;
+    }
+#pragma unroll
+    for (int k = 0; k < kRsItems; k++) {
+        const uint32_t i = base + k * kRsThreads + threadIdx.x;
+        if (i < n) atomicAdd(&h[(uint32_t)(kk[k] >> shift) & (kDig - 1u)], 1u);
     }
     __syncthreads();
     for (uint32_t d = threadIdx.x; d < kDig; d += kRsThreads) counts[d * ntiles + blockIdx.x] = h[d];
@@ -294,10 +302,12 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K* __restrict__
 // digits.  The passes alternate between the two buffer pairs; on return
 // (k0, v0) point to the pair that holds the result and (k1, v1) to the other
 // (swapped after an odd number of passes, nothing copied).  Scratch: counts
-// radix_counts_words<BITS>(n) words, scan temp.
+// radix_counts_words<BITS>(n) words, scan temp.  hist0_done: the producer of the
+// keys already wrote the first pass's per-tile digit counts into `counts`
+// (layout of k_rs_hist: digit-major, one column per kRsTile keys).
 template <class K, int BITS = 8>
 void radix_sort(K*& k0, uint32_t*& v0, K*& k1, uint32_t*& v1, uint32_t n, int bits, uint32_t* counts, uint32_t* temp,
-                cudaStream_t st)
+                cudaStream_t st, bool hist0_done = false)
 {
     if (n <= 1) return;
     uint32_t ntiles = (n + kRsTile - 1) / kRsTile;
@@ -307,12 +317,15 @@ void radix_sort(K*& k0, uint32_t*& v0, K*& k1, uint32_t*& v1, uint32_t n, int bi
     K* kd = k1;
     uint32_t* vd = v1;
     for (int p = 0; p < passes; p++) {
-        launch_dep(k_rs_hist<K, BITS>, ntiles, kRsThreads, st, (const K*)ks, n, BITS * p, counts, ntiles);
+        if (p > 0 || !hist0_done) {
+            launch_dep(k_rs_hist<K, BITS>, ntiles, kRsThreads, st, (const K*)ks, n, BITS * p, counts, ntiles);
+            note_launches(1);
+        }
         const uint32_t* sums = nullptr;
         scan_exclusive_split(counts, counts, (1u << BITS) * ntiles, temp, &sums, st);
         launch_dep(k_rs_scatter<K, BITS>, ntiles, kRsThreads, st, (const K*)ks, (const uint32_t*)vs, kd, vd, n,
                    BITS * p, (const uint32_t*)counts, sums, ntiles);
-        note_launches(2);
+        note_launches(1);
         K* tk = ks;
         ks = kd;
         kd = tk;
