@@ -3277,11 +3277,13 @@ cudaError_t launch_traverse(const Bufs& b, const LaunchCfg& cfg, int precision, 
     const int f64 = precision == 1 ? 1 : 0, q = shape.quad ? 1 : 0;
     if (shape.levels) {
         // cooperative: the grid barriers need every block resident.  Bit 0 of the
-        // shape selects the split form: a third of the blocks filter candidates
-        // while the other two thirds expand the levels' node pairs
+        // shape selects the split form: a quarter of the blocks filter candidates
+        // while the other three quarters expand the levels' node pairs (config-2
+        // pose stream on B200: 0.1065 ms of traversal against 0.1072 with a third,
+        // 0.1075-0.1083 with a fifth, more with a half)
         const int grid = cfg.levels_per_sm[f64] * cfg.sms;
         Bufs bb = b;
-        bb.cand_blocks = shape.one_per_sm ? (unsigned)(grid / 3) : 0u;
+        bb.cand_blocks = shape.one_per_sm ? (unsigned)(grid / 4) : 0u;
         bb.publish = shape.one_per_sm ? 1u : 0u;
         bb.quad_below = shape.quad ? (unsigned)((grid - (int)bb.cand_blocks) * (kTravThreads / 32) * 8) : 0u;
         void* args[] = {&bb};

@@ -59,7 +59,7 @@ struct LaunchCfg {
 // of lanes; for the level-synchronous traversal, the quad form on levels of at
 // most 8 node pairs per warp); bit 0: the work-queue traversal with one block
 // per SM (else all resident), the level-synchronous one in its split form
-// (a third of the blocks only filter candidates).
+// (a quarter of the blocks only filter candidates).
 struct TravShape {
     bool quad = false;
     bool one_per_sm = false;
