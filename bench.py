@@ -44,9 +44,8 @@ METRIC = "ms/intersect at 2×1.3M tris & tri-pair tests/s; pose-update p50/p99 v
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one traversal
 # launch on the level-8 pose workload with L2 flushed, from the ncu captures
 # summarised in profiles/k_traverse_config2.md, per traversal shape captured
-# (shape 7 captured with a third of the blocks filtering candidates; the
-# library now gives them a quarter)
-TRAVERSE_DRAM_BYTES = {0: 11.373824e6 + 512.0, 7: 13.247232e6 + 768.0}
+# (shape 7 with a quarter of the blocks filtering candidates)
+TRAVERSE_DRAM_BYTES = {0: 11.373824e6 + 512.0, 7: 13.270784e6 + 256.0}
 
 
 def parse():
@@ -758,8 +757,7 @@ def main():
                      "traffic": TRAVERSE_DRAM_BYTES.get(int(st["traverse_shape"])) if args.level == 8 else None,
                      "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the "
                                        "traversal on this workload with the same shape (null: shape not captured); "
-                                       "profiles/k_traverse_config2.md, shape 7 captured with a third of the "
-                                       "blocks filtering candidates (a quarter now)",
+                                       "profiles/k_traverse_config2.md",
                      "kernel": "k_traverse", "peak_source": peak_src,
                      "alg_bytes_per_launch": float(alg_bytes),
                      "note": "output-sensitive traversal: bytes = node pairs x 2 nodes x 128 B + leaf pairs x "
