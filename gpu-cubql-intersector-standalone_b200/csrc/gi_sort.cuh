@@ -207,7 +207,8 @@ __device__ __forceinline__ bool lookback(unsigned* status, unsigned tile, unsign
 // ---------------------------------------------------------------------------
 // 12 keys per thread: 427 tiles of 3,072 keys for a 1.3M-triangle mesh, which
 // keeps more scatter warps resident per SM than 4,096-key tiles (build 0.435 ->
-// 0.418 ms on B200; 2,048-key tiles, 0.436 ms, pay more per-tile overhead)
+// 0.418 ms on B200; 10 and 14 keys per thread gave 0.427 and 0.426 ms, 8 keys
+// 0.436 ms: smaller tiles pay more per-tile overhead)
 constexpr int kRsThreads = 256;
 constexpr int kRsItems = 12;
 constexpr int kRsTile = kRsThreads * kRsItems;  // 3072
