@@ -31,17 +31,14 @@ constexpr int kUnsure = 2;
 enum { KIND_NONE = 0, KIND_POINT = 1, KIND_SEGMENT = 2, KIND_TRIANGLE = 3, KIND_POLYGON = 4 };
 enum { DEC_NO = 0, DEC_YES = 1, DEC_ESC = 2 };
 
-// ---------------------------------------------------------------------------
-// Posed vertex, bit-identical to the host order (RotationTools.h:135-143):
-// x = v - C; r = (R0 x + R1 y) + R2 z; out = (r + C) + T; no fused multiply-add.
-// ---------------------------------------------------------------------------
 // Vertex i of a mesh's vertex array (FP64 x, y, z), read as the two aligned
 // 16-byte vectors that hold it: its 24 bytes start on a 16-byte boundary for
 // even i and 8 bytes past one for odd i.  Two loads instead of three; the
 // array must be 16-byte aligned and padded by 16 bytes past its last vertex
 // (mesh uploads allocate it so).  The build's box kernel reads vertices this
 // way; the intersection kernels keep three scalar loads (world_vertex), which
-// measured faster there (0.127 against 0.129 ms per config-2 intersect).
+// measured faster there (0.127 against 0.129 ms per intersect of two
+// 1.3M-triangle meshes).
 __device__ __forceinline__ double3 load_vertex(const double* __restrict__ V, uint32_t i)
 {
     const size_t o = 3 * (size_t)i;
@@ -51,6 +48,10 @@ __device__ __forceinline__ double3 load_vertex(const double* __restrict__ V, uin
     return make_double3(odd ? a.y : a.x, odd ? b.x : a.y, odd ? b.y : b.x);
 }
 
+// ---------------------------------------------------------------------------
+// Posed vertex, bit-identical to the host order (RotationTools.h:135-143):
+// x = v - C; r = (R0 x + R1 y) + R2 z; out = (r + C) + T; no fused multiply-add.
+// ---------------------------------------------------------------------------
 __device__ __forceinline__ double3 world_vertex(const double* __restrict__ V, uint32_t i, const DevPose& P)
 {
     double x = __ldg(V + 3 * (size_t)i), y = __ldg(V + 3 * (size_t)i + 1), z = __ldg(V + 3 * (size_t)i + 2);

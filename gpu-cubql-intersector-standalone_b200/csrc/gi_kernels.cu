@@ -3278,8 +3278,8 @@ cudaError_t launch_traverse(const Bufs& b, const LaunchCfg& cfg, int precision, 
     if (shape.levels) {
         // cooperative: the grid barriers need every block resident.  Bit 0 of the
         // shape selects the split form: a quarter of the blocks filter candidates
-        // while the other three quarters expand the levels' node pairs (config-2
-        // pose stream on B200: 0.1065 ms of traversal against 0.1072 with a third,
+        // while the other three quarters expand the levels' node pairs (pose
+        // stream of two 1.3M-triangle meshes on B200: 0.1065 ms of traversal against 0.1072 with a third,
         // 0.1075-0.1083 with a fifth, more with a half)
         const int grid = cfg.levels_per_sm[f64] * cfg.sms;
         Bufs bb = b;
