@@ -83,3 +83,24 @@ def test_oneshot_error_on_either_mesh_leaves_context_usable(ctx, gi):
     assert len(r.pairs) == 1 and np.array_equal(r.pairs, r2.pairs)
     A.release()
     B.release()
+
+
+@pytest.mark.parametrize("nv", [1, 2, 3, 4, 7, 8, 1001])
+def test_vertex_vector_reads_stay_in_the_padding(nv):
+    """The build's box kernel reads vertex i as the two aligned 16-byte vectors
+    that hold it (load_vertex in csrc/gi_classify.cuh): doubles [o & ~1, (o & ~1) + 4)
+    with o = 3i, the vertex being the first three of them for even i and the
+    last three for odd i.  A restatement of that arithmetic on the CPU: every
+    vertex comes out right, each vector starts on a 16-byte boundary, and no read
+    passes the 16 bytes (two doubles) of padding that mesh uploads allocate after
+    the last vertex."""
+    rng = np.random.default_rng(nv)
+    v = rng.uniform(-1.0, 1.0, (nv, 3))
+    flat = np.concatenate([v.ravel(), [np.nan, np.nan]])  # the padding
+    for i in range(nv):
+        base = (3 * i) & ~1
+        assert (8 * base) % 16 == 0
+        assert base + 4 <= 3 * nv + 2
+        a, b = flat[base:base + 2], flat[base + 2:base + 4]
+        got = (a[1], b[0], b[1]) if i & 1 else (a[0], a[1], b[0])
+        assert np.array_equal(np.array(got), v[i])
